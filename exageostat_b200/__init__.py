@@ -1,0 +1,259 @@
+"""B200 (sm_100a) ExaGeoStat maximum-likelihood path.
+
+Python view of the C ABI declared in ``include/exageostat_b200.h``.  The compute
+lives in ``libexageostat_b200.so`` (built in-tree by ``exageostat_b200.build``);
+this module only marshals numpy arrays through ctypes.  There is no CPU
+fallback: if the shared library is missing, importing the bindings raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libexageostat_b200.so")
+
+EGS_OK = 0
+EGS_ERR_INVALID = -1
+EGS_ERR_CUDA = -2
+EGS_ERR_NO_DEVICE = -3
+EGS_ERR_OOM = -4
+EGS_ERR_TIMEOUT = -5
+EGS_ERR_STATE = -6
+
+STAGES = ("generate", "panel", "update", "solve", "reduce")
+NUM_STAGES = len(STAGES)
+
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int)
+_LL = ctypes.POINTER(ctypes.c_longlong)
+_P = ctypes.c_void_p
+
+# name -> (restype, argtypes); every symbol of include/exageostat_b200.h.
+SIGNATURES = {
+    "egs_version": (ctypes.c_int, []),
+    "egs_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "egs_last_error": (ctypes.c_char_p, []),
+    "egs_hardware_init": (ctypes.c_int, [ctypes.c_int]),
+    "egs_problem_create": (ctypes.c_int, [ctypes.POINTER(_P), ctypes.c_int, ctypes.c_int]),
+    "egs_problem_destroy": (ctypes.c_int, [_P]),
+    "egs_problem_info": (ctypes.c_int, [_P, _I, _I, _I, _LL]),
+    "egs_problem_set_stream": (ctypes.c_int, [_P, _P]),
+    "egs_problem_set_locations": (ctypes.c_int, [_P, _D, _D]),
+    "egs_problem_set_locations_device": (ctypes.c_int, [_P, _P, _P]),
+    "egs_problem_set_observations": (ctypes.c_int, [_P, _D]),
+    "egs_problem_set_observations_device": (ctypes.c_int, [_P, _P]),
+    "egs_covariance_generate": (ctypes.c_int, [_P, _D]),
+    "egs_potrf": (ctypes.c_int, [_P]),
+    "egs_restore_observations": (ctypes.c_int, [_P]),
+    "egs_trsv": (ctypes.c_int, [_P]),
+    "egs_loglik_parts": (ctypes.c_int, [_P, _D, _D, _D]),
+    "egs_get_tile": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, _D]),
+    "egs_get_observations": (ctypes.c_int, [_P, _D]),
+    "egs_mle_eval": (ctypes.c_int, [_P, _D, _D, _D, _D]),
+    "egs_generate_locations": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _D, _D]),
+    "egs_dlarnv_normal": (ctypes.c_int, [_I, ctypes.c_int, _D]),
+    "egs_generate_observations": (ctypes.c_int, [_P, _D, ctypes.c_int, _D]),
+    "egs_problem_set_profiling": (ctypes.c_int, [_P, ctypes.c_int]),
+    "egs_problem_stage_stats": (ctypes.c_int, [_P, _D, _D, _LL]),
+    "egs_matern_block": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P, _P, _P, _D,
+                                        ctypes.c_int, _P]),
+    "egs_mle_loglik_host": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _D]),
+    "egs_predict_host": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _D, _D, _D,
+                                        _D, _D]),
+}
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Load the sm_100a library and declare every C ABI signature."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with `python -m exageostat_b200.build`; "
+                           "this package has no CPU fallback")
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+class EgsError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        lib = load_library()
+        msg = lib.egs_status_string(status).decode()
+        detail = lib.egs_last_error().decode()
+        super().__init__(f"{where}: {msg} ({status}) {detail}")
+        self.status = status
+
+
+class NotPositiveDefinite(EgsError):
+    pass
+
+
+def _check(status: int, where: str) -> None:
+    if status == EGS_OK:
+        return
+    if status > 0:
+        raise NotPositiveDefinite(status, where)
+    raise EgsError(status, where)
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(_D)
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Problem:
+    """Device-resident problem of n locations (``egs_problem``)."""
+
+    def __init__(self, n: int, dts: int):
+        self._lib = load_library()
+        self._h = _P()
+        _check(self._lib.egs_problem_create(ctypes.byref(self._h), int(n), int(dts)), "egs_problem_create")
+        self.n = int(n)
+        self.dts = int(dts)
+        nn, ts, nt, nb = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()
+        self._lib.egs_problem_info(self._h, ctypes.byref(nn), ctypes.byref(ts), ctypes.byref(nt), ctypes.byref(nb))
+        self.ts, self.nt, self.device_bytes = ts.value, nt.value, nb.value
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.egs_problem_destroy(self._h)
+            self._h = _P()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_locations(self, x, y) -> None:
+        x, y = _f64(x), _f64(y)
+        assert x.size == self.n and y.size == self.n
+        _check(self._lib.egs_problem_set_locations(self._h, _dptr(x), _dptr(y)), "set_locations")
+
+    def set_observations(self, z) -> None:
+        z = _f64(z)
+        assert z.size == self.n
+        _check(self._lib.egs_problem_set_observations(self._h, _dptr(z)), "set_observations")
+
+    def generate(self, theta) -> None:
+        th = _f64(theta)
+        _check(self._lib.egs_covariance_generate(self._h, _dptr(th)), "covariance_generate")
+
+    def potrf(self) -> None:
+        _check(self._lib.egs_potrf(self._h), "potrf")
+
+    def restore_observations(self) -> None:
+        _check(self._lib.egs_restore_observations(self._h), "restore_observations")
+
+    def trsv(self) -> None:
+        _check(self._lib.egs_trsv(self._h), "trsv")
+
+    def loglik_parts(self):
+        a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        _check(self._lib.egs_loglik_parts(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)),
+               "loglik_parts")
+        return a.value, b.value, c.value
+
+    def tile(self, i: int, j: int) -> np.ndarray:
+        out = np.empty((self.ts, self.ts), dtype=np.float64, order="F")
+        _check(self._lib.egs_get_tile(self._h, i, j, out.ctypes.data_as(_D)), "get_tile")
+        return out
+
+    def lower_matrix(self) -> np.ndarray:
+        """Assemble the stored lower tiles into an n x n lower-triangular array (tests)."""
+        npad = self.nt * self.ts
+        full = np.zeros((npad, npad))
+        for j in range(self.nt):
+            for i in range(j, self.nt):
+                full[i * self.ts:(i + 1) * self.ts, j * self.ts:(j + 1) * self.ts] = self.tile(i, j)
+        return np.tril(full)[: self.n, : self.n]
+
+    def observations(self) -> np.ndarray:
+        out = np.empty(self.n)
+        _check(self._lib.egs_get_observations(self._h, _dptr(out)), "get_observations")
+        return out
+
+    def generate_observations(self, theta, seed: int) -> np.ndarray:
+        """Z = L e at theta (the reference's synthetic observations); returns Z."""
+        th = _f64(theta)
+        z = np.empty(self.n)
+        _check(self._lib.egs_generate_observations(self._h, _dptr(th), int(seed), _dptr(z)),
+               "generate_observations")
+        return z
+
+    def set_profiling(self, enable: bool) -> None:
+        _check(self._lib.egs_problem_set_profiling(self._h, 1 if enable else 0), "set_profiling")
+
+    def stage_stats(self):
+        """(ms[5], flops[5], launches[5]) per stage: generate, panel, update, solve, reduce."""
+        ms = np.zeros(NUM_STAGES)
+        fl = np.zeros(NUM_STAGES)
+        ln = (ctypes.c_longlong * NUM_STAGES)()
+        _check(self._lib.egs_problem_stage_stats(self._h, _dptr(ms), _dptr(fl), ln), "stage_stats")
+        return ms, fl, np.array(list(ln), dtype=np.int64)
+
+    def set_stream(self, cuda_stream_handle) -> None:
+        _check(self._lib.egs_problem_set_stream(self._h, _P(cuda_stream_handle)), "set_stream")
+
+    def mle_eval(self, theta):
+        th = _f64(theta)
+        ll, ld, dt = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        _check(self._lib.egs_mle_eval(self._h, _dptr(th), ctypes.byref(ll), ctypes.byref(ld), ctypes.byref(dt)),
+               "mle_eval")
+        return ll.value, ld.value, dt.value
+
+
+def mle_loglik_host(x, y, z, theta, dts: int) -> float:
+    lib = load_library()
+    x, y, z, th = _f64(x), _f64(y), _f64(z), _f64(theta)
+    out = ctypes.c_double()
+    _check(lib.egs_mle_loglik_host(len(z), int(dts), _dptr(x), _dptr(y), _dptr(z), _dptr(th), ctypes.byref(out)),
+           "mle_loglik_host")
+    return out.value
+
+
+def predict_host(x_obs, y_obs, z_obs, x_miss, y_miss, theta, dts: int, z_actual=None):
+    lib = load_library()
+    x_obs, y_obs, z_obs = _f64(x_obs), _f64(y_obs), _f64(z_obs)
+    x_miss, y_miss, th = _f64(x_miss), _f64(y_miss), _f64(theta)
+    nm = len(x_miss)
+    zm = np.empty(nm)
+    mspe = ctypes.c_double()
+    za = _dptr(_f64(z_actual)) if z_actual is not None else None
+    keep = _f64(z_actual) if z_actual is not None else None  # noqa: F841 (keeps the buffer alive)
+    if keep is not None:
+        za = _dptr(keep)
+    _check(lib.egs_predict_host(len(z_obs), nm, int(dts), _dptr(x_obs), _dptr(y_obs), _dptr(z_obs), _dptr(x_miss),
+                                _dptr(y_miss), za, _dptr(th), _dptr(zm), ctypes.byref(mspe)), "predict_host")
+    return zm, mspe.value
+
+
+def generate_locations(n: int, seed: int, reseed: bool = True):
+    """The reference's synthetic locations (libc srand/rand, Morton sorted)."""
+    lib = load_library()
+    x, y = np.empty(n), np.empty(n)
+    _check(lib.egs_generate_locations(int(n), int(seed), 1 if reseed else 0, _dptr(x), _dptr(y)),
+           "generate_locations")
+    return x, y
+
+
+def dlarnv_normal(seed: int, n: int) -> np.ndarray:
+    """LAPACK DLARNV(3, {seed, seed, seed, 1}, n) restated in the library."""
+    lib = load_library()
+    iseed = (ctypes.c_int * 4)(seed, seed, seed, 1)
+    out = np.empty(n)
+    _check(lib.egs_dlarnv_normal(iseed, int(n), _dptr(out)), "dlarnv_normal")
+    return out

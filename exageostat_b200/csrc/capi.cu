@@ -1,0 +1,682 @@
+// extern "C" boundary of the B200 maximum-likelihood path and the host-side
+// driver that sequences the device kernels of one evaluation.
+//
+// The evaluation follows ChameleonImplementation<T>::ExaGeoStatMLETile
+// (src/linear-algebra-solvers/concrete/chameleon/ChameleonImplementation.cpp:35-327):
+//   Z <- Zcpy (:113-125), C <- Matern(theta) lower tiles (:168-174),
+//   C <- chol(C) (:180), logdet (:188-192), Z <- L^-1 Z (:216), dot (:224),
+//   loglik (:257-265).
+// All stages of one evaluation are enqueued on the problem's stream; the host
+// blocks once per evaluation to read a 32-byte result record.
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+#include <cuda.h>
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace egs {
+
+static thread_local std::string g_last_error;
+
+void set_last_error(const char* what, const char* where) {
+  g_last_error = std::string(what ? what : "") + (where ? std::string(" [") + where + "]" : std::string());
+}
+
+}  // namespace egs
+
+using namespace egs;
+
+struct egs_problem {
+  int n = 0, dts = 0, ts = 0, nt = 0, np = 0;
+  long long ntiles = 0;
+  long long bytes = 0;
+  double* tiles = nullptr;
+  double* x = nullptr;
+  double* y = nullptr;
+  double* z = nullptr;
+  double* zcpy = nullptr;
+  double* partial = nullptr;
+  double* result = nullptr;
+  int* flags = nullptr;  // [0] potrf info, [1] device wait error
+  MaternParams* dparams = nullptr;
+  // pinned host mirrors
+  MaternParams* hparams = nullptr;
+  double* hresult = nullptr;
+  int* hflags = nullptr;
+  alignas(64) unsigned char tmap[128];
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  bool have_locations = false;
+  bool have_observations = false;
+  // Per-stage accounting: launch counts always, CUDA-event times when profiling.
+  bool profiling = false;
+  struct Span {
+    int stage;
+    cudaEvent_t a, b;
+    double flops;
+  };
+  std::vector<cudaEvent_t> events;
+  size_t events_used = 0;
+  std::vector<Span> spans;
+  double stage_ms[EGS_NUM_STAGES] = {};
+  double stage_flops[EGS_NUM_STAGES] = {};
+  long long stage_launches[EGS_NUM_STAGES] = {};
+};
+
+namespace {
+
+constexpr int kInnerBlock = 64;
+
+int round_tile(int dts) {
+  int ts = dts < kInnerBlock ? kInnerBlock : dts;
+  return ((ts + kInnerBlock - 1) / kInnerBlock) * kInnerBlock;
+}
+
+int check_cuda(const char* where) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_last_error(cudaGetErrorString(e), where);
+    return EGS_ERR_CUDA;
+  }
+  return EGS_OK;
+}
+
+cudaEvent_t take_event(egs_problem* p) {
+  if (p->events_used == p->events.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    p->events.push_back(e);
+  }
+  return p->events[p->events_used++];
+}
+
+// Opens a timed span of `stage` on the problem stream (no-op unless profiling).
+int span_begin(egs_problem* p, int stage) {
+  if (!p->profiling) return -1;
+  egs_problem::Span s{stage, take_event(p), take_event(p), 0.0};
+  cudaEventRecord(s.a, p->stream);
+  p->spans.push_back(s);
+  return (int)p->spans.size() - 1;
+}
+
+void span_end(egs_problem* p, int idx, double flops) {
+  if (idx < 0) return;
+  cudaEventRecord(p->spans[idx].b, p->stream);
+  p->spans[idx].flops = flops;
+}
+
+void count_launches(egs_problem* p, int stage, long long n) { p->stage_launches[stage] += n; }
+
+// After the stream has been synchronised: fold the recorded spans into the totals.
+void collect_spans(egs_problem* p) {
+  for (auto& s : p->spans) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, s.a, s.b) == cudaSuccess) {
+      p->stage_ms[s.stage] += ms;
+      p->stage_flops[s.stage] += s.flops;
+    }
+  }
+  cudaGetLastError();
+  p->spans.clear();
+  p->events_used = 0;
+}
+
+template <typename T>
+int dev_alloc(T** p, size_t count, long long* bytes) {
+  const size_t b = count * sizeof(T);
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), b);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    set_last_error(cudaGetErrorString(e), "cudaMalloc");
+    *p = nullptr;
+    return e == cudaErrorMemoryAllocation ? EGS_ERR_OOM : EGS_ERR_CUDA;
+  }
+  *bytes += (long long)b;
+  return EGS_OK;
+}
+
+void free_problem(egs_problem* p) {
+  if (!p) return;
+  if (p->stream) cudaStreamSynchronize(p->stream);
+  cudaFree(p->tiles);
+  cudaFree(p->x);
+  cudaFree(p->y);
+  cudaFree(p->z);
+  cudaFree(p->zcpy);
+  cudaFree(p->partial);
+  cudaFree(p->result);
+  cudaFree(p->flags);
+  cudaFree(p->dparams);
+  cudaFreeHost(p->hparams);
+  cudaFreeHost(p->hresult);
+  cudaFreeHost(p->hflags);
+  if (p->own_stream && p->stream) cudaStreamDestroy(p->stream);
+  for (cudaEvent_t e : p->events) cudaEventDestroy(e);
+  delete p;
+}
+
+// Right-looking tiled Cholesky of the lower tiles (replaces CHAMELEON_dpotrf_Tile).
+// Step k: factor diagonal tile k (64-wide blocked: potrf of the 64x64 block,
+// row solve below it, tensor-core syrk of the rest of the tile), solve the tile
+// column below it (64-wide blocked: row solve + tensor-core update), then the
+// tensor-core trailing update of every tile (i, j), k < j <= i.
+int enqueue_potrf(egs_problem* p) {
+  const int ts = p->ts, nt = p->nt, n = p->n;
+  cudaStream_t st = p->stream;
+  int* info = p->flags;
+  int* err = p->flags + 1;
+  for (int k = 0; k < nt; ++k) {
+    const long long skk = tile_slot(k, k, nt);
+    int sp = span_begin(p, EGS_STAGE_PANEL);
+    for (int kb = 0; kb < ts; kb += kInnerBlock) {
+      launch_potrf_diag_block(p->tiles, ts, skk, kb, k * ts, info, st);
+      count_launches(p, EGS_STAGE_PANEL, 1);
+      if (kb + kInnerBlock < ts) {
+        launch_trsm_rows(p->tiles, ts, skk, 1, kb + kInnerBlock, kb, skk, st);
+        const int r0 = k * ts + kb + kInnerBlock;
+        const int m = ts - kb - kInnerBlock;
+        int rc = launch_gemm_rows(p->tmap, p->tiles, ts, nt, m, m, kInnerBlock, r0, kb, k, r0, kb, k, r0, r0, 1,
+                                  err, st);
+        if (rc != EGS_OK) return rc;
+        count_launches(p, EGS_STAGE_PANEL, 2);
+      }
+    }
+    if (k < nt - 1) {
+      const long long s0 = tile_slot(k + 1, k, nt);
+      const int ntl = nt - 1 - k;
+      for (int kb = 0; kb < ts; kb += kInnerBlock) {
+        launch_trsm_rows(p->tiles, ts, s0, ntl, 0, kb, skk, st);
+        count_launches(p, EGS_STAGE_PANEL, 1);
+        if (kb + kInnerBlock < ts) {
+          const int m = ntl * ts;
+          const int ncols = ts - kb - kInnerBlock;
+          const int brow = k * ts + kb + kInnerBlock;
+          int rc = launch_gemm_rows(p->tmap, p->tiles, ts, nt, m, ncols, kInnerBlock, (k + 1) * ts, kb, k, brow,
+                                    kb, k, (k + 1) * ts, brow, 0, err, st);
+          if (rc != EGS_OK) return rc;
+          count_launches(p, EGS_STAGE_PANEL, 1);
+        }
+      }
+    }
+    // Algorithmic flops of the panel step on the real (unpadded) rows: potrf of the
+    // diagonal block plus the triangular solve of the rows below it.
+    {
+      const double w = (double)std::min(ts, n - k * ts);
+      const double below = (double)std::max(0, n - (k + 1) * ts);
+      span_end(p, sp, w * w * w / 3.0 + w * w / 2.0 + w / 6.0 + below * w * w);
+    }
+    if (k < nt - 1) {
+      sp = span_begin(p, EGS_STAGE_UPDATE);
+      int rc = launch_gemm_trailing(p->tmap, p->tiles, ts, nt, k, err, st);
+      if (rc != EGS_OK) return rc;
+      count_launches(p, EGS_STAGE_UPDATE, 1);
+      const double m = (double)std::max(0, n - (k + 1) * ts);
+      span_end(p, sp, m * (m + 1.0) * (double)ts);
+    }
+  }
+  return check_cuda("enqueue_potrf");
+}
+
+// Z := L^-1 Z, tile by tile (forward substitution).
+void enqueue_trsv(egs_problem* p) {
+  const int sp = span_begin(p, EGS_STAGE_SOLVE);
+  for (int k = 0; k < p->nt; ++k) {
+    launch_trsv_diag(p->tiles, p->ts, tile_slot(k, k, p->nt), p->z + (long long)k * p->ts, p->stream);
+    launch_gemv_panel(p->tiles, p->ts, p->nt, k, p->z, p->stream);
+    count_launches(p, EGS_STAGE_SOLVE, k < p->nt - 1 ? 2 : 1);
+  }
+  span_end(p, sp, (double)p->n * (double)p->n);
+}
+
+// Z := L^-T Z (backward substitution), the second half of dposv.
+void enqueue_trsv_t(egs_problem* p) {
+  const int sp = span_begin(p, EGS_STAGE_SOLVE);
+  for (int k = p->nt - 1; k >= 0; --k) {
+    launch_trsv_t_diag(p->tiles, p->ts, tile_slot(k, k, p->nt), p->z + (long long)k * p->ts, p->stream);
+    launch_gemv_t_panel(p->tiles, p->ts, p->nt, k, p->z, p->stream);
+    count_launches(p, EGS_STAGE_SOLVE, k > 0 ? 2 : 1);
+  }
+  span_end(p, sp, (double)p->n * (double)p->n);
+}
+
+int set_params(egs_problem* p, const double* theta) {
+  if (!theta) return EGS_ERR_INVALID;
+  MaternParams mp;
+  int rc = make_matern_params(theta, &mp);
+  if (rc != EGS_OK) {
+    set_last_error("theta outside the Matern domain (sigma2 > 0, beta > 0, nu > 0)", "make_matern_params");
+    return rc;
+  }
+  // The pinned mirror may still be read by an earlier in-flight copy.
+  EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  *p->hparams = mp;
+  EGS_CUDA_TRY(cudaMemcpyAsync(p->dparams, p->hparams, sizeof(MaternParams), cudaMemcpyHostToDevice, p->stream));
+  return EGS_OK;
+}
+
+int sync_flags(egs_problem* p, bool want_result) {
+  EGS_CUDA_TRY(cudaMemcpyAsync(p->hflags, p->flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+  if (want_result)
+    EGS_CUDA_TRY(cudaMemcpyAsync(p->hresult, p->result, 4 * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+  EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  collect_spans(p);
+  if (p->hflags[1] != 0) {
+    set_last_error("a device-side wait exceeded its limit", "tensor-core update");
+    return EGS_ERR_TIMEOUT;
+  }
+  if (p->hflags[0] > 0) {
+    set_last_error("Matrix is not positive definite", "potrf");
+    return p->hflags[0];
+  }
+  return EGS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int egs_version(void) { return 100; }
+
+const char* egs_status_string(int status) {
+  switch (status) {
+    case EGS_OK: return "ok";
+    case EGS_ERR_INVALID: return "invalid argument";
+    case EGS_ERR_CUDA: return "CUDA error";
+    case EGS_ERR_NO_DEVICE: return "no CUDA device";
+    case EGS_ERR_OOM: return "device allocation refused";
+    case EGS_ERR_TIMEOUT: return "device wait timed out";
+    case EGS_ERR_STATE: return "invalid call order";
+    default: return status > 0 ? "matrix is not positive definite" : "unknown status";
+  }
+}
+
+const char* egs_last_error(void) { return g_last_error.c_str(); }
+
+int egs_hardware_init(int device) {
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) {
+    cudaGetLastError();
+    set_last_error("no CUDA device visible", "egs_hardware_init");
+    return EGS_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= count) return EGS_ERR_INVALID;
+  EGS_CUDA_TRY(cudaSetDevice(device));
+  EGS_CUDA_TRY(cudaFree(nullptr));
+  return EGS_OK;
+}
+
+int egs_problem_create(egs_problem** out, int n, int dts) {
+  if (!out || n <= 0 || dts <= 0) return EGS_ERR_INVALID;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) {
+    cudaGetLastError();
+    set_last_error("no CUDA device visible", "egs_problem_create");
+    return EGS_ERR_NO_DEVICE;
+  }
+  auto* p = new egs_problem();
+  p->n = n;
+  p->dts = dts;
+  p->ts = round_tile(dts);
+  p->nt = (n + p->ts - 1) / p->ts;
+  p->np = p->nt * p->ts;
+  p->ntiles = lower_tiles(p->nt);
+  int rc = EGS_OK;
+  if ((rc = dev_alloc(&p->tiles, (size_t)p->ntiles * p->ts * p->ts, &p->bytes)) ||
+      (rc = dev_alloc(&p->x, p->np, &p->bytes)) || (rc = dev_alloc(&p->y, p->np, &p->bytes)) ||
+      (rc = dev_alloc(&p->z, p->np, &p->bytes)) || (rc = dev_alloc(&p->zcpy, p->np, &p->bytes)) ||
+      (rc = dev_alloc(&p->partial, p->nt, &p->bytes)) || (rc = dev_alloc(&p->result, 4, &p->bytes)) ||
+      (rc = dev_alloc(&p->flags, 2, &p->bytes)) || (rc = dev_alloc(&p->dparams, 1, &p->bytes))) {
+    free_problem(p);
+    return rc;
+  }
+  if (cudaMallocHost(&p->hparams, sizeof(MaternParams)) != cudaSuccess ||
+      cudaMallocHost(&p->hresult, 4 * sizeof(double)) != cudaSuccess ||
+      cudaMallocHost(&p->hflags, 2 * sizeof(int)) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    set_last_error("pinned host allocation or stream creation failed", "egs_problem_create");
+    free_problem(p);
+    return EGS_ERR_CUDA;
+  }
+  p->own_stream = true;
+  if ((rc = gemm_init_tensor_map(p->tmap, p->tiles, p->ts, p->ntiles)) != EGS_OK) {
+    free_problem(p);
+    return rc;
+  }
+  // Padding rows: zero locations and observations (the generator writes the identity there).
+  if (cudaMemsetAsync(p->x, 0, p->np * sizeof(double), p->stream) != cudaSuccess ||
+      cudaMemsetAsync(p->y, 0, p->np * sizeof(double), p->stream) != cudaSuccess ||
+      cudaMemsetAsync(p->zcpy, 0, p->np * sizeof(double), p->stream) != cudaSuccess ||
+      cudaMemsetAsync(p->z, 0, p->np * sizeof(double), p->stream) != cudaSuccess ||
+      cudaStreamSynchronize(p->stream) != cudaSuccess) {
+    cudaGetLastError();
+    free_problem(p);
+    return EGS_ERR_CUDA;
+  }
+  *out = p;
+  return EGS_OK;
+}
+
+int egs_problem_destroy(egs_problem* p) {
+  free_problem(p);
+  return EGS_OK;
+}
+
+int egs_problem_info(const egs_problem* p, int* n, int* ts, int* nt, long long* bytes) {
+  if (!p) return EGS_ERR_INVALID;
+  if (n) *n = p->n;
+  if (ts) *ts = p->ts;
+  if (nt) *nt = p->nt;
+  if (bytes) *bytes = p->bytes;
+  return EGS_OK;
+}
+
+int egs_problem_set_stream(egs_problem* p, void* cuda_stream) {
+  if (!p) return EGS_ERR_INVALID;
+  EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  if (p->own_stream) cudaStreamDestroy(p->stream);
+  if (cuda_stream) {
+    p->stream = (cudaStream_t)cuda_stream;
+    p->own_stream = false;
+  } else {
+    EGS_CUDA_TRY(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+    p->own_stream = true;
+  }
+  return EGS_OK;
+}
+
+static int set_locs(egs_problem* p, const double* x, const double* y, cudaMemcpyKind kind) {
+  if (!p || !x || !y) return EGS_ERR_INVALID;
+  EGS_CUDA_TRY(cudaMemcpyAsync(p->x, x, p->n * sizeof(double), kind, p->stream));
+  EGS_CUDA_TRY(cudaMemcpyAsync(p->y, y, p->n * sizeof(double), kind, p->stream));
+  EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  p->have_locations = true;
+  return EGS_OK;
+}
+
+int egs_problem_set_locations(egs_problem* p, const double* x, const double* y) {
+  return set_locs(p, x, y, cudaMemcpyHostToDevice);
+}
+int egs_problem_set_locations_device(egs_problem* p, const double* x, const double* y) {
+  return set_locs(p, x, y, cudaMemcpyDeviceToDevice);
+}
+
+static int set_obs(egs_problem* p, const double* z, cudaMemcpyKind kind) {
+  if (!p || !z) return EGS_ERR_INVALID;
+  EGS_CUDA_TRY(cudaMemcpyAsync(p->zcpy, z, p->n * sizeof(double), kind, p->stream));
+  EGS_CUDA_TRY(cudaMemcpyAsync(p->z, p->zcpy, p->np * sizeof(double), cudaMemcpyDeviceToDevice, p->stream));
+  EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  p->have_observations = true;
+  return EGS_OK;
+}
+
+int egs_problem_set_observations(egs_problem* p, const double* z) { return set_obs(p, z, cudaMemcpyHostToDevice); }
+int egs_problem_set_observations_device(egs_problem* p, const double* z) {
+  return set_obs(p, z, cudaMemcpyDeviceToDevice);
+}
+
+int egs_covariance_generate(egs_problem* p, const double* theta) {
+  if (!p) return EGS_ERR_INVALID;
+  if (!p->have_locations) return EGS_ERR_STATE;
+  int rc = set_params(p, theta);
+  if (rc != EGS_OK) return rc;
+  rc = launch_matern_tiles(p->tiles, p->x, p->y, p->n, p->ts, p->nt, p->dparams, p->stream);
+  if (rc != EGS_OK) return check_cuda("egs_covariance_generate");
+  EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  return EGS_OK;
+}
+
+int egs_potrf(egs_problem* p) {
+  if (!p) return EGS_ERR_INVALID;
+  EGS_CUDA_TRY(cudaMemsetAsync(p->flags, 0, 2 * sizeof(int), p->stream));
+  int rc = enqueue_potrf(p);
+  if (rc != EGS_OK) return rc;
+  return sync_flags(p, false);
+}
+
+int egs_restore_observations(egs_problem* p) {
+  if (!p) return EGS_ERR_INVALID;
+  if (!p->have_observations) return EGS_ERR_STATE;
+  EGS_CUDA_TRY(cudaMemcpyAsync(p->z, p->zcpy, p->np * sizeof(double), cudaMemcpyDeviceToDevice, p->stream));
+  EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  return EGS_OK;
+}
+
+int egs_trsv(egs_problem* p) {
+  if (!p) return EGS_ERR_INVALID;
+  enqueue_trsv(p);
+  int rc = check_cuda("egs_trsv");
+  if (rc != EGS_OK) return rc;
+  EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  return EGS_OK;
+}
+
+int egs_loglik_parts(egs_problem* p, double* loglik, double* logdet, double* dot) {
+  if (!p) return EGS_ERR_INVALID;
+  launch_logdet_partials(p->tiles, p->ts, p->nt, p->n, p->partial, p->stream);
+  launch_finalize(p->partial, p->nt, p->z, p->n, p->result, nullptr, p->stream);
+  int rc = check_cuda("egs_loglik_parts");
+  if (rc != EGS_OK) return rc;
+  EGS_CUDA_TRY(cudaMemcpyAsync(p->hresult, p->result, 4 * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+  EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  if (loglik) *loglik = p->hresult[0];
+  if (logdet) *logdet = p->hresult[1];
+  if (dot) *dot = p->hresult[2];
+  return EGS_OK;
+}
+
+int egs_get_tile(egs_problem* p, int i, int j, double* host_out) {
+  if (!p || !host_out || i < j || i >= p->nt || j < 0) return EGS_ERR_INVALID;
+  const size_t ts2 = (size_t)p->ts * p->ts;
+  EGS_CUDA_TRY(cudaMemcpyAsync(host_out, p->tiles + tile_slot(i, j, p->nt) * ts2, ts2 * sizeof(double),
+                               cudaMemcpyDeviceToHost, p->stream));
+  EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  return EGS_OK;
+}
+
+int egs_get_observations(egs_problem* p, double* host_z) {
+  if (!p || !host_z) return EGS_ERR_INVALID;
+  EGS_CUDA_TRY(cudaMemcpyAsync(host_z, p->z, p->n * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+  EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  return EGS_OK;
+}
+
+int egs_mle_eval(egs_problem* p, const double* theta, double* loglik, double* logdet, double* dot) {
+  if (!p || !loglik) return EGS_ERR_INVALID;
+  if (!p->have_locations || !p->have_observations) return EGS_ERR_STATE;
+  int rc = set_params(p, theta);
+  if (rc != EGS_OK) return rc;
+  cudaStream_t st = p->stream;
+  EGS_CUDA_TRY(cudaMemsetAsync(p->flags, 0, 2 * sizeof(int), st));
+  EGS_CUDA_TRY(cudaMemcpyAsync(p->z, p->zcpy, p->np * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  int sp = span_begin(p, EGS_STAGE_GENERATE);
+  rc = launch_matern_tiles(p->tiles, p->x, p->y, p->n, p->ts, p->nt, p->dparams, st);
+  if (rc != EGS_OK) return check_cuda("matern");
+  count_launches(p, EGS_STAGE_GENERATE, (lower_tiles(p->nt) + 65534) / 65535);
+  span_end(p, sp, 0.0);
+  rc = enqueue_potrf(p);
+  if (rc != EGS_OK) return rc;
+  sp = span_begin(p, EGS_STAGE_REDUCE);
+  launch_logdet_partials(p->tiles, p->ts, p->nt, p->n, p->partial, st);
+  span_end(p, sp, 0.0);
+  count_launches(p, EGS_STAGE_REDUCE, 1);
+  enqueue_trsv(p);
+  sp = span_begin(p, EGS_STAGE_REDUCE);
+  launch_finalize(p->partial, p->nt, p->z, p->n, p->result, p->flags, st);
+  span_end(p, sp, 0.0);
+  count_launches(p, EGS_STAGE_REDUCE, 1);
+  rc = check_cuda("egs_mle_eval");
+  if (rc != EGS_OK) return rc;
+  rc = sync_flags(p, true);
+  if (rc != EGS_OK) return rc;
+  *loglik = p->hresult[0];
+  if (logdet) *logdet = p->hresult[1];
+  if (dot) *dot = p->hresult[2];
+  return EGS_OK;
+}
+
+int egs_generate_observations(egs_problem* p, const double* theta, int seed, double* z_out) {
+  if (!p || !theta || seed < 0 || seed > 4095) return EGS_ERR_INVALID;
+  if (!p->have_locations) return EGS_ERR_STATE;
+  if (lower_tiles(p->nt) > 65535) return EGS_ERR_INVALID;
+  std::vector<double> e(p->np, 0.0);
+  const int iseed[4] = {seed, seed, seed, 1};
+  int rc = egs_dlarnv_normal(iseed, p->n, e.data());
+  if (rc != EGS_OK) return rc;
+  EGS_CUDA_TRY(cudaMemcpyAsync(p->z, e.data(), p->np * sizeof(double), cudaMemcpyHostToDevice, p->stream));
+  if ((rc = egs_covariance_generate(p, theta)) != EGS_OK) return rc;
+  if ((rc = egs_potrf(p)) != EGS_OK) return rc;
+  double* part = nullptr;
+  long long dummy = 0;
+  if ((rc = dev_alloc(&part, (size_t)p->ntiles * p->ts, &dummy)) != EGS_OK) return rc;
+  launch_trmv(p->tiles, p->ts, p->nt, p->z, part, p->zcpy, p->stream);
+  cudaMemcpyAsync(p->z, p->zcpy, p->np * sizeof(double), cudaMemcpyDeviceToDevice, p->stream);
+  if (z_out) cudaMemcpyAsync(z_out, p->zcpy, p->n * sizeof(double), cudaMemcpyDeviceToHost, p->stream);
+  rc = check_cuda("egs_generate_observations");
+  cudaStreamSynchronize(p->stream);
+  cudaFree(part);
+  if (rc != EGS_OK) return rc;
+  p->have_observations = true;
+  return EGS_OK;
+}
+
+int egs_problem_set_profiling(egs_problem* p, int enable) {
+  if (!p) return EGS_ERR_INVALID;
+  EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  collect_spans(p);
+  p->profiling = enable != 0;
+  for (int i = 0; i < EGS_NUM_STAGES; ++i) {
+    p->stage_ms[i] = 0.0;
+    p->stage_flops[i] = 0.0;
+    p->stage_launches[i] = 0;
+  }
+  return EGS_OK;
+}
+
+int egs_problem_stage_stats(egs_problem* p, double* ms, double* flops, long long* launches) {
+  if (!p) return EGS_ERR_INVALID;
+  for (int i = 0; i < EGS_NUM_STAGES; ++i) {
+    if (ms) ms[i] = p->stage_ms[i];
+    if (flops) flops[i] = p->stage_flops[i];
+    if (launches) launches[i] = p->stage_launches[i];
+  }
+  return EGS_OK;
+}
+
+int egs_matern_block(double* a, int lda, int rows, int cols, const double* x1, const double* y1, const double* x2,
+                     const double* y2, const double* theta, int distance_metric, void* cuda_stream) {
+  if (!a || !x1 || !y1 || !x2 || !y2 || !theta || rows < 0 || cols < 0 || lda < rows) return EGS_ERR_INVALID;
+  if (distance_metric != 0) {
+    set_last_error("only the Euclidean distance (metric 0) is on the device path", "egs_matern_block");
+    return EGS_ERR_INVALID;
+  }
+  MaternParams mp;
+  int rc = make_matern_params(theta, &mp);
+  if (rc != EGS_OK) return rc;
+  rc = launch_matern_block(a, lda, rows, cols, x1, y1, x2, y2, mp, (cudaStream_t)cuda_stream);
+  if (rc != EGS_OK) return check_cuda("egs_matern_block");
+  return EGS_OK;
+}
+
+namespace {
+struct CachedProblem {
+  std::unique_ptr<egs_problem, int (*)(egs_problem*)> p{nullptr, egs_problem_destroy};
+  int n = 0, dts = 0;
+};
+thread_local CachedProblem g_cached;
+}  // namespace
+
+int egs_mle_loglik_host(int n, int dts, const double* x, const double* y, const double* z, const double* theta,
+                        double* loglik) {
+  if (n <= 0 || dts <= 0 || !x || !y || !z || !theta || !loglik) return EGS_ERR_INVALID;
+  if (!g_cached.p || g_cached.n != n || g_cached.dts != dts) {
+    g_cached.p.reset();
+    egs_problem* p = nullptr;
+    int rc = egs_problem_create(&p, n, dts);
+    if (rc != EGS_OK) return rc;
+    g_cached.p.reset(p);
+    g_cached.n = n;
+    g_cached.dts = dts;
+  }
+  egs_problem* p = g_cached.p.get();
+  int rc = egs_problem_set_locations(p, x, y);
+  if (rc != EGS_OK) return rc;
+  rc = egs_problem_set_observations(p, z);
+  if (rc != EGS_OK) return rc;
+  return egs_mle_eval(p, theta, loglik, nullptr, nullptr);
+}
+
+int egs_predict_host(int n_obs, int n_miss, int dts, const double* x_obs, const double* y_obs, const double* z_obs,
+                     const double* x_miss, const double* y_miss, const double* z_actual, const double* theta,
+                     double* z_miss, double* mspe) {
+  if (n_obs <= 0 || n_miss <= 0 || dts <= 0 || !x_obs || !y_obs || !z_obs || !x_miss || !y_miss || !theta ||
+      !z_miss || !mspe)
+    return EGS_ERR_INVALID;
+  egs_problem* p = nullptr;
+  int rc = egs_problem_create(&p, n_obs, dts);
+  if (rc != EGS_OK) return rc;
+  std::unique_ptr<egs_problem, int (*)(egs_problem*)> guard(p, egs_problem_destroy);
+  if ((rc = egs_problem_set_locations(p, x_obs, y_obs)) != EGS_OK) return rc;
+  if ((rc = egs_problem_set_observations(p, z_obs)) != EGS_OK) return rc;
+  if ((rc = egs_covariance_generate(p, theta)) != EGS_OK) return rc;
+  if ((rc = egs_potrf(p)) != EGS_OK) return rc;
+  // dposv: w = C22^-1 Zobs (LinearAlgebraMethods.cpp:544)
+  enqueue_trsv(p);
+  enqueue_trsv_t(p);
+  if ((rc = check_cuda("egs_predict_host/posv")) != EGS_OK) return rc;
+  // C12^T (obs x miss) and Zmiss = C12 w (:535, :552)
+  double *c12t = nullptr, *dxm = nullptr, *dym = nullptr, *dzm = nullptr, *dza = nullptr, *dsum = nullptr;
+  long long dummy = 0;
+  auto cleanup = [&]() {
+    cudaStreamSynchronize(p->stream);
+    cudaFree(c12t);
+    cudaFree(dxm);
+    cudaFree(dym);
+    cudaFree(dzm);
+    cudaFree(dza);
+    cudaFree(dsum);
+  };
+  if ((rc = dev_alloc(&c12t, (size_t)n_obs * n_miss, &dummy)) || (rc = dev_alloc(&dxm, n_miss, &dummy)) ||
+      (rc = dev_alloc(&dym, n_miss, &dummy)) || (rc = dev_alloc(&dzm, n_miss, &dummy)) ||
+      (rc = dev_alloc(&dza, n_miss, &dummy)) || (rc = dev_alloc(&dsum, 1, &dummy))) {
+    cleanup();
+    return rc;
+  }
+  cudaStream_t st = p->stream;
+  if (cudaMemcpyAsync(dxm, x_miss, n_miss * sizeof(double), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaMemcpyAsync(dym, y_miss, n_miss * sizeof(double), cudaMemcpyHostToDevice, st) != cudaSuccess) {
+    cleanup();
+    return EGS_ERR_CUDA;
+  }
+  MaternParams mp;
+  make_matern_params(theta, &mp);
+  launch_matern_block(c12t, n_obs, n_obs, n_miss, p->x, p->y, dxm, dym, mp, st);
+  launch_gemv_t_block(c12t, n_obs, n_obs, n_miss, p->z, dzm, st);
+  double sum = -1.0;
+  if (z_actual) {
+    cudaMemcpyAsync(dza, z_actual, n_miss * sizeof(double), cudaMemcpyHostToDevice, st);
+    launch_sumsq_diff(dza, dzm, n_miss, dsum, st);
+    cudaMemcpyAsync(&sum, dsum, sizeof(double), cudaMemcpyDeviceToHost, st);
+  }
+  cudaMemcpyAsync(z_miss, dzm, n_miss * sizeof(double), cudaMemcpyDeviceToHost, st);
+  if ((rc = check_cuda("egs_predict_host")) != EGS_OK) {
+    cleanup();
+    return rc;
+  }
+  if (cudaStreamSynchronize(st) != cudaSuccess) {
+    cleanup();
+    return check_cuda("egs_predict_host/sync");
+  }
+  *mspe = z_actual ? sum / n_miss : -1.0;
+  cleanup();
+  return EGS_OK;
+}
+
+}  // extern "C"

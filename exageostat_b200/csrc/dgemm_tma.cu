@@ -1,0 +1,449 @@
+// FP64 tensor-core update  C := C - A * B^T  on the tile-major lower storage,
+// fed by TMA, for sm_100a.
+//
+// This is the trailing syrk/gemm of the tiled Cholesky (the N^3/3 part of
+// CHAMELEON_dpotrf_Tile, ChameleonDense.cpp:25-37) and, with K = 64, the
+// updates inside the panel factorisation and the panel triangular solve.
+//
+// Geometry.  Every operand row is a *global* matrix row g in [0, Np); its data
+// lives in tile row g / ts at local row g % ts.  A and B take their K columns
+// from one tile column (a_tcol / b_tcol) starting at a local column offset; C is
+// addressed element by element through (global row, global column) and
+// elements of upper tiles are never written.  Because ts is a multiple of 64,
+// a 16-row TMA box never straddles two tiles, so a 128 x 128 CTA tile may span
+// tile boundaries and no MMA work is wasted when 128 does not divide ts.
+//
+// Pipeline.  Thread 0 issues 3-D TMA loads (rows x cols x tile-slot), running up
+// to five stages ahead, into a 6-stage ring of 128B-swizzled shared-memory
+// stages guarded by mbarriers; eight warps each own a 64 x 32 sub-tile and run
+// mma.sync m16n8k16 .f64 (the FP64 tensor path of sm_100a).  The 16 rows of an
+// MMA fragment are mapped to tile rows through fixed permutations chosen so
+// that every fragment load is free of shared-memory bank conflicts under the
+// 128-byte swizzle (A: 16-byte loads of row pairs; B: 8-byte loads).
+//
+// Every wait is bounded: a thread that polls longer than the limit records an
+// error in *err and leaves; the host turns that into EGS_ERR_TIMEOUT.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cstdint>
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace egs {
+
+namespace gemm {
+constexpr int BM = 128, BN = 128, BK = 16, STAGES = 6;
+constexpr int CONSUMER_WARPS = 8;
+constexpr int THREADS = CONSUMER_WARPS * 32;   // thread 0 also issues the TMA loads
+constexpr int BOX_ROWS = 16;                          // 16 doubles = one 128-byte swizzle row
+constexpr int BOX_BYTES = BOX_ROWS * BK * 8;          // 2 KB
+constexpr int A_STAGE_BYTES = (BM / BOX_ROWS) * BOX_BYTES;
+constexpr int B_STAGE_BYTES = (BN / BOX_ROWS) * BOX_BYTES;
+constexpr int STAGE_BYTES = A_STAGE_BYTES + B_STAGE_BYTES;
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 2 * STAGES * 8 + 1024;
+constexpr int GROUP = 8;                              // block-columns per raster group
+}  // namespace gemm
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Bounded wait: gives up after kSpinLimit polls or about two seconds.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
+  long long n = 0;
+  uint64_t t0 = 0;
+  while (!mbar_try_wait(bar, parity)) {
+    ++n;
+    if ((n & 1023) == 0) {
+      const uint64_t now = global_ns();
+      if (t0 == 0) {
+        t0 = now;
+      } else if (now - t0 > 2000000000ull) {
+        atomicOr(err, 1);
+        return false;
+      }
+    }
+    if (n > kSpinLimit) {
+      atomicOr(err, 1);
+      return false;
+    }
+  }
+  return true;
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y,
+                                            int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_u32(dst)),
+      "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void dmma_16816(double (&d)[4], const double (&a)[8], const double (&b)[4]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+      "{%12,%13,%14,%15}, {%0,%1,%2,%3};"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]),
+        "d"(b[1]), "d"(b[2]), "d"(b[3]));
+}
+
+// MMA row g (0..7) of an A fragment -> tile row 2*perm[g] within a 16-row box;
+// row g+8 -> the next row, so (a_2j, a_2j+1) is one 16-byte load.
+__device__ __forceinline__ int perm_a(int g) { return ((g & 1) << 2) | (g >> 1); }
+// MMA row r (0..15) of a B fragment (the n index) -> tile row within a 16-row box.
+__device__ __forceinline__ int perm_b(int r) {
+  return (r & 1) | (((r >> 2) & 1) << 1) | (((r >> 1) & 1) << 3) | (((r >> 3) & 1) << 2);
+}
+
+struct GemmDesc {
+  int M, N, K;
+  int a_row0, a_col0, a_tcol;
+  int b_row0, b_col0, b_tcol;
+  int c_row0, c_col0;
+  int lower;
+  int MB, NB;
+  long long total;
+  int ts, nt, np;
+};
+
+// Raster: groups of GROUP block-columns; inside a group, block-rows outer,
+// block-columns inner, so a group's B panel stays in L2 while A streams once.
+__device__ __forceinline__ bool decode_block(long long L, const GemmDesc& d, int& mb, int& nb) {
+  for (int nb0 = 0; nb0 < d.NB; nb0 += gemm::GROUP) {
+    const int ge = min(gemm::GROUP, d.NB - nb0);
+    const int mstart = d.lower ? nb0 : 0;
+    const long long cnt = (long long)ge * (d.MB - mstart);
+    if (L < cnt) {
+      mb = mstart + (int)(L / ge);
+      nb = nb0 + (int)(L % ge);
+      return true;
+    }
+    L -= cnt;
+  }
+  return false;
+}
+
+// Producer cursor: walks the same (block, k-step) sequence as the consumers,
+// running up to STAGES-1 stages ahead of them.
+struct Cursor {
+  long long L;
+  int kt, m0, n0;
+  bool valid;
+};
+
+__device__ __forceinline__ void cursor_seek(Cursor& c, const GemmDesc& d) {
+  while (c.L < d.total) {
+    int mb, nb;
+    decode_block(c.L, d, mb, nb);
+    if (!(d.lower && mb < nb)) {
+      c.m0 = mb * gemm::BM;
+      c.n0 = nb * gemm::BN;
+      c.valid = true;
+      return;
+    }
+    c.L += gridDim.x;
+  }
+  c.valid = false;
+}
+
+__device__ __forceinline__ void issue_stage(const CUtensorMap* tmap, uint8_t* smem, uint64_t* full, uint32_t s,
+                                            const Cursor& c, const GemmDesc& d) {
+  using namespace gemm;
+  mbar_expect_tx(&full[s], STAGE_BYTES);
+  uint8_t* sa = smem + s * STAGE_BYTES;
+  uint8_t* sb = sa + A_STAGE_BYTES;
+  const int kcol = c.kt * BK;
+#pragma unroll
+  for (int b = 0; b < BM / BOX_ROWS; ++b) {
+    const int g = d.a_row0 + c.m0 + b * BOX_ROWS;
+    int x = d.ts, z = 0;  // fully out of bounds -> zero fill
+    if (g < d.np) {
+      const int ti = g / d.ts;
+      x = g - ti * d.ts;
+      z = (int)tile_slot(ti, d.a_tcol, d.nt);
+    }
+    tma_load_3d(sa + b * BOX_BYTES, tmap, &full[s], x, d.a_col0 + kcol, z);
+  }
+#pragma unroll
+  for (int b = 0; b < BN / BOX_ROWS; ++b) {
+    const int g = d.b_row0 + c.n0 + b * BOX_ROWS;
+    int x = d.ts, z = 0;
+    if (g < d.np) {
+      const int ti = g / d.ts;
+      x = g - ti * d.ts;
+      z = (int)tile_slot(ti, d.b_tcol, d.nt);
+    }
+    tma_load_3d(sb + b * BOX_BYTES, tmap, &full[s], x, d.b_col0 + kcol, z);
+  }
+}
+
+__global__ void __launch_bounds__(gemm::THREADS, 1)
+dgemm_update_kernel(const __grid_constant__ CUtensorMap tmap, double* __restrict__ tiles, GemmDesc d,
+                    int* __restrict__ err) {
+  using namespace gemm;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
+  uint64_t* empty = full + STAGES;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const bool producer = threadIdx.x == 0;
+  const int ksteps = d.K / BK;
+  if (producer) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], CONSUMER_WARPS);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&tmap) : "memory");
+  }
+  __syncthreads();
+
+  // Producer state (meaningful in thread 0 only).
+  Cursor cur;
+  cur.L = blockIdx.x;
+  cur.kt = 0;
+  cur.valid = false;
+  uint32_t issued = 0;
+  bool alive = true;
+  if (producer) cursor_seek(cur, d);
+  auto top_up = [&](uint32_t consumed) {
+    // Keep up to STAGES-1 stages in flight ahead of the consumers.
+    while (alive && cur.valid && issued < consumed + STAGES - 1) {
+      const uint32_t s = issued % STAGES, ph = (issued / STAGES) & 1;
+      if (!mbar_wait(&empty[s], ph ^ 1, err)) {
+        alive = false;
+        break;
+      }
+      issue_stage(&tmap, smem, full, s, cur, d);
+      ++issued;
+      if (++cur.kt == ksteps) {
+        cur.kt = 0;
+        cur.L += gridDim.x;
+        cursor_seek(cur, d);
+      }
+    }
+  };
+
+  const int g = lane >> 2, t = lane & 3;
+  const int wm = warp & 1, wn = warp >> 1;  // warp sub-tile: rows wm*64.., cols wn*32..
+  const int pa = perm_a(g);
+  const int row_in_box = 2 * pa;  // accumulator rows row_in_box, row_in_box + 1
+
+  uint32_t it = 0;
+  bool ok = true;
+  for (long long L = blockIdx.x; L < d.total && ok; L += gridDim.x) {
+    int mb, nb;
+    decode_block(L, d, mb, nb);
+    if (d.lower && mb < nb) continue;
+    double acc[4][4][4];
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[mi][ni][q] = 0.0;
+
+    for (int kt = 0; kt < ksteps; ++kt, ++it) {
+      if (producer) top_up(it);
+      __syncwarp();
+      const uint32_t s = it % STAGES, ph = (it / STAGES) & 1;
+      if (!mbar_wait(&full[s], ph, err)) {
+        ok = false;
+        break;
+      }
+      __syncwarp();
+      const uint8_t* sa = smem + s * STAGE_BYTES;
+      const uint8_t* sb = sa + A_STAGE_BYTES;
+      double bf[4][4];
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni) {
+        const uint8_t* box = sb + (wn * 2 + (ni >> 1)) * BOX_BYTES;
+        const int fb = perm_b(g + 8 * (ni & 1));
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const int k = t + 4 * i;
+          bf[ni][i] = *reinterpret_cast<const double*>(box + k * 128 + (((fb >> 1) ^ (k & 7)) << 4) +
+                                                      ((fb & 1) << 3));
+        }
+      }
+#pragma unroll
+      for (int mi = 0; mi < 4; ++mi) {
+        const uint8_t* box = sa + (wm * 4 + mi) * BOX_BYTES;
+        double af[8];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int k = t + 4 * j;
+          const double2 v = *reinterpret_cast<const double2*>(box + k * 128 + ((pa ^ (k & 7)) << 4));
+          af[2 * j] = v.x;
+          af[2 * j + 1] = v.y;
+        }
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) dmma_16816(acc[mi][ni], af, bf[ni]);
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[s]);
+    }
+    if (!ok) break;
+
+    // Epilogue: C -= acc; element pairs (row, row+1) are contiguous in a column.
+    const int ts = d.ts;
+#pragma unroll
+    for (int ni = 0; ni < 4; ++ni) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int nl = nb * BN + wn * 32 + (ni >> 1) * 16 + perm_b(2 * t + 8 * (ni & 1)) + h;
+        if (nl >= d.N) continue;
+        const int gj = d.c_col0 + nl;
+        const int tj = gj / ts, lc = gj - tj * ts;
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi) {
+          const int ml = mb * BM + wm * 64 + mi * 16 + row_in_box;
+          if (ml >= d.M) continue;
+          const int gi = d.c_row0 + ml;
+          const int ti = gi / ts, lr = gi - ti * ts;
+          if (ti < tj) continue;
+          double2* p = reinterpret_cast<double2*>(tiles + tile_slot(ti, tj, d.nt) * (long long)ts * ts +
+                                                  (long long)lc * ts + lr);
+          double2 v = *p;
+          v.x -= acc[mi][ni][h];
+          v.y -= acc[mi][ni][2 + h];
+          *p = v;
+        }
+      }
+    }
+  }
+  // Drain: every stage this CTA issued must have landed before it exits.
+  if (producer) {
+    for (uint32_t j = (issued > (uint32_t)STAGES ? issued - STAGES : 0); j < issued; ++j)
+      mbar_wait(&full[j % STAGES], (j / STAGES) & 1, err);
+  }
+}
+
+static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+
+int gemm_init_tensor_map(void* tmap_storage, double* tiles, int ts, long long ntiles) {
+  if (!g_encode) {
+    cudaDriverEntryPointQueryResult q;
+    void* fn = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn) {
+      set_last_error("cuTensorMapEncodeTiled unavailable", "gemm_init_tensor_map");
+      return EGS_ERR_CUDA;
+    }
+    g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }
+  if (ts % 64 != 0 || ((uintptr_t)tiles & 15) != 0) return EGS_ERR_INVALID;
+  cuuint64_t dims[3] = {(cuuint64_t)ts, (cuuint64_t)ts, (cuuint64_t)ntiles};
+  cuuint64_t strides[2] = {(cuuint64_t)ts * 8, (cuuint64_t)ts * ts * 8};
+  cuuint32_t box[3] = {gemm::BOX_ROWS, gemm::BK, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = g_encode(reinterpret_cast<CUtensorMap*>(tmap_storage), CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, tiles,
+                        dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_last_error("cuTensorMapEncodeTiled failed", "gemm_init_tensor_map");
+    return EGS_ERR_CUDA;
+  }
+  return EGS_OK;
+}
+
+static int g_num_sms = 0;
+int gemm_num_sms() {
+  if (g_num_sms == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g_num_sms <= 0) g_num_sms = 148;
+  }
+  return g_num_sms;
+}
+
+static int launch_desc(const void* tmap, double* tiles, GemmDesc& d, int* err, cudaStream_t st) {
+  using namespace gemm;
+  if (d.M <= 0 || d.N <= 0 || d.K <= 0) return EGS_OK;
+  if (d.K % BK != 0) return EGS_ERR_INVALID;
+  d.MB = (d.M + BM - 1) / BM;
+  d.NB = (d.N + BN - 1) / BN;
+  long long total = 0;
+  for (int nb0 = 0; nb0 < d.NB; nb0 += GROUP) {
+    const int ge = (d.NB - nb0) < GROUP ? (d.NB - nb0) : GROUP;
+    total += (long long)ge * (d.MB - (d.lower ? nb0 : 0));
+  }
+  d.total = total;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(dgemm_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    attr_set = true;
+  }
+  const long long grid = total < gemm_num_sms() ? total : gemm_num_sms();
+  dgemm_update_kernel<<<(unsigned)grid, THREADS, SMEM_BYTES, st>>>(*reinterpret_cast<const CUtensorMap*>(tmap),
+                                                                    tiles, d, err);
+  return cudaGetLastError() == cudaSuccess ? EGS_OK : EGS_ERR_CUDA;
+}
+
+// Trailing update of step k: C(i, j) -= L(i, k) L(j, k)^T for all k < j <= i.
+int launch_gemm_trailing(const void* tmap, double* tiles, int ts, int nt, int k, int* err, cudaStream_t st) {
+  GemmDesc d{};
+  d.ts = ts;
+  d.nt = nt;
+  d.np = nt * ts;
+  const int r0 = (k + 1) * ts;
+  d.M = d.N = d.np - r0;
+  d.K = ts;
+  d.a_row0 = d.b_row0 = d.c_row0 = d.c_col0 = r0;
+  d.a_col0 = d.b_col0 = 0;
+  d.a_tcol = d.b_tcol = k;
+  d.lower = 1;
+  return launch_desc(tmap, tiles, d, err, st);
+}
+
+// General form used by the panel factorisation (see kernels.cuh).
+int launch_gemm_rows(const void* tmap, double* tiles, int ts, int nt, int M, int N, int K, int a_row0,
+                     int a_col0, int a_tcol, int b_row0, int b_col0, int b_tcol, int c_row0, int c_col0,
+                     int lower, int* err, cudaStream_t st) {
+  GemmDesc d{};
+  d.ts = ts;
+  d.nt = nt;
+  d.np = nt * ts;
+  d.M = M;
+  d.N = N;
+  d.K = K;
+  d.a_row0 = a_row0;
+  d.a_col0 = a_col0;
+  d.a_tcol = a_tcol;
+  d.b_row0 = b_row0;
+  d.b_col0 = b_col0;
+  d.b_tcol = b_tcol;
+  d.c_row0 = c_row0;
+  d.c_col0 = c_col0;
+  d.lower = lower;
+  return launch_desc(tmap, tiles, d, err, st);
+}
+
+}  // namespace egs

@@ -1,0 +1,41 @@
+// Launch helpers shared by the translation units of the B200 path.
+#pragma once
+#include <cuda_runtime.h>
+#include "common.cuh"
+#include "bessel_k.cuh"
+
+namespace egs {
+
+int make_matern_params(const double* theta, MaternParams* out);
+int launch_matern_tiles(double* tiles, const double* x, const double* y, int n, int ts, int nt,
+                        const MaternParams* dparams, cudaStream_t st);
+int launch_matern_block(double* a, int lda, int rows, int cols, const double* x1, const double* y1,
+                        const double* x2, const double* y2, const MaternParams& p, cudaStream_t st);
+
+// Factorisation building blocks (potrf.cu).  All offsets are element offsets
+// inside a tile; tiles are addressed by lower-tile slot.
+void launch_potrf_diag_block(double* tiles, int ts, long long slot, int off, int col_base, int* info,
+                             cudaStream_t st);
+void launch_trsm_rows(double* tiles, int ts, long long slot0, int ntiles, int row0, int col0,
+                      long long lslot, cudaStream_t st);
+void launch_trsv_diag(const double* tiles, int ts, long long slot, double* zk, cudaStream_t st);
+void launch_gemv_panel(const double* tiles, int ts, int nt, int k, double* z, cudaStream_t st);
+void launch_trsv_t_diag(const double* tiles, int ts, long long slot, double* zk, cudaStream_t st);
+void launch_gemv_t_panel(const double* tiles, int ts, int nt, int k, double* z, cudaStream_t st);
+void launch_logdet_partials(const double* tiles, int ts, int nt, int n, double* partial, cudaStream_t st);
+void launch_finalize(const double* partial, int nt, const double* z, int n, double* result,
+                     const int* info, cudaStream_t st);
+void launch_sumsq_diff(const double* a, const double* b, int n, double* out, cudaStream_t st);
+void launch_trmv(const double* tiles, int ts, int nt, const double* e, double* part, double* z, cudaStream_t st);
+void launch_gemv_t_block(const double* a, long long lda, int rows, int cols, const double* w, double* out,
+                         cudaStream_t st);
+
+// FP64 tensor-core update C -= A * B^T over global row indices (dgemm_tma.cu).
+int gemm_init_tensor_map(void* tmap_storage, double* tiles, int ts, long long ntiles);
+int launch_gemm_trailing(const void* tmap, double* tiles, int ts, int nt, int k, int* err, cudaStream_t st);
+int launch_gemm_rows(const void* tmap, double* tiles, int ts, int nt, int M, int N, int K, int a_row0,
+                     int a_col0, int a_tcol, int b_row0, int b_col0, int b_tcol, int c_row0, int c_col0,
+                     int lower, int* err, cudaStream_t st);
+int gemm_num_sms();
+
+}  // namespace egs

@@ -1,0 +1,425 @@
+// Panel-level building blocks of the tiled Cholesky path on sm_100a: the 64x64
+// diagonal-block factorisation, the row-parallel triangular solve of a 64-column
+// block, the single right-hand-side forward/backward substitution over tiles,
+// and the deterministic reductions that turn the factor into the log-likelihood.
+//
+// Reference counterparts:
+//   CHAMELEON_dpotrf_Tile            ChameleonDense.cpp:25-37   (panel part; the trailing
+//                                                                update is dgemm_tma.cu)
+//   CHAMELEON_dtrsm_Tile (Z := L^-1 Z) ChameleonImplementation.cpp:337-347
+//   DMDETCodelet::core_dmdet          dmdet-codelet.cpp:73-80   (sum of log L_kk, L_kk > 0)
+//   DDOTPCodelet::cl_ddotp_function   ddotp-codelet.cpp:63-72   (Z^T Z)
+//   log-likelihood assembly           ChameleonImplementation.cpp:257-265
+//   DMSECodelet                       dmse-codelet.cpp:60-73    (sum (zhat - z)^2)
+// Every reduction uses a fixed summation order, so a result does not depend on
+// what else runs on the GPU.
+#include <cmath>
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace egs {
+
+constexpr int kNB = 64;  // inner block width of the panel factorisation
+
+// ---------------------------------------------------------------------------
+// Unblocked Cholesky of the 64x64 diagonal block at (off, off) of one tile.
+// info records the 1-based global column of the first non-positive pivot.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+potrf_diag_block_kernel(double* __restrict__ tiles, int ts, long long slot, int off, int col_base,
+                        int* __restrict__ info) {
+  __shared__ double S[kNB][kNB + 1];
+  double* T = tiles + slot * (long long)ts * ts;
+  const int tid = threadIdx.x;
+  for (int e = tid; e < kNB * kNB; e += blockDim.x) {
+    const int r = e % kNB, c = e / kNB;
+    if (r >= c) S[r][c] = T[(long long)(off + c) * ts + off + r];
+  }
+  __syncthreads();
+  const int r = tid % kNB;
+  const int cg = tid / kNB;  // 4 column groups
+  for (int j = 0; j < kNB; ++j) {
+    const double d = S[j][j];
+    const double ljj = sqrt(d);
+    const double inv = 1.0 / ljj;
+    __syncthreads();
+    if (tid > j && tid < kNB) S[tid][j] *= inv;
+    if (tid == 0) {
+      S[j][j] = ljj;
+      if (!(d > 0.0)) atomicCAS(info, 0, col_base + off + j + 1);
+    }
+    __syncthreads();
+    for (int c = j + 1 + cg; c <= r; c += 4) S[r][c] = fma(-S[r][j], S[c][j], S[r][c]);
+    __syncthreads();
+  }
+  for (int e = tid; e < kNB * kNB; e += blockDim.x) {
+    const int rr = e % kNB, c = e / kNB;
+    if (rr >= c) T[(long long)(off + c) * ts + off + rr] = S[rr][c];
+  }
+}
+
+void launch_potrf_diag_block(double* tiles, int ts, long long slot, int off, int col_base, int* info,
+                             cudaStream_t st) {
+  potrf_diag_block_kernel<<<1, 256, 0, st>>>(tiles, ts, slot, off, col_base, info);
+}
+
+// ---------------------------------------------------------------------------
+// X := A * L^-T for the 64-column block [col0, col0+64) of rows [row0, ts) of
+// ntiles consecutive tiles starting at slot0; L is the factored 64x64 diagonal
+// block at (col0, col0) of tile lslot.  One thread per row, L broadcast from
+// shared memory.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128)
+trsm_rows_kernel(double* __restrict__ tiles, int ts, long long slot0, int row0, int col0,
+                 long long lslot) {
+  __shared__ __align__(16) double L[kNB][kNB];
+  __shared__ double invd[kNB];
+  const double* TL = tiles + lslot * (long long)ts * ts;
+  for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
+    const int rr = e % kNB, c = e / kNB;
+    L[rr][c] = (rr >= c) ? TL[(long long)(col0 + c) * ts + col0 + rr] : 0.0;
+  }
+  __syncthreads();
+  if (threadIdx.x < kNB) invd[threadIdx.x] = 1.0 / L[threadIdx.x][threadIdx.x];
+  __syncthreads();
+  const int row = row0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= ts) return;
+  double* A = tiles + (slot0 + blockIdx.y) * (long long)ts * ts + (long long)col0 * ts + row;
+  double x[kNB];
+#pragma unroll
+  for (int c = 0; c < kNB; ++c) x[c] = A[(long long)c * ts];
+#pragma unroll
+  for (int c = 0; c < kNB; ++c) {
+    double s = x[c];
+#pragma unroll
+    for (int q = 0; q < c; q += 2) {
+      if (q + 1 < c) {
+        const double2 l2 = *reinterpret_cast<const double2*>(&L[c][q]);
+        s = fma(-x[q], l2.x, s);
+        s = fma(-x[q + 1], l2.y, s);
+      } else {
+        s = fma(-x[q], L[c][q], s);
+      }
+    }
+    x[c] = s * invd[c];
+  }
+#pragma unroll
+  for (int c = 0; c < kNB; ++c) A[(long long)c * ts] = x[c];
+}
+
+void launch_trsm_rows(double* tiles, int ts, long long slot0, int ntiles, int row0, int col0,
+                      long long lslot, cudaStream_t st) {
+  const int rows = ts - row0;
+  if (rows <= 0 || ntiles <= 0) return;
+  const int threads = 128;
+  trsm_rows_kernel<<<dim3((rows + threads - 1) / threads, ntiles), threads, 0, st>>>(tiles, ts, slot0,
+                                                                                    row0, col0, lslot);
+}
+
+// ---------------------------------------------------------------------------
+// Forward substitution on one diagonal tile: z_k := L_kk^-1 z_k.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+trsv_diag_kernel(const double* __restrict__ tiles, int ts, long long slot, double* __restrict__ zk) {
+  extern __shared__ double zs[];  // ts
+  __shared__ double B[kNB][kNB + 1];
+  const double* T = tiles + slot * (long long)ts * ts;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int r = tid; r < ts; r += blockDim.x) zs[r] = zk[r];
+  for (int kb = 0; kb < ts; kb += kNB) {
+    for (int e = tid; e < kNB * kNB; e += blockDim.x) {
+      const int rr = e % kNB, c = e / kNB;
+      B[rr][c] = (rr >= c) ? T[(long long)(kb + c) * ts + kb + rr] : 0.0;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      double z0 = zs[kb + lane], z1 = zs[kb + 32 + lane];
+      for (int c = 0; c < kNB; ++c) {
+        double zc;
+        if (c < 32) {
+          if (lane == c) z0 = z0 / B[c][c];
+          zc = __shfl_sync(0xffffffffu, z0, c);
+        } else {
+          if (lane == c - 32) z1 = z1 / B[c][c];
+          zc = __shfl_sync(0xffffffffu, z1, c - 32);
+        }
+        if (lane > c) z0 = fma(-B[lane][c], zc, z0);
+        if (lane + 32 > c) z1 = fma(-B[lane + 32][c], zc, z1);
+      }
+      zs[kb + lane] = z0;
+      zs[kb + 32 + lane] = z1;
+    }
+    __syncthreads();
+    for (int r = kb + kNB + tid; r < ts; r += blockDim.x) {
+      double acc = 0.0;
+      const double* col = T + (long long)kb * ts + r;
+#pragma unroll 8
+      for (int c = 0; c < kNB; ++c) acc = fma(col[(long long)c * ts], zs[kb + c], acc);
+      zs[r] -= acc;
+    }
+    __syncthreads();
+  }
+  for (int r = tid; r < ts; r += blockDim.x) zk[r] = zs[r];
+}
+
+void launch_trsv_diag(const double* tiles, int ts, long long slot, double* zk, cudaStream_t st) {
+  trsv_diag_kernel<<<1, 256, ts * sizeof(double), st>>>(tiles, ts, slot, zk);
+}
+
+// z_i -= L_ik z_k for every tile row i > k.  256 threads = 64 rows x 4 column groups.
+__global__ void __launch_bounds__(256)
+gemv_panel_kernel(const double* __restrict__ tiles, int ts, int nt, int k, double* __restrict__ z) {
+  extern __shared__ double zks[];  // ts
+  __shared__ double red[4][kNB];
+  const int i = k + 1 + blockIdx.y;
+  const double* T = tiles + tile_slot(i, k, nt) * (long long)ts * ts;
+  for (int c = threadIdx.x; c < ts; c += blockDim.x) zks[c] = z[(long long)k * ts + c];
+  __syncthreads();
+  const int rl = threadIdx.x % kNB, g = threadIdx.x / kNB;
+  const int r = blockIdx.x * kNB + rl;
+  double acc = 0.0;
+  if (r < ts) {
+    for (int c = g; c < ts; c += 4) acc = fma(T[(long long)c * ts + r], zks[c], acc);
+  }
+  red[g][rl] = acc;
+  __syncthreads();
+  if (g == 0 && r < ts) z[(long long)i * ts + r] -= ((red[0][rl] + red[1][rl]) + red[2][rl]) + red[3][rl];
+}
+
+void launch_gemv_panel(const double* tiles, int ts, int nt, int k, double* z, cudaStream_t st) {
+  if (k >= nt - 1) return;
+  gemv_panel_kernel<<<dim3((ts + kNB - 1) / kNB, nt - 1 - k), 256, ts * sizeof(double), st>>>(tiles, ts, nt,
+                                                                                          k, z);
+}
+
+// ---------------------------------------------------------------------------
+// Backward substitution on one diagonal tile: z_k := L_kk^-T z_k.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+trsv_t_diag_kernel(const double* __restrict__ tiles, int ts, long long slot, double* __restrict__ zk) {
+  extern __shared__ double zs[];
+  __shared__ double B[kNB][kNB + 1];
+  const double* T = tiles + slot * (long long)ts * ts;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int r = tid; r < ts; r += blockDim.x) zs[r] = zk[r];
+  for (int kb = ts - kNB; kb >= 0; kb -= kNB) {
+    for (int e = tid; e < kNB * kNB; e += blockDim.x) {
+      const int rr = e % kNB, c = e / kNB;
+      B[rr][c] = (rr >= c) ? T[(long long)(kb + c) * ts + kb + rr] : 0.0;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      double z0 = zs[kb + lane], z1 = zs[kb + 32 + lane];
+      for (int c = kNB - 1; c >= 0; --c) {
+        double zc;
+        if (c >= 32) {
+          if (lane == c - 32) z1 = z1 / B[c][c];
+          zc = __shfl_sync(0xffffffffu, z1, c - 32);
+        } else {
+          if (lane == c) z0 = z0 / B[c][c];
+          zc = __shfl_sync(0xffffffffu, z0, c);
+        }
+        // rows r < c: z_r -= L[c][r] x_c
+        if (lane < c) z0 = fma(-B[c][lane], zc, z0);
+        if (lane + 32 < c) z1 = fma(-B[c][lane + 32], zc, z1);
+      }
+      zs[kb + lane] = z0;
+      zs[kb + 32 + lane] = z1;
+    }
+    __syncthreads();
+    // rows r < kb: z_r -= sum_c L[kb+c][r] x[kb+c]; column r of L is contiguous in rows.
+    for (int r = warp; r < kb; r += blockDim.x / 32) {
+      const double* col = T + (long long)r * ts + kb;
+      double acc = fma(col[lane], zs[kb + lane], col[lane + 32] * zs[kb + lane + 32]);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      if (lane == 0) zs[r] -= acc;
+    }
+    __syncthreads();
+  }
+  for (int r = tid; r < ts; r += blockDim.x) zk[r] = zs[r];
+}
+
+void launch_trsv_t_diag(const double* tiles, int ts, long long slot, double* zk, cudaStream_t st) {
+  trsv_t_diag_kernel<<<1, 256, ts * sizeof(double), st>>>(tiles, ts, slot, zk);
+}
+
+// z_i -= L_ki^T z_k for every tile column i < k (tile (k, i) is stored).  One warp per column.
+__global__ void __launch_bounds__(256)
+gemv_t_panel_kernel(const double* __restrict__ tiles, int ts, int nt, int k, double* __restrict__ z) {
+  const int i = blockIdx.y;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int c = blockIdx.x * 8 + warp;
+  if (c >= ts) return;
+  const double* col = tiles + tile_slot(k, i, nt) * (long long)ts * ts + (long long)c * ts;
+  const double* zk = z + (long long)k * ts;
+  double acc = 0.0;
+  for (int r = lane; r < ts; r += 32) acc = fma(col[r], zk[r], acc);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0) z[(long long)i * ts + c] -= acc;
+}
+
+void launch_gemv_t_panel(const double* tiles, int ts, int nt, int k, double* z, cudaStream_t st) {
+  if (k <= 0) return;
+  gemv_t_panel_kernel<<<dim3((ts + 7) / 8, k), 256, 0, st>>>(tiles, ts, nt, k, z);
+}
+
+// ---------------------------------------------------------------------------
+// Deterministic reductions.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double block_sum_256(double v, double* red) {
+  red[threadIdx.x] = v;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+    __syncthreads();
+  }
+  const double out = red[0];
+  __syncthreads();
+  return out;
+}
+
+// partial[k] = sum over the real rows of diagonal tile k of log L_rr (L_rr > 0 only,
+// dmdet-codelet.cpp:76-77).
+__global__ void __launch_bounds__(256)
+logdet_partials_kernel(const double* __restrict__ tiles, int ts, int nt, int n, double* __restrict__ partial) {
+  __shared__ double red[256];
+  const int k = blockIdx.x;
+  const double* T = tiles + tile_slot(k, k, nt) * (long long)ts * ts;
+  double acc = 0.0;
+  for (int r = threadIdx.x; r < ts; r += blockDim.x) {
+    if (k * ts + r < n) {
+      const double d = T[(long long)r * ts + r];
+      if (d > 0.0) acc += log(d);
+    }
+  }
+  const double s = block_sum_256(acc, red);
+  if (threadIdx.x == 0) partial[k] = s;
+}
+
+void launch_logdet_partials(const double* tiles, int ts, int nt, int n, double* partial, cudaStream_t st) {
+  logdet_partials_kernel<<<nt, 256, 0, st>>>(tiles, ts, nt, n, partial);
+}
+
+// result[0] = log-likelihood, result[1] = log|C|, result[2] = Z^T C^-1 Z (after trsv),
+// following ChameleonImplementation.cpp:188-192 and :257-265:
+//   logdet = 2 * sum log L_kk,  loglik = -0.5 dot - 0.5 logdet - (n/2) log(2 pi).
+__global__ void __launch_bounds__(256)
+finalize_kernel(const double* __restrict__ partial, int nt, const double* __restrict__ z, int n,
+                double* __restrict__ result, const int* __restrict__ info) {
+  __shared__ double red[256];
+  double acc = 0.0;
+  for (int r = threadIdx.x; r < n; r += blockDim.x) acc = fma(z[r], z[r], acc);
+  const double dot = block_sum_256(acc, red);
+  if (threadIdx.x == 0) {
+    double det = 0.0;
+    for (int k = 0; k < nt; ++k) det += partial[k];
+    const double logdet = 2.0 * det;
+    const double pi = 3.141592653589793;
+    const double nn = (double)n;
+    result[0] = -0.5 * dot - 0.5 * logdet - (double)(nn / 2.0) * log(2.0 * pi);
+    result[1] = logdet;
+    result[2] = dot;
+    result[3] = (double)(info ? *info : 0);
+  }
+}
+
+void launch_finalize(const double* partial, int nt, const double* z, int n, double* result, const int* info,
+                     cudaStream_t st) {
+  finalize_kernel<<<1, 256, 0, st>>>(partial, nt, z, n, result, info);
+}
+
+// out[0] = sum (a - b)^2 (DMSECodelet, dmse-codelet.cpp:60-73), fixed order.
+__global__ void __launch_bounds__(256)
+sumsq_diff_kernel(const double* __restrict__ a, const double* __restrict__ b, int n, double* __restrict__ out) {
+  __shared__ double red[256];
+  double acc = 0.0;
+  for (int r = threadIdx.x; r < n; r += blockDim.x) {
+    const double d = a[r] - b[r];
+    acc = fma(d, d, acc);
+  }
+  const double s = block_sum_256(acc, red);
+  if (threadIdx.x == 0) out[0] = s;
+}
+
+void launch_sumsq_diff(const double* a, const double* b, int n, double* out, cudaStream_t st) {
+  sumsq_diff_kernel<<<1, 256, 0, st>>>(a, b, n, out);
+}
+
+}  // namespace egs
+
+namespace egs {
+
+// out[j] = sum_i A[i + j*lda] * w[i] for j < cols (A is rows x cols column-major):
+// the kriging product Zmiss = C12 * Zobs with C12 stored transposed (obs x miss,
+// LinearAlgebraMethods.cpp:552).  One warp per output, fixed reduction order.
+__global__ void __launch_bounds__(256)
+gemv_t_block_kernel(const double* __restrict__ a, long long lda, int rows, int cols, const double* __restrict__ w,
+                    double* __restrict__ out) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int j = blockIdx.x * 8 + warp;
+  if (j >= cols) return;
+  const double* col = a + (long long)j * lda;
+  double acc = 0.0;
+  for (int i = lane; i < rows; i += 32) acc = fma(col[i], w[i], acc);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0) out[j] = acc;
+}
+
+void launch_gemv_t_block(const double* a, long long lda, int rows, int cols, const double* w, double* out,
+                         cudaStream_t st) {
+  if (cols <= 0) return;
+  gemv_t_block_kernel<<<(cols + 7) / 8, 256, 0, st>>>(a, lda, rows, cols, w, out);
+}
+
+}  // namespace egs
+
+namespace egs {
+
+// part[slot(i, j)][r] = sum_c L_ij[r][c] e_j[c] over the stored lower tiles (only
+// c <= r inside a diagonal tile): the tile products of Z = L e
+// (dtrmm in GenerateObservationsVector, LinearAlgebraMethods.cpp:400).
+__global__ void __launch_bounds__(256)
+trmv_tile_kernel(const double* __restrict__ tiles, int ts, int nt, const double* __restrict__ e,
+                 double* __restrict__ part) {
+  __shared__ double red[4][kNB];
+  const long long slot = blockIdx.y;
+  // slot -> (i, j)
+  int j = 0;
+  while (j < nt - 1 && tile_slot(j + 1, j + 1, nt) <= slot) ++j;
+  const int i = j + (int)(slot - tile_slot(j, j, nt));
+  const double* T = tiles + slot * (long long)ts * ts;
+  const double* ej = e + (long long)j * ts;
+  const int rl = threadIdx.x % kNB, g = threadIdx.x / kNB;
+  const int r = blockIdx.x * kNB + rl;
+  double acc = 0.0;
+  if (r < ts) {
+    const int cend = (i == j) ? r + 1 : ts;
+    for (int c = g; c < cend; c += 4) acc = fma(T[(long long)c * ts + r], ej[c], acc);
+  }
+  red[g][rl] = acc;
+  __syncthreads();
+  if (g == 0 && r < ts) part[slot * ts + r] = ((red[0][rl] + red[1][rl]) + red[2][rl]) + red[3][rl];
+}
+
+// z[i*ts + r] = sum_{j <= i} part[slot(i, j)][r], j ascending (fixed order).
+__global__ void __launch_bounds__(256)
+trmv_reduce_kernel(const double* __restrict__ part, int ts, int nt, double* __restrict__ z) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= (long long)nt * ts) return;
+  const int i = (int)(g / ts), r = (int)(g - (long long)i * ts);
+  double acc = 0.0;
+  for (int j = 0; j <= i; ++j) acc += part[tile_slot(i, j, nt) * ts + r];
+  z[g] = acc;
+}
+
+void launch_trmv(const double* tiles, int ts, int nt, const double* e, double* part, double* z, cudaStream_t st) {
+  const long long nslots = lower_tiles(nt);  // <= 65535 is checked by the caller
+  trmv_tile_kernel<<<dim3((ts + kNB - 1) / kNB, (unsigned)nslots), 256, 0, st>>>(tiles, ts, nt, e, part);
+  const long long total = (long long)nt * ts;
+  trmv_reduce_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(part, ts, nt, z);
+}
+
+}  // namespace egs

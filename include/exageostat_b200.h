@@ -1,0 +1,175 @@
+/*
+ * exageostat_b200.h -- C ABI of the B200 (sm_100a) maximum-likelihood path.
+ *
+ * Plain C: pointers, sizes and int status codes; nothing here throws, traps or
+ * needs a C++ or torch type.  Every function returns EGS_OK (0) on success, a
+ * positive value for a Cholesky failure (1-based global column of the first
+ * non-positive pivot, the LAPACK "info"), or a negative EGS_ERR_* code.
+ *
+ * Each entry point names the ExaGeoStatCPP interface it replaces (paths are
+ * relative to the ExaGeoStatCPP source tree).
+ */
+#ifndef EXAGEOSTAT_B200_H
+#define EXAGEOSTAT_B200_H
+
+#if defined(__GNUC__)
+#define EGS_API __attribute__((visibility("default")))
+#else
+#define EGS_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EGS_OK 0
+#define EGS_ERR_INVALID (-1)     /* bad argument: sizes, null pointers, theta outside its domain */
+#define EGS_ERR_CUDA (-2)        /* a CUDA runtime call failed */
+#define EGS_ERR_NO_DEVICE (-3)   /* no usable CUDA device */
+#define EGS_ERR_OOM (-4)         /* device allocation refused */
+#define EGS_ERR_TIMEOUT (-5)     /* a bounded device-side wait gave up */
+#define EGS_ERR_STATE (-6)       /* call order: e.g. evaluation before locations were set */
+
+/* Opaque device-resident problem: locations, observations, the tile-major lower
+ * covariance storage and the reduction buffers of one N.  Replaces the
+ * DescriptorData<T> set of Chameleon descriptors (C, Z, Zcpy, det, product)
+ * created by LinearAlgebraMethods<T>::InitiateDescriptors
+ * (src/linear-algebra-solvers/LinearAlgebraMethods.cpp:36-118). */
+typedef struct egs_problem egs_problem;
+
+/* Library version as MAJOR*10000 + MINOR*100 + PATCH. */
+EGS_API int egs_version(void);
+/* Human-readable name of a status code (static storage). */
+EGS_API const char* egs_status_string(int status);
+/* Message of the last error raised on the calling host thread ("" if none). */
+EGS_API const char* egs_last_error(void);
+
+/* Select and initialise the CUDA device.  Replaces
+ * ExaGeoStatHardware::InitHardware (src/hardware/ExaGeoStatHardware.cpp:126-172). */
+EGS_API int egs_hardware_init(int device);
+
+/* ---- descriptors ------------------------------------------------------- */
+
+/* Allocate a problem of n locations with dense tile size dts (the reference's
+ * --dts; the device tile is dts rounded up to a multiple of 64).
+ * Replaces LinearAlgebraMethods<T>::InitiateDescriptors
+ * (LinearAlgebraMethods.cpp:36-118) + DescriptorData<T>::SetDescriptor
+ * (src/data-units/DescriptorData.cpp:148-191). */
+EGS_API int egs_problem_create(egs_problem** out, int n, int dts);
+/* Free everything; replaces DescriptorData<T>::~DescriptorData (DescriptorData.cpp:21-62). */
+EGS_API int egs_problem_destroy(egs_problem* p);
+/* n, device tile size, number of tile rows, device bytes held. */
+EGS_API int egs_problem_info(const egs_problem* p, int* n, int* ts, int* nt, long long* bytes);
+/* Run all later work of this problem on the given cudaStream_t (NULL: the problem's own stream). */
+EGS_API int egs_problem_set_stream(egs_problem* p, void* cuda_stream);
+
+/* Copy n locations from host memory (Locations<T> SoA x[], y[],
+ * src/data-units/Locations.cpp:94-118). */
+EGS_API int egs_problem_set_locations(egs_problem* p, const double* x, const double* y);
+/* Same from device memory. */
+EGS_API int egs_problem_set_locations_device(egs_problem* p, const double* x, const double* y);
+/* Copy the n observations Z into the saved copy Zcpy (the iteration-0 dlacpy
+ * Z -> Zcpy of ChameleonImplementation.cpp:113-119). */
+EGS_API int egs_problem_set_observations(egs_problem* p, const double* z);
+EGS_API int egs_problem_set_observations_device(egs_problem* p, const double* z);
+
+/* ---- stages of one evaluation (device resident) ------------------------ */
+
+/* Lower tiles of C(theta), theta = (sigma^2, beta, nu).  Replaces
+ * RuntimeFunctions<T>::CovarianceMatrix (src/runtime/starpu/StarPuFunctions.cpp:24-45)
+ * with UnivariateMaternStationary<T>::GenerateCovarianceMatrix
+ * (src/kernels/concrete/UnivariateMaternStationary.cpp:39-67). */
+EGS_API int egs_covariance_generate(egs_problem* p, const double* theta);
+/* In-place lower Cholesky of the tiles.  Replaces ChameleonDense<T>::ExaGeoStatPotrfTile
+ * (src/linear-algebra-solvers/concrete/chameleon/dense/ChameleonDense.cpp:25-37).
+ * Returns > 0 (info) when the matrix is not positive definite. */
+EGS_API int egs_potrf(egs_problem* p);
+/* Z := Zcpy (ChameleonImplementation.cpp:120-124). */
+EGS_API int egs_restore_observations(egs_problem* p);
+/* Z := L^-1 Z.  Replaces ChameleonImplementation<T>::ExaGeoStatTrsmTile
+ * (ChameleonImplementation.cpp:337-347, called at :216-217). */
+EGS_API int egs_trsv(egs_problem* p);
+/* log|C| = 2 sum log L_kk (RuntimeFunctions<T>::ExaGeoStatMeasureDetTileAsync,
+ * StarPuFunctions.cpp:119-135; dmdet-codelet.cpp:73-80), Z^T Z
+ * (RuntimeFunctions<T>::ExaGeoStatDoubleDotProduct, StarPuFunctions.cpp:189-204)
+ * and the log-likelihood (ChameleonImplementation.cpp:257-265). */
+EGS_API int egs_loglik_parts(egs_problem* p, double* loglik, double* logdet, double* dot);
+/* Copy tile (i, j), i >= j, to host (ts*ts doubles, column-major). */
+EGS_API int egs_get_tile(egs_problem* p, int i, int j, double* host_out);
+/* Copy the current Z (n doubles) to host. */
+EGS_API int egs_get_observations(egs_problem* p, double* host_z);
+
+/* One full log-likelihood evaluation at theta on the resident data: restore Z,
+ * generate, factor, log-det, solve, dot, assemble.  Replaces
+ * ChameleonImplementation<T>::ExaGeoStatMLETile (ChameleonImplementation.cpp:35-327).
+ * logdet and dot may be NULL. */
+EGS_API int egs_mle_eval(egs_problem* p, const double* theta, double* loglik, double* logdet, double* dot);
+
+/* ---- synthetic data (the reference's generator semantics) ---------------- */
+
+/* n jittered-grid locations in [0,1]^2, Morton sorted and 16-bit quantised, drawn
+ * from the C library's rand(); srand(seed) first when reseed != 0.  Replaces
+ * LocationGenerator<T>::GenerateLocations (src/data-generators/LocationGenerator.cpp:25-123). */
+EGS_API int egs_generate_locations(int n, int seed, int reseed, double* x, double* y);
+/* n N(0,1) samples of LAPACK DLARNV(IDIST=3, ISEED) (ISEED entries in [0, 4095],
+ * ISEED[3] odd), as drawn at LinearAlgebraMethods.cpp:347-364. */
+EGS_API int egs_dlarnv_normal(const int* iseed, int n, double* out);
+/* Z = L e at theta with e = DLARNV(3, {seed, seed, seed, 1}) and L = chol(C(theta))
+ * on the resident locations; Z becomes the problem's observations (and is copied
+ * to z_out when it is not NULL).  Replaces
+ * LinearAlgebraMethods<T>::GenerateObservationsVector (LinearAlgebraMethods.cpp:333-449). */
+EGS_API int egs_generate_observations(egs_problem* p, const double* theta, int seed, double* z_out);
+
+/* ---- instrumentation ----------------------------------------------------- */
+
+/* Stages of an evaluation, for the per-stage counters below (the reference's
+ * START_TIMING/STOP_TIMING around matrix generation, factorisation and solve,
+ * ChameleonImplementation.cpp:127-220). */
+#define EGS_STAGE_GENERATE 0   /* Matern tiles */
+#define EGS_STAGE_PANEL 1      /* diagonal-tile factorisation + panel triangular solve */
+#define EGS_STAGE_UPDATE 2     /* trailing syrk/gemm on the FP64 tensor path */
+#define EGS_STAGE_SOLVE 3      /* Z := L^-1 Z (and L^-T for kriging) */
+#define EGS_STAGE_REDUCE 4     /* log-det, dot, log-likelihood assembly */
+#define EGS_NUM_STAGES 5
+
+/* Enable (1) or disable (0) CUDA-event timing of every stage on the problem's
+ * stream; either call resets the counters.  Kernel launches are always counted. */
+EGS_API int egs_problem_set_profiling(egs_problem* p, int enable);
+/* Accumulated device milliseconds, algorithmic flops (real rows only) and kernel
+ * launches per stage since the last egs_problem_set_profiling; each pointer may be
+ * NULL or point to EGS_NUM_STAGES elements. */
+EGS_API int egs_problem_stage_stats(egs_problem* p, double* ms, double* flops, long long* launches);
+
+/* ---- kernel plugin ------------------------------------------------------ */
+
+/* rows x cols column-major block (leading dimension lda) on caller device
+ * memory: A[i + j*lda] = Matern(|loc1[i] - loc2[j]|; theta); the device form of
+ * Kernel<T>::GenerateCovarianceMatrix (inst/include/kernels/Kernel.hpp:93-97)
+ * for "UnivariateMaternStationary".  The location pointers are already offset
+ * to the block's first row / column.  distance_metric must be 0 (Euclidean),
+ * which is what the MLE passes (ChameleonImplementation.cpp:172). */
+EGS_API int egs_matern_block(double* a, int lda, int rows, int cols, const double* x1, const double* y1,
+                     const double* x2, const double* y2, const double* theta, int distance_metric,
+                     void* cuda_stream);
+
+/* ---- host-buffer entry points ------------------------------------------- */
+
+/* Log-likelihood of host data: copies locations and Z to the device, evaluates,
+ * returns the scalar.  Reuses one cached problem per (n, dts) on the calling
+ * thread, the way ExaGeoStatData keeps its descriptors across NLopt iterations. */
+EGS_API int egs_mle_loglik_host(int n, int dts, const double* x, const double* y, const double* z,
+                        const double* theta, double* loglik);
+
+/* Kriging.  Replaces LinearAlgebraMethods<T>::ExaGeoStatMLEPredictTile
+ * (src/linear-algebra-solvers/LinearAlgebraMethods.cpp:451-605):
+ * C22 = C(obs, obs), w = C22^-1 z_obs (dposv), z_miss = C12 w, and
+ * mspe = sum (z_actual - z_miss)^2 / n_miss, or -1 when z_actual is NULL
+ * (:579-581).  All arrays are host memory. */
+EGS_API int egs_predict_host(int n_obs, int n_miss, int dts, const double* x_obs, const double* y_obs,
+                     const double* z_obs, const double* x_miss, const double* y_miss,
+                     const double* z_actual, const double* theta, double* z_miss, double* mspe);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EXAGEOSTAT_B200_H */

@@ -1,0 +1,232 @@
+"""Parity of the sm_100a path (through the C ABI) with the CPU oracle.
+
+Tolerances (stated in the MLE contract):
+  * Matern tiles, element-wise: |gpu - ref| <= 1e-12 |ref| + 1e-15 sigma2
+  * plain FP64 log-likelihood: relative error <= 1e-10
+  * kriging predictions and MSPE: relative error <= 1e-8
+"""
+import numpy as np
+import pytest
+
+import exageostat_b200 as egs
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+LOGLIK_RTOL = 1e-10
+PREDICT_RTOL = 1e-8
+
+
+def synthetic(n, seed, theta):
+    return O.load_data(n, seed, theta)
+
+
+@pytest.mark.parametrize("nu", [0.5, 1.5, 2.5, 0.8, 0.4, 1.0, 0.3, 2.2, 3.7])
+@pytest.mark.parametrize("n,dts", [(300, 64), (130, 960)])
+def test_matern_tiles_elementwise(n, dts, nu):
+    x, y = O.generate_locations(n, O.GlibcRand(3))
+    theta = [1.7, 0.09, nu]
+    p = egs.Problem(n, dts)
+    p.set_locations(x, y)
+    p.generate(theta)
+    ref = np.tril(O.covariance(x, y, theta))
+    # assemble the generated lower tiles (before any factorisation)
+    got = p.lower_matrix()
+    err = np.abs(got - ref)
+    assert np.all(err <= 1e-12 * np.abs(ref) + 1e-15 * theta[0]), err.max()
+    # padding rows/cols hold the identity
+    if p.nt * p.ts > n:
+        last = p.tile(p.nt - 1, p.nt - 1)
+        r0 = n - (p.nt - 1) * p.ts
+        pad = last[r0:, r0:]
+        assert np.array_equal(pad, np.eye(pad.shape[0]))
+
+
+@pytest.mark.parametrize("n,dts", [(64, 64), (300, 64), (1000, 128), (700, 320), (200, 960)])
+def test_potrf_matches_lapack(n, dts):
+    x, y = O.generate_locations(n, O.GlibcRand(5))
+    theta = [1.0, 0.1, 0.5]
+    p = egs.Problem(n, dts)
+    p.set_locations(x, y)
+    p.generate(theta)
+    p.potrf()
+    L = p.lower_matrix()
+    Lr = O.cholesky_lower(O.covariance(x, y, theta))
+    assert np.abs(L - Lr).max() <= 1e-10 * np.abs(Lr).max()
+
+
+@pytest.mark.parametrize("key", ["z_n9_dts5_seed0", "z_n16_dts9_seed0"])
+def test_loglik_on_reference_fixtures(goldens, key):
+    g = goldens[key]
+    x, y, z = synthetic(g["n"], g["seed"], g["theta"])
+    p = egs.Problem(g["n"], g["dts"])
+    p.set_locations(x, y)
+    p.set_observations(z)
+    for theta in ([1.0, 0.1, 0.5], [1.325, 0.1, 0.1], [0.9, 0.09, 0.4], [2.0, 0.3, 1.7]):
+        ll, logdet, dot = p.mle_eval(theta)
+        ref, rlogdet, rdot = O.mle_loglik(x, y, z, theta, return_parts=True)
+        assert ll == pytest.approx(ref, rel=LOGLIK_RTOL, abs=0)
+
+
+def test_modeling_golden_minus_24_026(goldens):
+    f = goldens["fixture_n16"]
+    g = goldens["modeling_loglik_n16"]
+    p = egs.Problem(16, g["dts"])
+    p.set_locations(f["x"], f["y"])
+    p.set_observations(f["z"])
+    ll, _, _ = p.mle_eval([1.325, 0.1, 0.1])
+    assert abs(ll - g["exact_dense"]) < g["margin"]
+
+
+@pytest.mark.parametrize("theta", [[1.0, 0.1, 0.5], [1.0, 0.05, 0.8], [1.0, 0.03, 1.5], [1.2, 0.2, 2.5]])
+def test_loglik_n1600_ts320(theta):
+    # the reference's CPU configuration: N = 1600, tile 320, Z generated at theta_true = (1, 0.1, 0.5)
+    x, y, z = synthetic(1600, 0, [1.0, 0.1, 0.5])
+    p = egs.Problem(1600, 320)
+    p.set_locations(x, y)
+    p.set_observations(z)
+    ll, logdet, dot = p.mle_eval(theta)
+    ref, rlogdet, rdot = O.mle_loglik(x, y, z, theta, return_parts=True)
+    # Two backward-stable Cholesky factorisations differ by about cond(C) * eps in
+    # Z^T C^-1 Z; the 1e-10 bound holds wherever cond(C) * eps stays below it.
+    kappa = np.linalg.cond(O.covariance(x, y, theta))
+    tol = max(LOGLIK_RTOL, 50.0 * kappa * np.finfo(float).eps)
+    assert ll == pytest.approx(ref, rel=tol, abs=0)
+    assert dot == pytest.approx(rdot, rel=tol)
+    if kappa * np.finfo(float).eps < 1e-12:
+        assert ll == pytest.approx(ref, rel=LOGLIK_RTOL, abs=0)
+
+
+def test_eval_is_deterministic_and_restores_z():
+    x, y, z = synthetic(900, 2, [1.0, 0.1, 0.5])
+    p = egs.Problem(900, 128)
+    p.set_locations(x, y)
+    p.set_observations(z)
+    a = p.mle_eval([1.0, 0.1, 0.5])
+    p.mle_eval([0.5, 0.2, 1.3])
+    b = p.mle_eval([1.0, 0.1, 0.5])
+    assert a == b
+
+
+def test_host_entry_point_matches_resident_eval():
+    x, y, z = synthetic(500, 4, [1.0, 0.1, 0.5])
+    p = egs.Problem(500, 64)
+    p.set_locations(x, y)
+    p.set_observations(z)
+    a = p.mle_eval([0.8, 0.12, 0.9])[0]
+    b = egs.mle_loglik_host(x, y, z, [0.8, 0.12, 0.9], 64)
+    assert a == b
+
+
+def test_stagewise_api_matches_eval():
+    x, y, z = synthetic(400, 6, [1.0, 0.1, 0.5])
+    p = egs.Problem(400, 64)
+    p.set_locations(x, y)
+    p.set_observations(z)
+    theta = [1.1, 0.08, 0.7]
+    full = p.mle_eval(theta)
+    p.restore_observations()
+    p.generate(theta)
+    p.potrf()
+    p.trsv()
+    parts = p.loglik_parts()
+    assert parts == pytest.approx(full, rel=1e-14)
+    w = O.scipy.linalg.solve_triangular(O.cholesky_lower(O.covariance(x, y, theta)), z, lower=True)
+    assert np.abs(p.observations() - w).max() <= 1e-9 * np.abs(w).max()
+
+
+def test_not_positive_definite_is_reported():
+    x, y, z = synthetic(200, 1, [1.0, 0.1, 0.5])
+    x = x.copy()
+    x[77] = np.nan
+    p = egs.Problem(200, 64)
+    p.set_locations(x, y)
+    p.set_observations(z)
+    with pytest.raises(egs.NotPositiveDefinite):
+        p.mle_eval([1.0, 0.1, 0.5])
+    # the context stays usable
+    p.set_locations(*synthetic(200, 1, [1.0, 0.1, 0.5])[:2])
+    assert np.isfinite(p.mle_eval([1.0, 0.1, 0.5])[0])
+
+
+@pytest.mark.parametrize("theta", [[0.0, 0.1, 0.5], [1.0, -0.1, 0.5], [1.0, 0.1, 0.0], [np.nan, 0.1, 0.5]])
+def test_invalid_theta_rejected(theta):
+    p = egs.Problem(50, 64)
+    x, y = O.generate_locations(50, O.GlibcRand(1))
+    p.set_locations(x, y)
+    p.set_observations(np.ones(50))
+    with pytest.raises(egs.EgsError) as ei:
+        p.mle_eval(theta)
+    assert ei.value.status == egs.EGS_ERR_INVALID
+
+
+def test_call_order_enforced():
+    p = egs.Problem(50, 64)
+    with pytest.raises(egs.EgsError) as ei:
+        p.mle_eval([1.0, 0.1, 0.5])
+    assert ei.value.status == egs.EGS_ERR_STATE
+
+
+def test_prediction_mspe_golden(goldens):
+    f = goldens["fixture_n16"]
+    g = goldens["prediction_mspe_n16"]
+    zo, xo, yo, za, xm, ym = O.shuffle_split(f["z"], f["x"], f["y"], g["z_miss_number"], O.GlibcRand(1))
+    zm, mspe = egs.predict_host(xo, yo, zo, xm, ym, g["estimated_theta"], g["dts"], z_actual=za)
+    assert mspe == pytest.approx(g["mspe"], rel=1.2e-5)
+    zr, mr = O.predict(xo, yo, zo, xm, ym, g["estimated_theta"], za)
+    assert mspe == pytest.approx(mr, rel=PREDICT_RTOL)
+    assert np.abs(zm - zr).max() <= PREDICT_RTOL * np.abs(zr).max()
+
+
+@pytest.mark.parametrize("theta", [[1.0, 0.05, 0.8], [1.0, 0.1, 0.5]])
+def test_prediction_vs_oracle(theta):
+    x, y, z = synthetic(2100, 9, theta)
+    zo, xo, yo, za, xm, ym = O.shuffle_split(z, x, y, 100, O.GlibcRand(3))
+    zm, mspe = egs.predict_host(xo, yo, zo, xm, ym, theta, 320, z_actual=za)
+    zr, mr = O.predict(xo, yo, zo, xm, ym, theta, za)
+    assert np.abs(zm - zr).max() <= PREDICT_RTOL * np.abs(zr).max()
+    assert mspe == pytest.approx(mr, rel=PREDICT_RTOL)
+    # without the truth the reference reports -1 (LinearAlgebraMethods.cpp:579-581)
+    _, m2 = egs.predict_host(xo, yo, zo, xm, ym, theta, 320)
+    assert m2 == -1.0
+
+
+def test_matern_block_plugin_entry_point():
+    torch = pytest.importorskip("torch")
+    import ctypes
+    x1, y1 = O.generate_locations(70, O.GlibcRand(11))
+    x2, y2 = O.generate_locations(33, O.GlibcRand(12))
+    theta = np.array([1.3, 0.07, 1.2])
+    dev = torch.device("cuda:0")
+    tx1, ty1 = torch.tensor(x1, device=dev), torch.tensor(y1, device=dev)
+    tx2, ty2 = torch.tensor(x2, device=dev), torch.tensor(y2, device=dev)
+    lda = 80
+    a = torch.zeros(33 * lda, dtype=torch.float64, device=dev)
+    lib = egs.load_library()
+    rc = lib.egs_matern_block(ctypes.c_void_p(a.data_ptr()), lda, 70, 33, ctypes.c_void_p(tx1.data_ptr()),
+                              ctypes.c_void_p(ty1.data_ptr()), ctypes.c_void_p(tx2.data_ptr()),
+                              ctypes.c_void_p(ty2.data_ptr()), theta.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                              0, None)
+    assert rc == 0
+    torch.cuda.synchronize()
+    got = a.cpu().numpy().reshape(33, lda).T[:70, :]
+    ref = O.matern_block(x1, y1, x2, y2, theta)
+    assert np.all(np.abs(got - ref) <= 1e-12 * np.abs(ref) + 1e-15)
+    assert np.all(a.cpu().numpy().reshape(33, lda).T[70:, :] == 0)  # rows beyond `rows` untouched
+    rc = lib.egs_matern_block(ctypes.c_void_p(a.data_ptr()), lda, 70, 33, ctypes.c_void_p(tx1.data_ptr()),
+                              ctypes.c_void_p(ty1.data_ptr()), ctypes.c_void_p(tx2.data_ptr()),
+                              ctypes.c_void_p(ty2.data_ptr()), theta.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                              1, None)
+    assert rc == egs.EGS_ERR_INVALID
+
+
+@pytest.mark.slow
+def test_loglik_n10000_ts960_nonhalf_nu():
+    theta = [1.0, 0.05, 0.8]
+    x, y, z = synthetic(10000, 1, theta)
+    p = egs.Problem(10000, 960)
+    p.set_locations(x, y)
+    p.set_observations(z)
+    ll, logdet, dot = p.mle_eval(theta)
+    ref, rlogdet, rdot = O.mle_loglik(x, y, z, theta, return_parts=True)
+    assert ll == pytest.approx(ref, rel=LOGLIK_RTOL, abs=0)
