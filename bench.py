@@ -210,6 +210,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-eval", action="store_true",
                     help="one evaluation between cudaProfilerStart/Stop (for ncu --profile-from-start off)")
+    ap.add_argument("--profile-n", type=int, default=0,
+                    help="with --profile-eval: evaluate this many of the workload's locations with "
+                         "DLARNV observations instead of the full workload (small ncu captures)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -238,7 +241,11 @@ def main():
         pass
 
     if args.profile_eval:
-        x, y, z = workload_data(egs)
+        if args.profile_n:
+            x, y = egs.generate_locations(args.profile_n, SEED)
+            z = egs.dlarnv_normal(SEED, args.profile_n)
+        else:
+            x, y, z = workload_data(egs)
         p = egs.Problem(len(z), DTS)
         p.set_locations(x, y)
         p.set_observations(z)

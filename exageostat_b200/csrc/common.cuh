@@ -14,7 +14,7 @@
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
-#include "../../include/exageostat_b200.h"
+#include "exageostat_b200.h"
 
 namespace egs {
 

@@ -13,8 +13,8 @@
 // a 16-row TMA box never straddles two tiles, so a 128 x 128 CTA tile may span
 // tile boundaries and no MMA work is wasted when 128 does not divide ts.
 //
-// Pipeline.  Thread 0 issues 3-D TMA loads (rows x cols x tile-slot), running up
-// to five stages ahead, into a 6-stage ring of 128B-swizzled shared-memory
+// Pipeline.  Thread 0 issues 3-D TMA loads (rows x cols x tile-slot), running up to
+// two stages ahead, into a 3-stage ring of 32-column 128B-swizzled shared-memory
 // stages guarded by mbarriers; eight warps each own a 64 x 32 sub-tile and run
 // mma.sync m16n8k16 .f64 (the FP64 tensor path of sm_100a).  The 16 rows of an
 // MMA fragment are mapped to tile rows through fixed permutations chosen so
@@ -32,11 +32,17 @@
 namespace egs {
 
 namespace gemm {
-constexpr int BM = 128, BN = 128, BK = 16, STAGES = 6;
+#ifndef EGS_GEMM_BK
+#define EGS_GEMM_BK 32
+#endif
+#ifndef EGS_GEMM_STAGES
+#define EGS_GEMM_STAGES 3
+#endif
+constexpr int BM = 128, BN = 128, BK = EGS_GEMM_BK, STAGES = EGS_GEMM_STAGES;
 constexpr int CONSUMER_WARPS = 8;
 constexpr int THREADS = CONSUMER_WARPS * 32;   // thread 0 also issues the TMA loads
 constexpr int BOX_ROWS = 16;                          // 16 doubles = one 128-byte swizzle row
-constexpr int BOX_BYTES = BOX_ROWS * BK * 8;          // 2 KB
+constexpr int BOX_BYTES = BOX_ROWS * BK * 8;          // 16 rows x BK columns
 constexpr int A_STAGE_BYTES = (BM / BOX_ROWS) * BOX_BYTES;
 constexpr int B_STAGE_BYTES = (BN / BOX_ROWS) * BOX_BYTES;
 constexpr int STAGE_BYTES = A_STAGE_BYTES + B_STAGE_BYTES;
@@ -103,6 +109,20 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, u
       "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
       : "memory");
 }
+__device__ __forceinline__ double lds_f64(uint32_t addr) {
+  double v;
+  asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(addr));
+  return v;
+}
+__device__ __forceinline__ void lds_v2f64(uint32_t addr, double& a, double& b) {
+  asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(a), "=d"(b) : "r"(addr));
+}
+__device__ __forceinline__ void ldg_v2f64(const double* p, double& a, double& b) {
+  asm volatile("ld.global.v2.f64 {%0, %1}, [%2];" : "=d"(a), "=d"(b) : "l"(p));
+}
+__device__ __forceinline__ void stg_v2f64(double* p, double a, double b) {
+  asm volatile("st.global.v2.f64 [%0], {%1, %2};" ::"l"(p), "d"(a), "d"(b) : "memory");
+}
 __device__ __forceinline__ void dmma_16816(double (&d)[4], const double (&a)[8], const double (&b)[4]) {
   asm volatile(
       "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
@@ -149,20 +169,36 @@ __device__ __forceinline__ bool decode_block(long long L, const GemmDesc& d, int
 }
 
 // Producer cursor: walks the same (block, k-step) sequence as the consumers,
-// running up to STAGES-1 stages ahead of them.
+// running up to STAGES-1 stages ahead of them.  The TMA (x, z) coordinates of
+// the 2 x 8 boxes of a block depend only on the block, so they are computed
+// once per block into shared memory; a stage then only adds its k offset.
 struct Cursor {
   long long L;
-  int kt, m0, n0;
+  int kt;
   bool valid;
 };
 
-__device__ __forceinline__ void cursor_seek(Cursor& c, const GemmDesc& d) {
+__device__ __forceinline__ void box_coords(int g0, int tcol, const GemmDesc& d, int2* out) {
+#pragma unroll
+  for (int b = 0; b < gemm::BM / gemm::BOX_ROWS; ++b) {
+    const int g = g0 + b * gemm::BOX_ROWS;
+    int x = d.ts, z = 0;  // fully out of bounds -> zero fill
+    if (g < d.np) {
+      const int ti = g / d.ts;
+      x = g - ti * d.ts;
+      z = (int)tile_slot(ti, tcol, d.nt);
+    }
+    out[b] = make_int2(x, z);
+  }
+}
+
+__device__ __forceinline__ void cursor_seek(Cursor& c, const GemmDesc& d, int2* coords) {
   while (c.L < d.total) {
     int mb, nb;
     decode_block(c.L, d, mb, nb);
     if (!(d.lower && mb < nb)) {
-      c.m0 = mb * gemm::BM;
-      c.n0 = nb * gemm::BN;
+      box_coords(d.a_row0 + mb * gemm::BM, d.a_tcol, d, coords);
+      box_coords(d.b_row0 + nb * gemm::BN, d.b_tcol, d, coords + gemm::BM / gemm::BOX_ROWS);
       c.valid = true;
       return;
     }
@@ -172,33 +208,21 @@ __device__ __forceinline__ void cursor_seek(Cursor& c, const GemmDesc& d) {
 }
 
 __device__ __forceinline__ void issue_stage(const CUtensorMap* tmap, uint8_t* smem, uint64_t* full, uint32_t s,
-                                            const Cursor& c, const GemmDesc& d) {
+                                            const Cursor& c, const GemmDesc& d, const int2* coords) {
   using namespace gemm;
   mbar_expect_tx(&full[s], STAGE_BYTES);
   uint8_t* sa = smem + s * STAGE_BYTES;
   uint8_t* sb = sa + A_STAGE_BYTES;
-  const int kcol = c.kt * BK;
+  const int ya = d.a_col0 + c.kt * BK, yb = d.b_col0 + c.kt * BK;
 #pragma unroll
   for (int b = 0; b < BM / BOX_ROWS; ++b) {
-    const int g = d.a_row0 + c.m0 + b * BOX_ROWS;
-    int x = d.ts, z = 0;  // fully out of bounds -> zero fill
-    if (g < d.np) {
-      const int ti = g / d.ts;
-      x = g - ti * d.ts;
-      z = (int)tile_slot(ti, d.a_tcol, d.nt);
-    }
-    tma_load_3d(sa + b * BOX_BYTES, tmap, &full[s], x, d.a_col0 + kcol, z);
+    const int2 xz = coords[b];
+    tma_load_3d(sa + b * BOX_BYTES, tmap, &full[s], xz.x, ya, xz.y);
   }
 #pragma unroll
   for (int b = 0; b < BN / BOX_ROWS; ++b) {
-    const int g = d.b_row0 + c.n0 + b * BOX_ROWS;
-    int x = d.ts, z = 0;
-    if (g < d.np) {
-      const int ti = g / d.ts;
-      x = g - ti * d.ts;
-      z = (int)tile_slot(ti, d.b_tcol, d.nt);
-    }
-    tma_load_3d(sb + b * BOX_BYTES, tmap, &full[s], x, d.b_col0 + kcol, z);
+    const int2 xz = coords[BM / BOX_ROWS + b];
+    tma_load_3d(sb + b * BOX_BYTES, tmap, &full[s], xz.x, yb, xz.y);
   }
 }
 
@@ -206,8 +230,11 @@ __global__ void __launch_bounds__(gemm::THREADS, 1)
 dgemm_update_kernel(const __grid_constant__ CUtensorMap tmap, double* __restrict__ tiles, GemmDesc d,
                     int* __restrict__ err) {
   using namespace gemm;
-  extern __shared__ uint8_t smem_raw[];
-  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  // 1024-byte aligned stage base (128B-swizzle atoms), kept as an offset into the
+  // shared array so every access stays a shared-memory access.
+  uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+  const uint32_t smem_s = smem_u32(smem);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
   uint64_t* empty = full + STAGES;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -225,13 +252,14 @@ dgemm_update_kernel(const __grid_constant__ CUtensorMap tmap, double* __restrict
   __syncthreads();
 
   // Producer state (meaningful in thread 0 only).
+  __shared__ int2 coords[(BM + BN) / BOX_ROWS];
   Cursor cur;
   cur.L = blockIdx.x;
   cur.kt = 0;
   cur.valid = false;
   uint32_t issued = 0;
   bool alive = true;
-  if (producer) cursor_seek(cur, d);
+  if (producer) cursor_seek(cur, d, coords);
   auto top_up = [&](uint32_t consumed) {
     // Keep up to STAGES-1 stages in flight ahead of the consumers.
     while (alive && cur.valid && issued < consumed + STAGES - 1) {
@@ -240,12 +268,12 @@ dgemm_update_kernel(const __grid_constant__ CUtensorMap tmap, double* __restrict
         alive = false;
         break;
       }
-      issue_stage(&tmap, smem, full, s, cur, d);
+      issue_stage(&tmap, smem, full, s, cur, d, coords);
       ++issued;
       if (++cur.kt == ksteps) {
         cur.kt = 0;
         cur.L += gridDim.x;
-        cursor_seek(cur, d);
+        cursor_seek(cur, d, coords);
       }
     }
   };
@@ -254,6 +282,22 @@ dgemm_update_kernel(const __grid_constant__ CUtensorMap tmap, double* __restrict
   const int wm = warp & 1, wn = warp >> 1;  // warp sub-tile: rows wm*64.., cols wn*32..
   const int pa = perm_a(g);
   const int row_in_box = 2 * pa;  // accumulator rows row_in_box, row_in_box + 1
+  // Byte offsets (inside one 16-row box) of this thread's fragment elements.
+  uint32_t aoff[4], boff[2][4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int k = t + 4 * j;
+    aoff[j] = k * 128 + ((pa ^ (k & 7)) << 4);
+  }
+#pragma unroll
+  for (int sN = 0; sN < 2; ++sN) {
+    const int fb = perm_b(g + 8 * sN);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int k = t + 4 * i;
+      boff[sN][i] = k * 128 + (((fb >> 1) ^ (k & 7)) << 4) + ((fb & 1) << 3);
+    }
+  }
 
   uint32_t it = 0;
   bool ok = true;
@@ -278,33 +322,27 @@ dgemm_update_kernel(const __grid_constant__ CUtensorMap tmap, double* __restrict
         break;
       }
       __syncwarp();
-      const uint8_t* sa = smem + s * STAGE_BYTES;
-      const uint8_t* sb = sa + A_STAGE_BYTES;
-      double bf[4][4];
+      const uint32_t sa = smem_s + s * STAGE_BYTES;
+      const uint32_t sb = sa + A_STAGE_BYTES;
 #pragma unroll
-      for (int ni = 0; ni < 4; ++ni) {
-        const uint8_t* box = sb + (wn * 2 + (ni >> 1)) * BOX_BYTES;
-        const int fb = perm_b(g + 8 * (ni & 1));
+      for (int kk = 0; kk < BK / 16; ++kk) {
+        const uint32_t koff = kk * 16 * 128;  // 16 k-rows of 128 bytes per MMA k-step
+        double bf[4][4];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const int k = t + 4 * i;
-          bf[ni][i] = *reinterpret_cast<const double*>(box + k * 128 + (((fb >> 1) ^ (k & 7)) << 4) +
-                                                      ((fb & 1) << 3));
-        }
-      }
+        for (int ni = 0; ni < 4; ++ni) {
+          const uint32_t box = sb + (wn * 2 + (ni >> 1)) * BOX_BYTES + koff;
 #pragma unroll
-      for (int mi = 0; mi < 4; ++mi) {
-        const uint8_t* box = sa + (wm * 4 + mi) * BOX_BYTES;
-        double af[8];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const int k = t + 4 * j;
-          const double2 v = *reinterpret_cast<const double2*>(box + k * 128 + ((pa ^ (k & 7)) << 4));
-          af[2 * j] = v.x;
-          af[2 * j + 1] = v.y;
+          for (int i = 0; i < 4; ++i) bf[ni][i] = lds_f64(box + boff[ni & 1][i]);
         }
 #pragma unroll
-        for (int ni = 0; ni < 4; ++ni) dmma_16816(acc[mi][ni], af, bf[ni]);
+        for (int mi = 0; mi < 4; ++mi) {
+          const uint32_t box = sa + (wm * 4 + mi) * BOX_BYTES + koff;
+          double af[8];
+#pragma unroll
+          for (int j = 0; j < 4; ++j) lds_v2f64(box + aoff[j], af[2 * j], af[2 * j + 1]);
+#pragma unroll
+          for (int ni = 0; ni < 4; ++ni) dmma_16816(acc[mi][ni], af, bf[ni]);
+        }
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[s]);
@@ -312,30 +350,35 @@ dgemm_update_kernel(const __grid_constant__ CUtensorMap tmap, double* __restrict
     if (!ok) break;
 
     // Epilogue: C -= acc; element pairs (row, row+1) are contiguous in a column.
+    // Per n8 block the eight 16-byte loads are issued before any store, so a
+    // thread pays one memory round trip per block instead of one per pair.
     const int ts = d.ts;
 #pragma unroll
     for (int ni = 0; ni < 4; ++ni) {
+      double* ptr[2][4];
+      double cv[2][4][2];
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int nl = nb * BN + wn * 32 + (ni >> 1) * 16 + perm_b(2 * t + 8 * (ni & 1)) + h;
-        if (nl >= d.N) continue;
         const int gj = d.c_col0 + nl;
         const int tj = gj / ts, lc = gj - tj * ts;
 #pragma unroll
         for (int mi = 0; mi < 4; ++mi) {
           const int ml = mb * BM + wm * 64 + mi * 16 + row_in_box;
-          if (ml >= d.M) continue;
           const int gi = d.c_row0 + ml;
           const int ti = gi / ts, lr = gi - ti * ts;
-          if (ti < tj) continue;
-          double2* p = reinterpret_cast<double2*>(tiles + tile_slot(ti, tj, d.nt) * (long long)ts * ts +
-                                                  (long long)lc * ts + lr);
-          double2 v = *p;
-          v.x -= acc[mi][ni][h];
-          v.y -= acc[mi][ni][2 + h];
-          *p = v;
+          const bool ok_el = nl < d.N && ml < d.M && ti >= tj;
+          ptr[h][mi] = ok_el ? tiles + tile_slot(ti, tj, d.nt) * (long long)ts * ts + (long long)lc * ts + lr
+                             : nullptr;
+          if (ok_el) ldg_v2f64(ptr[h][mi], cv[h][mi][0], cv[h][mi][1]);
         }
       }
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+          if (ptr[h][mi])
+            stg_v2f64(ptr[h][mi], cv[h][mi][0] - acc[mi][ni][h], cv[h][mi][1] - acc[mi][ni][2 + h]);
     }
   }
   // Drain: every stage this CTA issued must have landed before it exits.

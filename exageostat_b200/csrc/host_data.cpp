@@ -19,7 +19,7 @@
 #include <cstdint>
 #include <cstdlib>
 #include <vector>
-#include "../../include/exageostat_b200.h"
+#include "exageostat_b200.h"
 
 namespace {
 

@@ -22,45 +22,87 @@ namespace egs {
 constexpr int kNB = 64;  // inner block width of the panel factorisation
 
 // ---------------------------------------------------------------------------
-// Unblocked Cholesky of the 64x64 diagonal block at (off, off) of one tile.
-// info records the 1-based global column of the first non-positive pivot.
+// Cholesky of the 64x64 diagonal block at (off, off) of one tile, two warps.
+// The block is split 2 x 2 into 32 x 32 blocks: warp 0 factors A11 in
+// registers (lane = row, pivots and column entries exchanged by shuffles),
+// warp 1 solves A21 := A21 L11^-T, updates A22 -= L21 L21^T and factors A22 the
+// same way.  info records the 1-based global column of the first pivot that is
+// not positive (or NaN).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256)
-potrf_diag_block_kernel(double* __restrict__ tiles, int ts, long long slot, int off, int col_base,
-                        int* __restrict__ info) {
-  __shared__ double S[kNB][kNB + 1];
-  double* T = tiles + slot * (long long)ts * ts;
-  const int tid = threadIdx.x;
-  for (int e = tid; e < kNB * kNB; e += blockDim.x) {
-    const int r = e % kNB, c = e / kNB;
-    if (r >= c) S[r][c] = T[(long long)(off + c) * ts + off + r];
-  }
-  __syncthreads();
-  const int r = tid % kNB;
-  const int cg = tid / kNB;  // 4 column groups
-  for (int j = 0; j < kNB; ++j) {
-    const double d = S[j][j];
+__device__ __forceinline__ void warp_potrf32(double (&a)[32], int lane, int col_base, int* info) {
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    const double d = __shfl_sync(0xffffffffu, a[j], j);
+    if (lane == 0 && !(d > 0.0)) atomicCAS(info, 0, col_base + j + 1);
     const double ljj = sqrt(d);
     const double inv = 1.0 / ljj;
-    __syncthreads();
-    if (tid > j && tid < kNB) S[tid][j] *= inv;
-    if (tid == 0) {
-      S[j][j] = ljj;
-      if (!(d > 0.0)) atomicCAS(info, 0, col_base + off + j + 1);
+    if (lane == j) a[j] = ljj;
+    else if (lane > j) a[j] *= inv;
+#pragma unroll
+    for (int c = j + 1; c < 32; ++c) {
+      const double lcj = __shfl_sync(0xffffffffu, a[j], c);
+      if (lane >= c) a[c] = fma(-a[j], lcj, a[c]);
     }
-    __syncthreads();
-    for (int c = j + 1 + cg; c <= r; c += 4) S[r][c] = fma(-S[r][j], S[c][j], S[r][c]);
-    __syncthreads();
   }
-  for (int e = tid; e < kNB * kNB; e += blockDim.x) {
-    const int rr = e % kNB, c = e / kNB;
-    if (rr >= c) T[(long long)(off + c) * ts + off + rr] = S[rr][c];
+}
+
+__global__ void __launch_bounds__(64)
+potrf_diag_block_kernel(double* __restrict__ tiles, int ts, long long slot, int off, int col_base,
+                        int* __restrict__ info) {
+  __shared__ double L11[32][33];
+  __shared__ double L21[32][33];
+  double* T = tiles + slot * (long long)ts * ts + (long long)off * ts + off;  // block origin, ld = ts
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gcol = col_base + off;
+  double a[32];
+  if (warp == 0) {
+#pragma unroll
+    for (int c = 0; c < 32; ++c) a[c] = (lane >= c) ? T[(long long)c * ts + lane] : 0.0;
+    warp_potrf32(a, lane, gcol, info);
+#pragma unroll
+    for (int c = 0; c < 32; ++c) {
+      L11[lane][c] = a[c];
+      if (lane >= c) T[(long long)c * ts + lane] = a[c];
+    }
+  } else {
+    // row 32 + lane, columns 0..31 of A21
+#pragma unroll
+    for (int c = 0; c < 32; ++c) a[c] = T[(long long)c * ts + 32 + lane];
+  }
+  __syncthreads();
+  if (warp == 1) {
+    // A21 := A21 L11^-T (row solve, L11 broadcast from shared memory)
+#pragma unroll
+    for (int c = 0; c < 32; ++c) {
+      double s = a[c];
+#pragma unroll
+      for (int q = 0; q < c; ++q) s = fma(-a[q], L11[c][q], s);
+      a[c] = s / L11[c][c];
+      L21[lane][c] = a[c];
+      T[(long long)c * ts + 32 + lane] = a[c];
+    }
+    __syncwarp();
+    // A22 -= L21 L21^T on the lower part (both factors read back from shared
+    // memory so the row registers can be reused), then factor A22.
+#pragma unroll
+    for (int c = 0; c < 32; ++c) {
+      double v = (lane >= c) ? T[(long long)(32 + c) * ts + 32 + lane] : 0.0;
+      if (lane >= c) {
+#pragma unroll 8
+        for (int q = 0; q < 32; ++q) v = fma(-L21[lane][q], L21[c][q], v);
+      }
+      a[c] = v;
+    }
+    warp_potrf32(a, lane, gcol + 32, info);
+#pragma unroll
+    for (int c = 0; c < 32; ++c)
+      if (lane >= c) T[(long long)(32 + c) * ts + 32 + lane] = a[c];
   }
 }
 
 void launch_potrf_diag_block(double* tiles, int ts, long long slot, int off, int col_base, int* info,
                              cudaStream_t st) {
-  potrf_diag_block_kernel<<<1, 256, 0, st>>>(tiles, ts, slot, off, col_base, info);
+  potrf_diag_block_kernel<<<1, 64, 0, st>>>(tiles, ts, slot, off, col_base, info);
 }
 
 // ---------------------------------------------------------------------------
@@ -119,7 +161,7 @@ void launch_trsm_rows(double* tiles, int ts, long long slot0, int ntiles, int ro
 // ---------------------------------------------------------------------------
 // Forward substitution on one diagonal tile: z_k := L_kk^-1 z_k.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(1024)
 trsv_diag_kernel(const double* __restrict__ tiles, int ts, long long slot, double* __restrict__ zk) {
   extern __shared__ double zs[];  // ts
   __shared__ double B[kNB][kNB + 1];
@@ -151,11 +193,16 @@ trsv_diag_kernel(const double* __restrict__ tiles, int ts, long long slot, doubl
     }
     __syncthreads();
     for (int r = kb + kNB + tid; r < ts; r += blockDim.x) {
-      double acc = 0.0;
       const double* col = T + (long long)kb * ts + r;
-#pragma unroll 8
-      for (int c = 0; c < kNB; ++c) acc = fma(col[(long long)c * ts], zs[kb + c], acc);
-      zs[r] -= acc;
+      double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
+#pragma unroll 4
+      for (int c = 0; c < kNB; c += 4) {
+        acc0 = fma(col[(long long)c * ts], zs[kb + c], acc0);
+        acc1 = fma(col[(long long)(c + 1) * ts], zs[kb + c + 1], acc1);
+        acc2 = fma(col[(long long)(c + 2) * ts], zs[kb + c + 2], acc2);
+        acc3 = fma(col[(long long)(c + 3) * ts], zs[kb + c + 3], acc3);
+      }
+      zs[r] -= (acc0 + acc1) + (acc2 + acc3);
     }
     __syncthreads();
   }
@@ -163,7 +210,7 @@ trsv_diag_kernel(const double* __restrict__ tiles, int ts, long long slot, doubl
 }
 
 void launch_trsv_diag(const double* tiles, int ts, long long slot, double* zk, cudaStream_t st) {
-  trsv_diag_kernel<<<1, 256, ts * sizeof(double), st>>>(tiles, ts, slot, zk);
+  trsv_diag_kernel<<<1, 1024, ts * sizeof(double), st>>>(tiles, ts, slot, zk);
 }
 
 // z_i -= L_ik z_k for every tile row i > k.  256 threads = 64 rows x 4 column groups.
