@@ -56,6 +56,9 @@ SIGNATURES = {
     "egs_generate_locations": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _D, _D]),
     "egs_dlarnv_normal": (ctypes.c_int, [_I, ctypes.c_int, _D]),
     "egs_generate_observations": (ctypes.c_int, [_P, _D, ctypes.c_int, _D]),
+    "egs_mle_noalloc_workspace": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _LL]),
+    "egs_mle_eval_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _P, _P, _P, _D, _P, ctypes.c_longlong, _D,
+                                            _P]),
     "egs_problem_set_profiling": (ctypes.c_int, [_P, ctypes.c_int]),
     "egs_problem_stage_stats": (ctypes.c_int, [_P, _D, _D, _LL]),
     "egs_matern_block": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P, _P, _P, _D,

@@ -547,6 +547,166 @@ int egs_generate_observations(egs_problem* p, const double* theta, int seed, dou
   return EGS_OK;
 }
 
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Evaluation without allocation.
+//
+// Some callers cannot call cudaMalloc: a host application whose device memory
+// is owned by another allocator (a framework's caching allocator, or a pool
+// sized once at start-up), where an extra cudaMalloc would go around that
+// budget, and latency-bound loops such as an optimizer driving thousands of
+// evaluations, where cudaMalloc / cudaFree would add device-wide
+// synchronisation to every call.  egs_mle_eval_noalloc takes every large buffer
+// from the caller and keeps the small per-call state (log-determinant partial
+// sums, the result record, the status flags and the Matern parameters) in the
+// file-scope device array below, which every GPU that loads this library holds
+// until the process exits.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kNoAllocMaxTileRows = 4096;  // n <= 4096 * device tile size
+constexpr size_t kNoAllocPartialOff = 0;
+constexpr size_t kNoAllocResultOff = kNoAllocPartialOff + kNoAllocMaxTileRows * sizeof(double);
+constexpr size_t kNoAllocFlagsOff = kNoAllocResultOff + 4 * sizeof(double);
+constexpr size_t kNoAllocParamsOff = kNoAllocFlagsOff + 256;
+constexpr size_t kNoAllocScratchBytes = kNoAllocParamsOff + 256;
+constexpr int kNoAllocMaxDevices = 64;
+
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+
+std::mutex g_noalloc_mutex;
+unsigned char* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device, looked up once per
+// device (the host-side symbol is only a stand-in and must not reach a kernel).
+int noalloc_scratch(unsigned char** out) {
+  int dev = 0;
+  EGS_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices) {
+    set_last_error("device ordinal beyond the supported range", "egs_mle_eval_noalloc");
+    return EGS_ERR_INVALID;
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_addr[dev]) {
+    void* ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess || !ptr) {
+      cudaGetLastError();
+      set_last_error(cudaGetErrorString(e), "cudaGetSymbolAddress(g_noalloc_scratch)");
+      return EGS_ERR_CUDA;
+    }
+    g_noalloc_addr[dev] = static_cast<unsigned char*>(ptr);
+  }
+  *out = g_noalloc_addr[dev];
+  return EGS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int egs_mle_noalloc_workspace(int n, int dts, long long* doubles) {
+  if (n <= 0 || dts <= 0 || !doubles) return EGS_ERR_INVALID;
+  const int ts = round_tile(dts);
+  const int nt = (n + ts - 1) / ts;
+  if (nt > kNoAllocMaxTileRows) {
+    set_last_error("n exceeds 4096 device tiles, the limit of the allocation-free evaluation",
+                   "egs_mle_noalloc_workspace");
+    return EGS_ERR_INVALID;
+  }
+  const long long np = (long long)nt * ts;
+  *doubles = lower_tiles(nt) * (long long)ts * ts + 3 * np;
+  return EGS_OK;
+}
+
+int egs_mle_eval_noalloc(int n, int dts, const double* x, const double* y, const double* z, const double* theta,
+                         double* work, long long work_doubles, double* loglik, void* cuda_stream) {
+  if (n <= 0 || dts <= 0 || !x || !y || !z || !theta || !work || !loglik) return EGS_ERR_INVALID;
+  long long need = 0;
+  int rc = egs_mle_noalloc_workspace(n, dts, &need);
+  if (rc != EGS_OK) return rc;
+  if (work_doubles < need) {
+    set_last_error("workspace smaller than egs_mle_noalloc_workspace requires", "egs_mle_eval_noalloc");
+    return EGS_ERR_INVALID;
+  }
+  if (((uintptr_t)work & 15) != 0) {
+    set_last_error("workspace must be 16-byte aligned", "egs_mle_eval_noalloc");
+    return EGS_ERR_INVALID;
+  }
+  MaternParams mp;
+  if ((rc = make_matern_params(theta, &mp)) != EGS_OK) {
+    set_last_error("theta outside the Matern domain (sigma2 > 0, beta > 0, nu > 0)", "egs_mle_eval_noalloc");
+    return rc;
+  }
+  unsigned char* scratch = nullptr;
+  if ((rc = noalloc_scratch(&scratch)) != EGS_OK) return rc;
+  double* partial = reinterpret_cast<double*>(scratch + kNoAllocPartialOff);
+  double* result = reinterpret_cast<double*>(scratch + kNoAllocResultOff);
+  int* flags = reinterpret_cast<int*>(scratch + kNoAllocFlagsOff);
+  MaternParams* dparams = reinterpret_cast<MaternParams*>(scratch + kNoAllocParamsOff);
+
+  // A problem record on the stack that points at the caller's workspace and the
+  // static scratch; it owns nothing.
+  egs_problem q;
+  q.n = n;
+  q.dts = dts;
+  q.ts = round_tile(dts);
+  q.nt = (n + q.ts - 1) / q.ts;
+  q.np = q.nt * q.ts;
+  q.ntiles = lower_tiles(q.nt);
+  q.tiles = work;
+  q.x = work + q.ntiles * (long long)q.ts * q.ts;
+  q.y = q.x + q.np;
+  q.z = q.y + q.np;
+  q.partial = partial;
+  q.result = result;
+  q.flags = flags;
+  q.dparams = dparams;
+  q.stream = (cudaStream_t)cuda_stream;
+  q.own_stream = false;
+  if ((rc = gemm_init_tensor_map(q.tmap, q.tiles, q.ts, q.ntiles)) != EGS_OK) return rc;
+
+  cudaStream_t st = q.stream;
+  const size_t pad = (size_t)(q.np - n) * sizeof(double);
+  EGS_CUDA_TRY(cudaMemcpyAsync(dparams, &mp, sizeof(MaternParams), cudaMemcpyHostToDevice, st));
+  EGS_CUDA_TRY(cudaMemsetAsync(flags, 0, 2 * sizeof(int), st));
+  EGS_CUDA_TRY(cudaMemcpyAsync(q.x, x, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  EGS_CUDA_TRY(cudaMemcpyAsync(q.y, y, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  EGS_CUDA_TRY(cudaMemcpyAsync(q.z, z, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  if (pad) {
+    EGS_CUDA_TRY(cudaMemsetAsync(q.x + n, 0, pad, st));
+    EGS_CUDA_TRY(cudaMemsetAsync(q.y + n, 0, pad, st));
+    EGS_CUDA_TRY(cudaMemsetAsync(q.z + n, 0, pad, st));
+  }
+  if ((rc = launch_matern_tiles(q.tiles, q.x, q.y, n, q.ts, q.nt, dparams, st)) != EGS_OK)
+    return check_cuda("egs_mle_eval_noalloc/matern");
+  if ((rc = enqueue_potrf(&q)) != EGS_OK) return rc;
+  launch_logdet_partials(q.tiles, q.ts, q.nt, n, partial, st);
+  enqueue_trsv(&q);
+  launch_finalize(partial, q.nt, q.z, n, result, flags, st);
+  if ((rc = check_cuda("egs_mle_eval_noalloc")) != EGS_OK) return rc;
+  double hres[4];
+  int hflags[2];
+  EGS_CUDA_TRY(cudaMemcpyAsync(hflags, flags, sizeof(hflags), cudaMemcpyDeviceToHost, st));
+  EGS_CUDA_TRY(cudaMemcpyAsync(hres, result, sizeof(hres), cudaMemcpyDeviceToHost, st));
+  EGS_CUDA_TRY(cudaStreamSynchronize(st));
+  if (hflags[1] != 0) {
+    set_last_error("a device-side wait exceeded its limit", "egs_mle_eval_noalloc");
+    return EGS_ERR_TIMEOUT;
+  }
+  if (hflags[0] > 0) {
+    set_last_error("Matrix is not positive definite", "egs_mle_eval_noalloc");
+    return hflags[0];
+  }
+  *loglik = hres[0];
+  return EGS_OK;
+}
+
 int egs_problem_set_profiling(egs_problem* p, int enable) {
   if (!p) return EGS_ERR_INVALID;
   EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));

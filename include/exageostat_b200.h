@@ -140,6 +140,34 @@ EGS_API int egs_problem_set_profiling(egs_problem* p, int enable);
  * NULL or point to EGS_NUM_STAGES elements. */
 EGS_API int egs_problem_stage_stats(egs_problem* p, double* ms, double* flops, long long* launches);
 
+/* ---- evaluation without allocation ---------------------------------------- */
+
+/* No counterpart in the reference.  For callers that cannot call cudaMalloc --
+ * an application whose device memory belongs to another allocator (a
+ * framework's caching allocator, or a pool sized once at start-up) and loops
+ * that must not pay the device-wide synchronisation of cudaMalloc/cudaFree on
+ * every evaluation -- this pair evaluates one log-likelihood without allocating
+ * anything.  egs_mle_noalloc_workspace reports how many doubles of device
+ * workspace an evaluation of n points with tile dts needs (lower tiles plus
+ * three padded vectors); it rejects n above 4096 device tiles (4096 *
+ * round-up(dts, 64) points).
+ *
+ * egs_mle_eval_noalloc then runs the whole evaluation of egs_mle_eval on the
+ * caller's stream: x, y, z are n device doubles (read only), theta is host
+ * memory, work is the 16-byte aligned device workspace (overwritten), and the
+ * log-likelihood is written to the host double *loglik.  It calls no
+ * cudaMalloc, cudaFree or other allocating routine: its small per-call state
+ * lives in one static device array of about 33 KB that every GPU which loads
+ * the library keeps until the process exits.  The first call on a device looks
+ * up that array's device address, so make this first call before any stream
+ * capture.  All calls share the array: calls whose work overlaps on the GPU
+ * (other streams, other host threads) race on it and must be serialised by the
+ * caller. */
+EGS_API int egs_mle_noalloc_workspace(int n, int dts, long long* doubles);
+EGS_API int egs_mle_eval_noalloc(int n, int dts, const double* x, const double* y, const double* z,
+                                 const double* theta, double* work, long long work_doubles, double* loglik,
+                                 void* cuda_stream);
+
 /* ---- kernel plugin ------------------------------------------------------ */
 
 /* rows x cols column-major block (leading dimension lda) on caller device
