@@ -41,9 +41,21 @@ CONFIG = {
     "n": N_TOTAL - N_MISS, "tile": DTS, "theta": list(THETA), "precision": "fp64",
     "l2": "inputs larger than L2 (6.6 GB tile storage vs 126 MB L2); no flush",
 }
-# DRAM bytes per launch of the trailing-update kernel (ncu capture; see
-# profiles/dgemm_update_kernel_n40000.md).  None until a capture exists.
-UPDATE_TRAFFIC_BYTES_PER_LAUNCH = None
+# DRAM bytes per updated C element of the trailing-update kernel, from one ncu
+# capture of a full trailing update (N = 8,000, tile 960: 571 MB for 1,830
+# 128 x 128 blocks; profiles/dgemm_update_kernel_n8000.md).  The per-launch
+# traffic of this workload is that figure times each launch's block count.
+UPDATE_DRAM_BYTES_PER_C_ELEMENT = 571.28e6 / (1830 * 128 * 128)
+
+
+def update_traffic_per_launch(n: int, ts: int) -> float:
+    """Mean DRAM bytes of one trailing-update launch at (n, ts), scaled from the capture."""
+    nt = -(-n // ts)
+    per = []
+    for k in range(nt - 1):
+        mb = -(-((nt - k - 1) * ts) // 128)
+        per.append(mb * (mb + 1) // 2 * 128 * 128 * UPDATE_DRAM_BYTES_PER_C_ELEMENT)
+    return sum(per) / max(len(per), 1)
 
 
 def env_rank():
@@ -321,7 +333,9 @@ def main():
             "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
             "frac": (achieved / peak) if achieved else None,
             "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor; MEASURED_PEAKS.json has no FP64 entry)",
-            "traffic": UPDATE_TRAFFIC_BYTES_PER_LAUNCH,
+            "traffic": update_traffic_per_launch(n, DTS),
+            "traffic_note": "DRAM bytes per launch: 19.0 B per updated C element (ncu, N=8000 trailing update) "
+                            "times the mean block count of this workload's launches",
             "launches": n_up,
             "flops_per_launch": stage_flops[up] / max(n_up, 1)}
     eval_flops = n ** 3 / 3.0 + n ** 2 / 2.0 + n / 6.0 + n ** 2

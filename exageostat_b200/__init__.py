@@ -41,6 +41,7 @@ SIGNATURES = {
     "egs_problem_destroy": (ctypes.c_int, [_P]),
     "egs_problem_info": (ctypes.c_int, [_P, _I, _I, _I, _LL]),
     "egs_problem_set_stream": (ctypes.c_int, [_P, _P]),
+    "egs_problem_set_band": (ctypes.c_int, [_P, ctypes.c_int]),
     "egs_problem_set_locations": (ctypes.c_int, [_P, _D, _D]),
     "egs_problem_set_locations_device": (ctypes.c_int, [_P, _P, _P]),
     "egs_problem_set_observations": (ctypes.c_int, [_P, _D]),
@@ -67,6 +68,10 @@ SIGNATURES = {
     "egs_predict_host": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _D, _D, _D,
                                         _D, _D]),
 }
+
+OBJECTIVE = ctypes.CFUNCTYPE(ctypes.c_double, ctypes.c_int, _D, ctypes.c_void_p)
+SIGNATURES["egs_bobyqa_maximize"] = (ctypes.c_int, [ctypes.c_int, _D, _D, _D, ctypes.c_double, ctypes.c_double,
+                                                    ctypes.c_int, OBJECTIVE, ctypes.c_void_p, _D, _I])
 
 _lib = None
 
@@ -140,6 +145,10 @@ class Problem:
             self.close()
         except Exception:
             pass
+
+    def set_band(self, band: int) -> None:
+        """0: exact dense Cholesky; >= 1: diagonal super-tile approximation with this band."""
+        _check(self._lib.egs_problem_set_band(self._h, int(band)), "set_band")
 
     def set_locations(self, x, y) -> None:
         x, y = _f64(x), _f64(y)
@@ -260,3 +269,27 @@ def dlarnv_normal(seed: int, n: int) -> np.ndarray:
     out = np.empty(n)
     _check(lib.egs_dlarnv_normal(iseed, int(n), _dptr(out)), "dlarnv_normal")
     return out
+
+
+def bobyqa_maximize(f, x0, lb, ub, ftol_abs: float, maxeval: int, rhobeg: float = 0.0):
+    """Maximise f(theta) over the box with the library's BOBYQA; returns (theta, fbest, nevals)."""
+    lib = load_library()
+    x = _f64(x0).copy()
+    lo, hi = _f64(lb), _f64(ub)
+    err = []
+
+    def cb(n, xp, ctx):
+        try:
+            return float(f(np.ctypeslib.as_array(xp, shape=(n,)).copy()))
+        except Exception as exc:  # keep the exception for the caller; stop improving
+            err.append(exc)
+            return float("-inf")
+
+    fn = OBJECTIVE(cb)
+    fb = ctypes.c_double()
+    ne = ctypes.c_int()
+    _check(lib.egs_bobyqa_maximize(len(x), _dptr(x), _dptr(lo), _dptr(hi), float(rhobeg), float(ftol_abs),
+                                   int(maxeval), fn, None, ctypes.byref(fb), ctypes.byref(ne)), "bobyqa_maximize")
+    if err:
+        raise err[0]
+    return x, fb.value, ne.value

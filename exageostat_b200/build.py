@@ -18,7 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libexageostat_b200.so")
 
-SOURCES = ["matern.cu", "potrf.cu", "dgemm_tma.cu", "capi.cu", "host_data.cpp"]
+SOURCES = ["matern.cu", "potrf.cu", "dgemm_tma.cu", "capi.cu", "host_data.cpp", "host_bobyqa.cpp"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -61,5 +61,24 @@ def build(verbose: bool = False) -> str:
     return LIB
 
 
+HOST_INCLUDE = os.path.join(HERE, "host", "include")
+HOST_SOURCES = [os.path.join(HERE, "host", "src", "Configurations.cpp")]
+API_TEST_SRC = os.path.join(ROOT, "tests", "cpp", "test_exageostat_api.cpp")
+API_TEST_BIN = os.path.join(ROOT, "tests", "cpp", "_build", "test_exageostat_api")
+
+
+def build_host_tests() -> str:
+    """Compile the C++ API test driver against the host headers and the library."""
+    os.makedirs(os.path.dirname(API_TEST_BIN), exist_ok=True)
+    cmd = [nvcc(), "-std=c++17", "-O2", "-x", "c++", "-I", HOST_INCLUDE, "-I", os.path.join(ROOT, "include"),
+           *HOST_SOURCES, API_TEST_SRC, "-L", HERE, "-lexageostat_b200",
+           "-Xlinker", "-rpath", "-Xlinker", "$ORIGIN/../../../exageostat_b200", "-o", API_TEST_BIN]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"host API test build failed:\n{res.stdout}\n{res.stderr}")
+    return API_TEST_BIN
+
+
 if __name__ == "__main__":
     print(build(verbose="-v" in sys.argv))
+    print(build_host_tests())

@@ -54,6 +54,7 @@ struct egs_problem {
   bool own_stream = false;
   bool have_locations = false;
   bool have_observations = false;
+  int band = 0;  // >= 1: diagonal super-tile approximation with this tile band
   // Per-stage accounting: launch counts always, CUDA-event times when profiling.
   bool profiling = false;
   struct Span {
@@ -223,6 +224,69 @@ int enqueue_potrf(egs_problem* p) {
   return check_cuda("enqueue_potrf");
 }
 
+// Diagonal super-tile (band) approximation of the factorisation, following
+// ChameleonDST<T>::ExaGeoStatParallelPotrfDiagonal (src/linear-algebra-solvers/
+// concrete/chameleon/dst/ChameleonDST.cpp:90-150): at step k only tiles (m, k)
+// with m < k + band are solved, and only tiles (m, n) with k < n < k + band,
+// n <= m < n + band are updated; the update reads tile (m, k) whether or not it
+// was solved, and tiles outside the band keep their covariance values.
+int enqueue_potrf_band(egs_problem* p) {
+  const int ts = p->ts, nt = p->nt, n = p->n, band = p->band;
+  cudaStream_t st = p->stream;
+  int* info = p->flags;
+  int* err = p->flags + 1;
+  for (int k = 0; k < nt; ++k) {
+    const long long skk = tile_slot(k, k, nt);
+    int sp = span_begin(p, EGS_STAGE_PANEL);
+    for (int kb = 0; kb < ts; kb += kInnerBlock) {
+      launch_potrf_diag_block(p->tiles, ts, skk, kb, k * ts, info, st);
+      count_launches(p, EGS_STAGE_PANEL, 1);
+      if (kb + kInnerBlock < ts) {
+        launch_trsm_rows(p->tiles, ts, skk, 1, kb + kInnerBlock, kb, skk, st);
+        const int r0 = k * ts + kb + kInnerBlock;
+        const int m = ts - kb - kInnerBlock;
+        int rc = launch_gemm_rows(p->tmap, p->tiles, ts, nt, m, m, kInnerBlock, r0, kb, k, r0, kb, k, r0, r0, 1,
+                                  err, st);
+        if (rc != EGS_OK) return rc;
+        count_launches(p, EGS_STAGE_PANEL, 2);
+      }
+    }
+    const int mend = std::min(nt, k + band);  // solved tiles: k < m < mend
+    const int ntl = mend - k - 1;
+    if (ntl > 0) {
+      const long long s0 = tile_slot(k + 1, k, nt);
+      for (int kb = 0; kb < ts; kb += kInnerBlock) {
+        launch_trsm_rows(p->tiles, ts, s0, ntl, 0, kb, skk, st);
+        count_launches(p, EGS_STAGE_PANEL, 1);
+        if (kb + kInnerBlock < ts) {
+          const int ncols = ts - kb - kInnerBlock;
+          const int brow = k * ts + kb + kInnerBlock;
+          int rc = launch_gemm_rows(p->tmap, p->tiles, ts, nt, ntl * ts, ncols, kInnerBlock, (k + 1) * ts, kb, k,
+                                    brow, kb, k, (k + 1) * ts, brow, 0, err, st);
+          if (rc != EGS_OK) return rc;
+          count_launches(p, EGS_STAGE_PANEL, 1);
+        }
+      }
+    }
+    span_end(p, sp, 0.0);
+    sp = span_begin(p, EGS_STAGE_UPDATE);
+    double flops = 0.0;
+    for (int c = k + 1; c < mend; ++c) {
+      // tiles (m, c), c <= m < min(nt, c + band): one launch on the global rows of that range
+      const int rows = (std::min(nt, c + band) - c) * ts;
+      int rc = launch_gemm_rows(p->tmap, p->tiles, ts, nt, rows, ts, ts, c * ts, 0, k, c * ts, 0, k, c * ts, c * ts,
+                                1, err, st);
+      if (rc != EGS_OK) return rc;
+      count_launches(p, EGS_STAGE_UPDATE, 1);
+      const double rr = (double)std::max(0, std::min(n, std::min(nt, c + band) * ts) - c * ts);
+      const double cc = (double)std::max(0, std::min(n, (c + 1) * ts) - c * ts);
+      flops += 2.0 * rr * cc * ts - cc * (cc - 1.0) * ts;
+    }
+    span_end(p, sp, flops);
+  }
+  return check_cuda("enqueue_potrf_band");
+}
+
 // Z := L^-1 Z, tile by tile (forward substitution).
 void enqueue_trsv(egs_problem* p) {
   const int sp = span_begin(p, EGS_STAGE_SOLVE);
@@ -378,6 +442,18 @@ int egs_problem_info(const egs_problem* p, int* n, int* ts, int* nt, long long* 
   return EGS_OK;
 }
 
+int egs_problem_set_band(egs_problem* p, int band) {
+  if (!p || band < 0) return EGS_ERR_INVALID;
+  if (band > 0 && p->dts != p->ts) {
+    // The approximation is defined on the caller's tiles; merging them into a
+    // larger device tile would change the result.
+    set_last_error("the band approximation needs a tile size that is a multiple of 64", "egs_problem_set_band");
+    return EGS_ERR_INVALID;
+  }
+  p->band = band;
+  return EGS_OK;
+}
+
 int egs_problem_set_stream(egs_problem* p, void* cuda_stream) {
   if (!p) return EGS_ERR_INVALID;
   EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
@@ -436,7 +512,7 @@ int egs_covariance_generate(egs_problem* p, const double* theta) {
 int egs_potrf(egs_problem* p) {
   if (!p) return EGS_ERR_INVALID;
   EGS_CUDA_TRY(cudaMemsetAsync(p->flags, 0, 2 * sizeof(int), p->stream));
-  int rc = enqueue_potrf(p);
+  int rc = p->band > 0 ? enqueue_potrf_band(p) : enqueue_potrf(p);
   if (rc != EGS_OK) return rc;
   return sync_flags(p, false);
 }
@@ -501,7 +577,7 @@ int egs_mle_eval(egs_problem* p, const double* theta, double* loglik, double* lo
   if (rc != EGS_OK) return check_cuda("matern");
   count_launches(p, EGS_STAGE_GENERATE, (lower_tiles(p->nt) + 65534) / 65535);
   span_end(p, sp, 0.0);
-  rc = enqueue_potrf(p);
+  rc = p->band > 0 ? enqueue_potrf_band(p) : enqueue_potrf(p);
   if (rc != EGS_OK) return rc;
   sp = span_begin(p, EGS_STAGE_REDUCE);
   launch_logdet_partials(p->tiles, p->ts, p->nt, p->n, p->partial, st);

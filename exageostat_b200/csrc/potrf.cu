@@ -22,87 +22,56 @@ namespace egs {
 constexpr int kNB = 64;  // inner block width of the panel factorisation
 
 // ---------------------------------------------------------------------------
-// Cholesky of the 64x64 diagonal block at (off, off) of one tile, two warps.
-// The block is split 2 x 2 into 32 x 32 blocks: warp 0 factors A11 in
-// registers (lane = row, pivots and column entries exchanged by shuffles),
-// warp 1 solves A21 := A21 L11^-T, updates A22 -= L21 L21^T and factors A22 the
-// same way.  info records the 1-based global column of the first pivot that is
-// not positive (or NaN).
+// Cholesky of the 64x64 diagonal block at (off, off) of one tile by one warp.
+// The block sits in shared memory; lane l owns rows l and l + 32.  Step j:
+// every lane reads the pivot (a broadcast), scales its entries of column j, and
+// applies the rank-1 update to its rows, reading L[c][j] as broadcasts.  Only
+// __syncwarp separates the steps.  info records the 1-based global column of
+// the first pivot that is not positive (or NaN).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void warp_potrf32(double (&a)[32], int lane, int col_base, int* info) {
-#pragma unroll
-  for (int j = 0; j < 32; ++j) {
-    const double d = __shfl_sync(0xffffffffu, a[j], j);
-    if (lane == 0 && !(d > 0.0)) atomicCAS(info, 0, col_base + j + 1);
-    const double ljj = sqrt(d);
-    const double inv = 1.0 / ljj;
-    if (lane == j) a[j] = ljj;
-    else if (lane > j) a[j] *= inv;
-#pragma unroll
-    for (int c = j + 1; c < 32; ++c) {
-      const double lcj = __shfl_sync(0xffffffffu, a[j], c);
-      if (lane >= c) a[c] = fma(-a[j], lcj, a[c]);
-    }
-  }
-}
-
-__global__ void __launch_bounds__(64)
+__global__ void __launch_bounds__(32)
 potrf_diag_block_kernel(double* __restrict__ tiles, int ts, long long slot, int off, int col_base,
                         int* __restrict__ info) {
-  __shared__ double L11[32][33];
-  __shared__ double L21[32][33];
+  __shared__ double S[kNB][kNB + 1];
   double* T = tiles + slot * (long long)ts * ts + (long long)off * ts + off;  // block origin, ld = ts
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int gcol = col_base + off;
-  double a[32];
-  if (warp == 0) {
-#pragma unroll
-    for (int c = 0; c < 32; ++c) a[c] = (lane >= c) ? T[(long long)c * ts + lane] : 0.0;
-    warp_potrf32(a, lane, gcol, info);
-#pragma unroll
-    for (int c = 0; c < 32; ++c) {
-      L11[lane][c] = a[c];
-      if (lane >= c) T[(long long)c * ts + lane] = a[c];
-    }
-  } else {
-    // row 32 + lane, columns 0..31 of A21
-#pragma unroll
-    for (int c = 0; c < 32; ++c) a[c] = T[(long long)c * ts + 32 + lane];
+  const int lane = threadIdx.x;
+  for (int c = 0; c < kNB; ++c) {
+    S[lane][c] = (lane >= c) ? T[(long long)c * ts + lane] : 0.0;
+    S[lane + 32][c] = T[(long long)c * ts + lane + 32];
   }
-  __syncthreads();
-  if (warp == 1) {
-    // A21 := A21 L11^-T (row solve, L11 broadcast from shared memory)
-#pragma unroll
-    for (int c = 0; c < 32; ++c) {
-      double s = a[c];
-#pragma unroll
-      for (int q = 0; q < c; ++q) s = fma(-a[q], L11[c][q], s);
-      a[c] = s / L11[c][c];
-      L21[lane][c] = a[c];
-      T[(long long)c * ts + 32 + lane] = a[c];
+  __syncwarp();
+  const int r0 = lane, r1 = lane + 32;
+  for (int j = 0; j < kNB; ++j) {
+    const double d = S[j][j];
+    if (lane == 0 && !(d > 0.0)) atomicCAS(info, 0, col_base + off + j + 1);
+    const double ljj = sqrt(d);
+    const double inv = 1.0 / ljj;
+    const double l0 = (r0 > j) ? S[r0][j] * inv : 0.0;
+    const double l1 = (r1 > j) ? S[r1][j] * inv : 0.0;
+    __syncwarp();
+    if (r0 > j) S[r0][j] = l0;
+    if (r1 > j) S[r1][j] = l1;
+    if (r0 == j) S[r0][j] = ljj;
+    if (r1 == j) S[r1][j] = ljj;
+    __syncwarp();
+    // Independent columns: unrolled so their shared-memory latencies overlap.
+#pragma unroll 8
+    for (int c = j + 1; c < kNB; ++c) {
+      const double lcj = S[c][j];
+      if (r0 >= c) S[r0][c] = fma(-l0, lcj, S[r0][c]);
+      if (r1 >= c) S[r1][c] = fma(-l1, lcj, S[r1][c]);
     }
     __syncwarp();
-    // A22 -= L21 L21^T on the lower part (both factors read back from shared
-    // memory so the row registers can be reused), then factor A22.
-#pragma unroll
-    for (int c = 0; c < 32; ++c) {
-      double v = (lane >= c) ? T[(long long)(32 + c) * ts + 32 + lane] : 0.0;
-      if (lane >= c) {
-#pragma unroll 8
-        for (int q = 0; q < 32; ++q) v = fma(-L21[lane][q], L21[c][q], v);
-      }
-      a[c] = v;
-    }
-    warp_potrf32(a, lane, gcol + 32, info);
-#pragma unroll
-    for (int c = 0; c < 32; ++c)
-      if (lane >= c) T[(long long)(32 + c) * ts + 32 + lane] = a[c];
+  }
+  for (int c = 0; c < kNB; ++c) {
+    if (lane >= c) T[(long long)c * ts + lane] = S[lane][c];
+    T[(long long)c * ts + lane + 32] = S[lane + 32][c];
   }
 }
 
 void launch_potrf_diag_block(double* tiles, int ts, long long slot, int off, int col_base, int* info,
                              cudaStream_t st) {
-  potrf_diag_block_kernel<<<1, 64, 0, st>>>(tiles, ts, slot, off, col_base, info);
+  potrf_diag_block_kernel<<<1, 32, 0, st>>>(tiles, ts, slot, off, col_base, info);
 }
 
 // ---------------------------------------------------------------------------

@@ -1,0 +1,96 @@
+// Non-template parts of Configurations (src/configurations/Configurations.cpp,
+// Parser.cpp:23-81, Validator.cpp:209-255 for the theta strings).
+#include "configurations/Configurations.hpp"
+
+#include <cctype>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+
+#include "kernels/Kernel.hpp"
+
+namespace exageostat::configurations {
+
+void Configurations::InitTheta(std::vector<double>& aTheta, int size) {
+  if (aTheta.empty()) {
+    for (int i = 0; i < size; i++) aTheta.push_back(-1);
+  } else if ((int)aTheta.size() < size) {
+    for (int i = (int)aTheta.size(); i < size; i++) aTheta.push_back(0);
+  }
+}
+
+void Configurations::InitializeAllTheta() {
+  if (mIsThetaInit) return;
+  int np = kernels::KernelsConfigurations::GetParametersNumberKernelMap()[GetKernelName()];
+  if (np <= 0) np = 3;
+  InitTheta(mInitialTheta, np);
+  InitTheta(mLowerBounds, np);
+  InitTheta(mUpperBounds, np);
+  mStartingTheta = mLowerBounds;
+  InitTheta(mEstimatedTheta, np);
+  for (int i = 0; i < np; i++) {
+    if (mEstimatedTheta[i] != -1) {
+      mLowerBounds[i] = mEstimatedTheta[i];
+      mUpperBounds[i] = mEstimatedTheta[i];
+      mStartingTheta[i] = mEstimatedTheta[i];
+    }
+  }
+  mIsThetaInit = true;
+}
+
+namespace {
+
+std::string normalise_key(const std::string& key) {
+  std::string out;
+  for (char c : key)
+    if (std::isalnum((unsigned char)c)) out += (char)std::tolower((unsigned char)c);
+  return out;
+}
+
+std::vector<double> parse_theta(const std::string& v) {
+  std::vector<double> out;
+  std::stringstream ss(v);
+  std::string item;
+  while (std::getline(ss, item, ':')) out.push_back(item == "?" ? -1.0 : std::stod(item));
+  return out;
+}
+
+bool parse_bool(const std::string& v) { return v == "true" || v == "1" || v == "TRUE" || v == "True"; }
+
+}  // namespace
+
+void Configurations::InitializeArguments(const int& argc, char** argv) {
+  for (int i = 1; i < argc; ++i) {
+    std::string arg = argv[i];
+    if (arg.rfind("--", 0) != 0) continue;
+    arg = arg.substr(2);
+    const size_t eq = arg.find('=');
+    const std::string key = normalise_key(arg.substr(0, eq));
+    const std::string val = eq == std::string::npos ? "true" : arg.substr(eq + 1);
+    if (key == "n") SetProblemSize(std::stoi(val));
+    else if (key == "kernel") SetKernelName(val);
+    else if (key == "dts") SetDenseTileSize(std::stoi(val));
+    else if (key == "seed") SetSeed(std::stoi(val));
+    else if (key == "maxmleiterations") SetMaxMleIterations(std::stoi(val));
+    else if (key == "tolerance") SetTolerance(std::stod(val));
+    else if (key == "zmiss") SetUnknownObservationsNb(std::stoi(val));
+    else if (key == "itheta" || key == "initialtheta") SetInitialTheta(parse_theta(val));
+    else if (key == "lb" || key == "lowerbounds") SetLowerBounds(parse_theta(val));
+    else if (key == "ub" || key == "upperbounds") SetUpperBounds(parse_theta(val));
+    else if (key == "etheta" || key == "estimatedtheta") SetEstimatedTheta(parse_theta(val));
+    else if (key == "mspe") SetIsMSPE(parse_bool(val));
+    else if (key == "computation") {
+      if (val != "exact") throw std::domain_error("only --computation=exact is on the B200 path");
+      SetComputation(common::EXACT_DENSE);
+    } else if (key == "dimension") {
+      if (val != "2D" && val != "2d") throw std::domain_error("only 2D locations are on the B200 path");
+      SetDimension(common::Dimension2D);
+    } else if (key == "cores") SetCoresNumber(std::stoi(val));
+    else if (key == "gpus") SetGPUsNumbers(std::stoi(val));
+    else if (key == "verbose") SetVerbosity(val == "quiet" ? common::QUIET_MODE
+                                            : val == "detailed" ? common::DETAILED_MODE : common::STANDARD_MODE);
+    else throw std::invalid_argument("unknown or unsupported argument --" + arg);
+  }
+}
+
+}  // namespace exageostat::configurations

@@ -63,6 +63,15 @@ EGS_API int egs_problem_info(const egs_problem* p, int* n, int* ts, int* nt, lon
 /* Run all later work of this problem on the given cudaStream_t (NULL: the problem's own stream). */
 EGS_API int egs_problem_set_stream(egs_problem* p, void* cuda_stream);
 
+/* Select the factorisation of this problem: band = 0 (default) is the exact dense
+ * Cholesky; band >= 1 is the diagonal super-tile approximation with that many
+ * tiles in the band, replacing ChameleonDST<T>::ExaGeoStatPotrfTile
+ * (src/linear-algebra-solvers/concrete/chameleon/dst/ChameleonDST.cpp:23-150,
+ * --computation=diag_approx --band=b).  The approximation is defined on the
+ * caller's tiles, so band >= 1 requires dts to be a multiple of 64 (the device
+ * tile); other sizes return EGS_ERR_INVALID. */
+EGS_API int egs_problem_set_band(egs_problem* p, int band);
+
 /* Copy n locations from host memory (Locations<T> SoA x[], y[],
  * src/data-units/Locations.cpp:94-118). */
 EGS_API int egs_problem_set_locations(egs_problem* p, const double* x, const double* y);
@@ -119,6 +128,22 @@ EGS_API int egs_dlarnv_normal(const int* iseed, int n, double* out);
  * to z_out when it is not NULL).  Replaces
  * LinearAlgebraMethods<T>::GenerateObservationsVector (LinearAlgebraMethods.cpp:333-449). */
 EGS_API int egs_generate_observations(egs_problem* p, const double* theta, int seed, double* z_out);
+
+/* ---- optimiser ----------------------------------------------------------- */
+
+/* Objective for egs_bobyqa_maximize: value at x (n parameters). */
+typedef double (*egs_objective_fn)(int n, const double* x, void* ctx);
+/* Maximise f over the box [lb, ub] without derivatives, starting from x (in/out:
+ * the best point on return), with initial trust radius rhobeg (<= 0: a quarter
+ * of the narrowest box width), stopping after maxeval evaluations or when an
+ * improvement of the best value is below ftol_abs.  *fbest receives the best
+ * value, *nevals the number of evaluations.  Replaces the NLopt LN_BOBYQA run of
+ * StarpuRuntimeSolver<T>::ModelingOperations (src/runtime-solver/concrete/
+ * StarpuRuntimeSolver.cpp:28-66): same first evaluations (x0, then x0 + rhobeg
+ * e_i ...), same maxeval / ftol_abs stopping, best value returned. */
+EGS_API int egs_bobyqa_maximize(int n, double* x, const double* lb, const double* ub, double rhobeg,
+                                double ftol_abs, int maxeval, egs_objective_fn f, void* ctx, double* fbest,
+                                int* nevals);
 
 /* ---- instrumentation ----------------------------------------------------- */
 

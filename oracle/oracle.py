@@ -256,6 +256,42 @@ def mle_loglik(x, y, z, theta, return_parts: bool = False):
     return loglik
 
 
+def dst_loglik(x, y, z, theta, ts: int, band: int, return_parts: bool = False):
+    """Log-likelihood with the diagonal super-tile (band) factorisation.
+
+    Follows ChameleonDST<T>::ExaGeoStatParallelPotrfDiagonal
+    (src/linear-algebra-solvers/concrete/chameleon/dst/ChameleonDST.cpp:90-150) for
+    the lower case: at step k, potrf of tile (k,k); trsm of tiles (m,k) for
+    k < m < k+band; syrk of (n,n) and gemm of (m,n) for k < n < k+band,
+    n < m < n+band, reading tile (m,k) whether solved or not.  The rest of the
+    evaluation (log-det over diagonal tiles, Z := L^-1 Z over the whole lower
+    triangle, dot) is ChameleonImplementation.cpp:180-265 unchanged.
+    """
+    n = len(z)
+    A = np.tril(covariance(x, y, theta)).copy()
+    nt = -(-n // ts)
+    blk = lambda i: slice(i * ts, min(n, (i + 1) * ts))  # noqa: E731
+    for k in range(nt):
+        try:
+            A[blk(k), blk(k)] = cholesky_lower(A[blk(k), blk(k)])
+        except (np.linalg.LinAlgError, ValueError) as exc:
+            raise np.linalg.LinAlgError("Matrix is not positive definite") from exc
+        for m in range(k + 1, min(nt, k + band)):
+            A[blk(m), blk(k)] = scipy.linalg.solve_triangular(A[blk(k), blk(k)], A[blk(m), blk(k)].T,
+                                                              lower=True).T
+        for c in range(k + 1, min(nt, k + band)):
+            A[blk(c), blk(c)] -= np.tril(A[blk(c), blk(k)] @ A[blk(c), blk(k)].T)
+            for m in range(c + 1, min(nt, c + band)):
+                A[blk(m), blk(c)] -= A[blk(m), blk(k)] @ A[blk(c), blk(k)].T
+    L = np.tril(A)
+    d = np.diag(L)
+    logdet = 2.0 * float(np.sum(np.log(d[d > 0])))
+    w = scipy.linalg.solve_triangular(L, np.asarray(z, dtype=np.float64), lower=True, check_finite=False)
+    dot = float(w @ w)
+    loglik = -0.5 * dot - 0.5 * logdet - (n / 2.0) * math.log(2.0 * PI)
+    return (loglik, logdet, dot) if return_parts else loglik
+
+
 # --------------------------------------------------------------------------
 # Random hold-out split: PredictionHelpers.cpp:23-168 (Shuffle :140-168)
 # --------------------------------------------------------------------------

@@ -1,0 +1,256 @@
+// C++ API test driver: the reference's API-level tests (TestExaGeoStatApi.cpp,
+// TestUnivariateMaternStationary.cpp, TestPrediction.cpp, TestSyntheticGenerator.cpp)
+// re-expressed against the B200 host API.  Each case sets up Configurations the way
+// the reference test does, runs the API, and prints one JSON line of results;
+// tests/test_gpu_host_api.py compares them with the reference goldens.
+//
+// usage: test_exageostat_api <case> [fixture-file]
+//   fixture-file: three lines of 16 numbers (x, y, z) -- the reference's N=16 fixture.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <iostream>
+#include <memory>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "api/ExaGeoStat.hpp"
+#include "hardware/ExaGeoStatHardware.hpp"
+
+using namespace exageostat;
+using namespace exageostat::common;
+using namespace exageostat::configurations;
+using namespace exageostat::dataunits;
+
+namespace {
+
+std::string json_array(const double* v, int n) {
+  std::ostringstream os;
+  os.precision(17);
+  os << "[";
+  for (int i = 0; i < n; ++i) os << (i ? "," : "") << v[i];
+  os << "]";
+  return os.str();
+}
+
+struct Fixture {
+  std::vector<double> x, y, z;
+};
+
+Fixture read_fixture(const char* path) {
+  Fixture f;
+  std::ifstream in(path);
+  std::vector<double>* rows[3] = {&f.x, &f.y, &f.z};
+  std::string line;
+  for (int r = 0; r < 3 && std::getline(in, line); ++r) {
+    std::istringstream ls(line);
+    double v;
+    while (ls >> v) rows[r]->push_back(v);
+  }
+  if (f.x.size() != 16 || f.y.size() != 16 || f.z.size() != 16) throw std::runtime_error("bad fixture file");
+  return f;
+}
+
+// TestExaGeoStatApi.cpp TEST_GENERATE_DATA / TestUnivariateMaternStationary.cpp
+void generate(int n, int dts) {
+  Configurations c;
+  c.SetSeed(0);
+  c.SetProblemSize(n);
+  c.SetKernelName("UnivariateMaternStationary");
+  c.SetDenseTileSize(dts);
+  c.SetComputation(EXACT_DENSE);
+  Configurations::SetVerbosity(QUIET_MODE);
+  c.SetLowerBounds({0.1, 0.1, 0.1});
+  c.SetUpperBounds({5, 5, 5});
+  c.SetInitialTheta({1, 0.1, 0.5});
+  auto hardware = ExaGeoStatHardware(EXACT_DENSE, 4, 0);
+  std::unique_ptr<ExaGeoStatData<double>> data;
+  api::ExaGeoStat<double>::ExaGeoStatLoadData(c, data);
+  auto* A = (double*)data->GetDescriptorData()->GetDescriptor(CHAMELEON_DESCRIPTOR, DESCRIPTOR_Z).chameleon_desc->mat;
+  std::cout << "{\"z\": " << json_array(A, n) << ", \"x\": " << json_array(data->GetLocations()->GetLocationX(), n)
+            << ", \"y\": " << json_array(data->GetLocations()->GetLocationY(), n) << "}" << std::endl;
+}
+
+Configurations modeling_config() {
+  Configurations c;
+  c.SetSeed(0);
+  c.SetProblemSize(16);
+  c.SetKernelName("UnivariateMaternStationary");
+  c.SetDenseTileSize(8);
+  c.SetComputation(EXACT_DENSE);
+  c.SetMaxMleIterations(3);
+  c.SetTolerance(4);
+  c.SetLowerBounds({0.1, 0.1, 0.1});
+  c.SetStartingTheta({0.1, 0.1, 0.1});
+  c.SetUpperBounds({5, 5, 5});
+  c.SetInitialTheta({1, 0.1, 0.5});
+  Configurations::SetVerbosity(QUIET_MODE);
+  return c;
+}
+
+// TestExaGeoStatApi.cpp TEST_MODEL_DATA, section "Data Modeling"
+void modeling_fixture(const Fixture& f) {
+  Configurations c = modeling_config();
+  auto hardware = ExaGeoStatHardware(EXACT_DENSE, 4, 0);
+  auto data = std::make_unique<ExaGeoStatData<double>>(c.GetProblemSize(), c.GetDimension());
+  std::vector<double> z = f.z, x = f.x, y = f.y;
+  data->GetLocations()->SetLocationX(*x.data(), 16);
+  data->GetLocations()->SetLocationY(*y.data(), 16);
+  double ll = api::ExaGeoStat<double>::ExaGeoStatDataModeling(c, data, z.data());
+  std::cout.precision(17);
+  std::cout << "{\"loglik\": " << ll << ", \"theta\": " << json_array(c.GetEstimatedTheta().data(), 3)
+            << ", \"iterations\": " << data->GetMleIterations() << "}" << std::endl;
+}
+
+// TestExaGeoStatApi.cpp TEST_MODEL_DATA, section "Data Generation and Modeling"
+void generate_and_model() {
+  Configurations c = modeling_config();
+  auto hardware = ExaGeoStatHardware(EXACT_DENSE, 4, 0);
+  std::unique_ptr<ExaGeoStatData<double>> data;
+  api::ExaGeoStat<double>::ExaGeoStatLoadData(c, data);
+  double ll = api::ExaGeoStat<double>::ExaGeoStatDataModeling(c, data);
+  std::cout.precision(17);
+  std::cout << "{\"loglik\": " << ll << ", \"theta\": " << json_array(c.GetEstimatedTheta().data(), 3) << "}"
+            << std::endl;
+}
+
+// TestPrediction.cpp TEST_PREDICTION_MISSING_DATA, section "Test Prediction - MSPE"
+void prediction_mspe(const Fixture& f) {
+  Configurations c;
+  c.SetUnknownObservationsNb(4);
+  c.SetProblemSize(16);
+  c.SetKernelName("UnivariateMaternStationary");
+  c.SetDenseTileSize(8);
+  c.SetComputation(EXACT_DENSE);
+  c.SetMaxMleIterations(3);
+  c.SetTolerance(4);
+  c.SetLowerBounds({0.1, 0.1, 0.1});
+  c.SetStartingTheta({0.1, 0.1, 0.1});
+  c.SetUpperBounds({5, 5, 5});
+  c.SetInitialTheta({1, 0.1, 0.5});
+  Configurations::SetVerbosity(QUIET_MODE);
+  auto hardware = ExaGeoStatHardware(EXACT_DENSE, c.GetCoresNumber(), c.GetGPUsNumbers());
+  auto data = std::make_unique<ExaGeoStatData<double>>(c.GetProblemSize(), c.GetDimension());
+  std::vector<double> z = f.z, x = f.x, y = f.y;
+  data->GetLocations()->SetLocationX(*x.data(), 16);
+  data->GetLocations()->SetLocationY(*y.data(), 16);
+  c.SetIsMSPE(true);
+  c.SetEstimatedTheta({0.9, 0.09, 0.4});
+  kernels::Kernel<double>* pKernel =
+      plugins::PluginRegistry<kernels::Kernel<double>>::Create(c.GetKernelName(), c.GetTimeSlot());
+  prediction::Prediction<double>::PredictMissingData(data, c, z.data(), *pKernel);
+  delete pKernel;
+  auto zm = results::Results::GetInstance()->GetPredictedMissedValues();
+  std::cout.precision(17);
+  std::cout << "{\"mspe\": " << results::Results::GetInstance()->GetMSPEError()
+            << ", \"z_miss\": " << json_array(zm.data(), (int)zm.size()) << "}" << std::endl;
+}
+
+// TestSyntheticGenerator.cpp TEST_GENERATION
+void generated_locations() {
+  Configurations c;
+  c.SetDimension(Dimension2D);
+  c.SetInitialTheta({1, 0.1, 0.5});
+  c.SetProblemSize(9);
+  c.SetDenseTileSize(1);
+  c.SetKernelName("UnivariateMaternStationary");
+  c.SetComputation(EXACT_DENSE);
+  srand(0);
+  Locations<double> l(9, Dimension2D);
+  generators::SyntheticGenerator<double>::GenerateLocations(9, l);
+  Locations<double> l1(9, Dimension2D);
+  generators::SyntheticGenerator<double>::GenerateLocations(9, l1);  // continues the rand() sequence
+  srand(0);
+  Locations<double> l2(9, Dimension2D);
+  generators::SyntheticGenerator<double>::GenerateLocations(9, l2);
+  std::cout << "{\"x\": " << json_array(l.GetLocationX(), 9) << ", \"y\": " << json_array(l.GetLocationY(), 9)
+            << ", \"x_second\": " << json_array(l1.GetLocationX(), 9)
+            << ", \"x_reseeded\": " << json_array(l2.GetLocationX(), 9) << "}" << std::endl;
+}
+
+// Kernel plugin on the host interface, and the reference's error behaviour.
+void plugin_and_errors(const Fixture& f) {
+  auto hardware = ExaGeoStatHardware(EXACT_DENSE, 1, 1);
+  Locations<double> l(16, Dimension2D);
+  std::vector<double> x = f.x, y = f.y;
+  l.SetLocationX(*x.data(), 16);
+  l.SetLocationY(*y.data(), 16);
+  kernels::Kernel<double>* k =
+      plugins::PluginRegistry<kernels::Kernel<double>>::Create("UnivariateMaternStationary", 1);
+  double theta[3] = {1.3, 0.2, 0.5};
+  std::vector<double> a(5 * 7);
+  k->GenerateCovarianceMatrix(a.data(), 5, 7, 3, 6, l, l, l, theta, 0);
+  double maxerr = 0;
+  for (int j = 0; j < 7; ++j)
+    for (int i = 0; i < 5; ++i) {
+      const double dx = x[6 + j] - x[3 + i], dy = y[6 + j] - y[3 + i];
+      const double d = std::sqrt(dx * dx + dy * dy) / 0.2;
+      const double ref = d == 0 ? 1.3 : 1.3 * std::exp(-d);
+      maxerr = std::max(maxerr, std::fabs(a[i + j * 5] - ref) / std::fabs(ref));
+    }
+  delete k;
+  std::string unknown_kernel, non_spd, no_theta;
+  try {
+    plugins::PluginRegistry<kernels::Kernel<double>>::Create("NoSuchKernel", 1);
+  } catch (const std::exception& e) {
+    unknown_kernel = e.what();
+  }
+  try {
+    Configurations c = modeling_config();
+    auto data = std::make_unique<ExaGeoStatData<double>>(16, Dimension2D);
+    std::vector<double> xs = f.x, ys = f.y, z = f.z;
+    xs[5] = std::nan("");
+    data->GetLocations()->SetLocationX(*xs.data(), 16);
+    data->GetLocations()->SetLocationY(*ys.data(), 16);
+    api::ExaGeoStat<double>::ExaGeoStatDataModeling(c, data, z.data());
+  } catch (const std::exception& e) {
+    non_spd = e.what();
+  }
+  try {
+    Configurations c = modeling_config();
+    c.SetIsMSPE(true);
+    c.SetUnknownObservationsNb(4);
+    auto data = std::make_unique<ExaGeoStatData<double>>(16, Dimension2D);
+    std::vector<double> z = f.z;
+    kernels::Kernel<double>* kk =
+        plugins::PluginRegistry<kernels::Kernel<double>>::Create("UnivariateMaternStationary", 1);
+    std::unique_ptr<kernels::Kernel<double>> guard(kk);
+    c.InitializeAllTheta();
+    prediction::Prediction<double>::PredictMissingData(data, c, z.data(), *kk);
+  } catch (const std::exception& e) {
+    no_theta = e.what();
+  }
+  std::cout.precision(17);
+  std::cout << "{\"plugin_max_rel_err\": " << maxerr << ", \"unknown_kernel\": \"" << unknown_kernel
+            << "\", \"non_spd\": \"" << non_spd << "\", \"no_theta\": \"" << no_theta.substr(0, 40) << "\"}"
+            << std::endl;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  if (argc < 2) {
+    std::cerr << "usage: test_exageostat_api <case> [fixture-file]\n";
+    return 2;
+  }
+  const std::string which = argv[1];
+  try {
+    if (which == "generate_n16") generate(16, 9);
+    else if (which == "generate_n9") generate(9, 5);
+    else if (which == "modeling_fixture") modeling_fixture(read_fixture(argv[2]));
+    else if (which == "generate_and_model") generate_and_model();
+    else if (which == "prediction_mspe") prediction_mspe(read_fixture(argv[2]));
+    else if (which == "generated_locations") generated_locations();
+    else if (which == "plugin_and_errors") plugin_and_errors(read_fixture(argv[2]));
+    else {
+      std::cerr << "unknown case " << which << "\n";
+      return 2;
+    }
+  } catch (const std::exception& e) {
+    std::cerr << "exception: " << e.what() << "\n";
+    return 1;
+  }
+  return 0;
+}

@@ -1,0 +1,86 @@
+"""The C++ host API (ExaGeoStat<T>, Configurations, Kernel plugin, Prediction) against
+the reference's API-level goldens.  The driver tests/cpp/test_exageostat_api.cpp sets
+up each case the way the reference's Catch2 test does; this file checks its output.
+"""
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+BIN = os.path.join(ROOT, "tests", "cpp", "_build", "test_exageostat_api")
+
+
+@pytest.fixture(scope="module")
+def driver():
+    if not os.path.exists(BIN):
+        from exageostat_b200 import build as b
+        b.build_host_tests()
+    return BIN
+
+
+@pytest.fixture(scope="module")
+def fixture_file(goldens, tmp_path_factory):
+    f = goldens["fixture_n16"]
+    p = tmp_path_factory.mktemp("fx") / "fixture.txt"
+    p.write_text("\n".join(" ".join(repr(v) for v in f[k]) for k in ("x", "y", "z")) + "\n")
+    return str(p)
+
+
+def run(driver, *args):
+    res = subprocess.run([driver, *args], capture_output=True, text=True, timeout=600)
+    assert res.returncode == 0, res.stderr
+    return json.loads(res.stdout.strip().splitlines()[-1])
+
+
+def test_generated_locations_cpu(driver, goldens):
+    # CPU only: the location generator draws from the C library's rand()
+    out = run(driver, "generated_locations")
+    g = goldens["locations_n9_seed0"]
+    assert np.abs(np.array(out["x"]) - g["x"]).max() < g["margin"]
+    assert np.abs(np.array(out["y"]) - g["y"]).max() < g["margin"]
+    assert np.abs(np.array(out["x_second"]) - g["x"]).max() > g["margin"]   # continues the sequence
+    assert np.array_equal(out["x_reseeded"], out["x"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case,key", [("generate_n16", "z_n16_dts9_seed0"), ("generate_n9", "z_n9_dts5_seed0")])
+def test_load_data_observations(driver, goldens, case, key):
+    out = run(driver, case)
+    g = goldens[key]
+    assert np.abs(np.array(out["z"]) - g["z"]).max() < g["margin"]
+
+
+@pytest.mark.gpu
+def test_data_modeling_fixture(driver, goldens, fixture_file):
+    out = run(driver, "modeling_fixture", fixture_file)
+    g = goldens["modeling_loglik_n16"]
+    assert abs(out["loglik"] - g["exact_dense"]) < g["margin"]
+    assert out["iterations"] == g["max_mle_iterations"]
+    assert out["theta"] == pytest.approx([1.325, 0.1, 0.1], abs=1e-12)
+
+
+@pytest.mark.gpu
+def test_data_generation_and_modeling(driver, goldens):
+    out = run(driver, "generate_and_model")
+    g = goldens["modeling_loglik_n16"]
+    assert abs(out["loglik"] - g["exact_dense"]) < g["margin"]
+
+
+@pytest.mark.gpu
+def test_prediction_mspe(driver, goldens, fixture_file):
+    out = run(driver, "prediction_mspe", fixture_file)
+    g = goldens["prediction_mspe_n16"]
+    assert out["mspe"] == pytest.approx(g["mspe"], rel=1.2e-5)
+    assert len(out["z_miss"]) == g["z_miss_number"]
+
+
+@pytest.mark.gpu
+def test_kernel_plugin_and_error_behaviour(driver, fixture_file):
+    out = run(driver, "plugin_and_errors", fixture_file)
+    assert out["plugin_max_rel_err"] < 1e-13
+    assert "NoSuchKernel" in out["unknown_kernel"]
+    assert out["non_spd"] == "Matrix is not positive definite"
+    assert out["no_theta"].startswith("Can't predict without an estimated")

@@ -78,3 +78,18 @@ def test_oracle_cholesky_failure_is_reported():
     x = np.array([0.1, 0.2, np.nan])
     with pytest.raises(Exception):
         O.mle_loglik(x, x, np.ones(3), [1.0, 0.1, 0.5])
+
+
+def test_diagonal_approximation_golden(goldens):
+    # TestExaGeoStatApi.cpp:95: DIAGONAL_APPROX with band 1, same 3 BOBYQA evaluations
+    f = goldens["fixture_n16"]
+    g = goldens["modeling_loglik_n16"]
+    vals = [O.dst_loglik(f["x"], f["y"], f["z"], th, g["dts"], 1)
+            for th in ([0.1, 0.1, 0.1], [1.325, 0.1, 0.1], [0.1, 1.325, 0.1])]
+    assert abs(max(vals) - g["diag_approx_band1"]) < g["margin"]
+
+
+def test_wide_band_is_exact():
+    x, y, z = O.load_data(200, 2, [1.0, 0.1, 0.5])
+    th = [0.9, 0.12, 0.7]
+    assert O.dst_loglik(x, y, z, th, 64, 4) == pytest.approx(O.mle_loglik(x, y, z, th), rel=1e-12)
