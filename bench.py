@@ -145,6 +145,24 @@ def fp64_dgemm_peak_tflops(torch) -> float:
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
+def small_problem_rate(egs, torch, steps: int = 200):
+    """Evaluations/s of the reference's N = 1,600, tile 320 configuration (CUDA-graph replay)."""
+    x, y = egs.generate_locations(1600, 0)
+    p = egs.Problem(1600, 320)
+    p.set_locations(x, y)
+    p.generate_observations((1.0, 0.1, 0.5), 0)
+    for _ in range(5):
+        p.mle_eval((1.0, 0.1, 0.5))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        p.mle_eval((1.0, 0.1, 0.5))
+    dt = time.perf_counter() - t0
+    p.close()
+    return {"config": "N=1600, tile 320, theta=(1,0.1,0.5), one GPU, host-timed incl. result read-back",
+            "evals_per_s": steps / dt, "ms_per_eval": 1e3 * dt / steps}
+
+
 def cpu_sample(x, y, z, target_s: float = 12.0):
     """Time the CPU restatement on a bounded sample; returns (evals/s scaled to N, info)."""
     from oracle import cpu_baseline as C
@@ -339,6 +357,7 @@ def main():
             "launches": n_up,
             "flops_per_launch": stage_flops[up] / max(n_up, 1)}
     eval_flops = n ** 3 / 3.0 + n ** 2 / 2.0 + n / 6.0 + n ** 2
+    small = small_problem_rate(egs, torch)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -350,6 +369,7 @@ def main():
         "stages_ms_per_eval": {s: float(stage_ms[i]) / args.steps for i, s in enumerate(egs.STAGES)},
         "roofline": roof, "e2e": e2e,
         "gpu_launches": int(stage_launches.sum()),
+        "small_n": small,
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -42,6 +42,7 @@ SIGNATURES = {
     "egs_problem_info": (ctypes.c_int, [_P, _I, _I, _I, _LL]),
     "egs_problem_set_stream": (ctypes.c_int, [_P, _P]),
     "egs_problem_set_band": (ctypes.c_int, [_P, ctypes.c_int]),
+    "egs_problem_set_graphs": (ctypes.c_int, [_P, ctypes.c_int]),
     "egs_problem_set_locations": (ctypes.c_int, [_P, _D, _D]),
     "egs_problem_set_locations_device": (ctypes.c_int, [_P, _P, _P]),
     "egs_problem_set_observations": (ctypes.c_int, [_P, _D]),
@@ -145,6 +146,10 @@ class Problem:
             self.close()
         except Exception:
             pass
+
+    def set_graphs(self, enable: bool) -> None:
+        """Replay evaluations as one CUDA graph (default on)."""
+        _check(self._lib.egs_problem_set_graphs(self._h, 1 if enable else 0), "set_graphs")
 
     def set_band(self, band: int) -> None:
         """0: exact dense Cholesky; >= 1: diagonal super-tile approximation with this band."""

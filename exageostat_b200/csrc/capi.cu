@@ -55,6 +55,13 @@ struct egs_problem {
   bool have_locations = false;
   bool have_observations = false;
   int band = 0;  // >= 1: diagonal super-tile approximation with this tile band
+  // Replay of a whole evaluation: captured at the second evaluation, relaunched after.
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  int graph_band = -1;
+  long long graph_launches[EGS_NUM_STAGES] = {};
+  long long evals = 0;
+  bool graphs_enabled = true;
   // Per-stage accounting: launch counts always, CUDA-event times when profiling.
   bool profiling = false;
   struct Span {
@@ -157,6 +164,8 @@ void free_problem(egs_problem* p) {
   cudaFreeHost(p->hparams);
   cudaFreeHost(p->hresult);
   cudaFreeHost(p->hflags);
+  if (p->graph_exec) cudaGraphExecDestroy(p->graph_exec);
+  if (p->graph) cudaGraphDestroy(p->graph);
   if (p->own_stream && p->stream) cudaStreamDestroy(p->stream);
   for (cudaEvent_t e : p->events) cudaEventDestroy(e);
   delete p;
@@ -338,6 +347,69 @@ int sync_flags(egs_problem* p, bool want_result) {
     set_last_error("Matrix is not positive definite", "potrf");
     return p->hflags[0];
   }
+  return EGS_OK;
+}
+
+// Device work of one evaluation after the parameter record is on the device:
+// Z <- Zcpy, generation, factorisation, log-det, solve, assembly, and the copy
+// of the result record and status words to the pinned host mirrors.
+int enqueue_eval(egs_problem* p) {
+  cudaStream_t st = p->stream;
+  EGS_CUDA_TRY(cudaMemsetAsync(p->flags, 0, 2 * sizeof(int), st));
+  EGS_CUDA_TRY(cudaMemcpyAsync(p->z, p->zcpy, p->np * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  int sp = span_begin(p, EGS_STAGE_GENERATE);
+  int rc = launch_matern_tiles(p->tiles, p->x, p->y, p->n, p->ts, p->nt, p->dparams, st);
+  if (rc != EGS_OK) return check_cuda("matern");
+  count_launches(p, EGS_STAGE_GENERATE, (lower_tiles(p->nt) + 65534) / 65535);
+  span_end(p, sp, 0.0);
+  rc = p->band > 0 ? enqueue_potrf_band(p) : enqueue_potrf(p);
+  if (rc != EGS_OK) return rc;
+  sp = span_begin(p, EGS_STAGE_REDUCE);
+  launch_logdet_partials(p->tiles, p->ts, p->nt, p->n, p->partial, st);
+  span_end(p, sp, 0.0);
+  count_launches(p, EGS_STAGE_REDUCE, 1);
+  enqueue_trsv(p);
+  sp = span_begin(p, EGS_STAGE_REDUCE);
+  launch_finalize(p->partial, p->nt, p->z, p->n, p->result, p->flags, st);
+  span_end(p, sp, 0.0);
+  count_launches(p, EGS_STAGE_REDUCE, 1);
+  EGS_CUDA_TRY(cudaMemcpyAsync(p->hflags, p->flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+  EGS_CUDA_TRY(cudaMemcpyAsync(p->hresult, p->result, 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  return check_cuda("egs_mle_eval");
+}
+
+// Capture the parameter upload and enqueue_eval into a graph.  Capture problems
+// (an unsupported call inside the stream) disable replay for this problem.
+int capture_eval(egs_problem* p) {
+  if (p->graph_exec) cudaGraphExecDestroy(p->graph_exec);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  p->graph_exec = nullptr;
+  p->graph = nullptr;
+  long long before[EGS_NUM_STAGES];
+  for (int i = 0; i < EGS_NUM_STAGES; ++i) before[i] = p->stage_launches[i];
+  cudaStream_t st = p->stream;
+  if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    p->graphs_enabled = false;
+    return EGS_OK;
+  }
+  cudaMemcpyAsync(p->dparams, p->hparams, sizeof(MaternParams), cudaMemcpyHostToDevice, st);
+  const int rc = enqueue_eval(p);
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(st, &g);
+  for (int i = 0; i < EGS_NUM_STAGES; ++i) {
+    p->graph_launches[i] = p->stage_launches[i] - before[i];
+    p->stage_launches[i] = before[i];
+  }
+  if (rc != EGS_OK || e != cudaSuccess || !g || cudaGraphInstantiate(&p->graph_exec, g, 0) != cudaSuccess) {
+    cudaGetLastError();
+    if (g) cudaGraphDestroy(g);
+    p->graph_exec = nullptr;
+    p->graphs_enabled = false;
+    return EGS_OK;
+  }
+  p->graph = g;
+  p->graph_band = p->band;
   return EGS_OK;
 }
 
@@ -567,34 +639,47 @@ int egs_get_observations(egs_problem* p, double* host_z) {
 int egs_mle_eval(egs_problem* p, const double* theta, double* loglik, double* logdet, double* dot) {
   if (!p || !loglik) return EGS_ERR_INVALID;
   if (!p->have_locations || !p->have_observations) return EGS_ERR_STATE;
-  int rc = set_params(p, theta);
-  if (rc != EGS_OK) return rc;
+  MaternParams mp;
+  int rc = make_matern_params(theta, &mp);
+  if (rc != EGS_OK) {
+    set_last_error("theta outside the Matern domain (sigma2 > 0, beta > 0, nu > 0)", "make_matern_params");
+    return rc;
+  }
   cudaStream_t st = p->stream;
-  EGS_CUDA_TRY(cudaMemsetAsync(p->flags, 0, 2 * sizeof(int), st));
-  EGS_CUDA_TRY(cudaMemcpyAsync(p->z, p->zcpy, p->np * sizeof(double), cudaMemcpyDeviceToDevice, st));
-  int sp = span_begin(p, EGS_STAGE_GENERATE);
-  rc = launch_matern_tiles(p->tiles, p->x, p->y, p->n, p->ts, p->nt, p->dparams, st);
-  if (rc != EGS_OK) return check_cuda("matern");
-  count_launches(p, EGS_STAGE_GENERATE, (lower_tiles(p->nt) + 65534) / 65535);
-  span_end(p, sp, 0.0);
-  rc = p->band > 0 ? enqueue_potrf_band(p) : enqueue_potrf(p);
-  if (rc != EGS_OK) return rc;
-  sp = span_begin(p, EGS_STAGE_REDUCE);
-  launch_logdet_partials(p->tiles, p->ts, p->nt, p->n, p->partial, st);
-  span_end(p, sp, 0.0);
-  count_launches(p, EGS_STAGE_REDUCE, 1);
-  enqueue_trsv(p);
-  sp = span_begin(p, EGS_STAGE_REDUCE);
-  launch_finalize(p->partial, p->nt, p->z, p->n, p->result, p->flags, st);
-  span_end(p, sp, 0.0);
-  count_launches(p, EGS_STAGE_REDUCE, 1);
-  rc = check_cuda("egs_mle_eval");
-  if (rc != EGS_OK) return rc;
-  rc = sync_flags(p, true);
-  if (rc != EGS_OK) return rc;
+  // The pinned mirrors may still be in use by the previous evaluation.
+  EGS_CUDA_TRY(cudaStreamSynchronize(st));
+  *p->hparams = mp;
+  const bool replay = p->graphs_enabled && !p->profiling && p->evals > 0;
+  if (replay && (!p->graph_exec || p->graph_band != p->band)) {
+    if ((rc = capture_eval(p)) != EGS_OK) return rc;
+  }
+  if (replay && p->graph_exec) {
+    EGS_CUDA_TRY(cudaGraphLaunch(p->graph_exec, st));
+    for (int i = 0; i < EGS_NUM_STAGES; ++i) p->stage_launches[i] += p->graph_launches[i];
+  } else {
+    EGS_CUDA_TRY(cudaMemcpyAsync(p->dparams, p->hparams, sizeof(MaternParams), cudaMemcpyHostToDevice, st));
+    if ((rc = enqueue_eval(p)) != EGS_OK) return rc;
+  }
+  ++p->evals;
+  EGS_CUDA_TRY(cudaStreamSynchronize(st));
+  collect_spans(p);
+  if (p->hflags[1] != 0) {
+    set_last_error("a device-side wait exceeded its limit", "tensor-core update");
+    return EGS_ERR_TIMEOUT;
+  }
+  if (p->hflags[0] > 0) {
+    set_last_error("Matrix is not positive definite", "potrf");
+    return p->hflags[0];
+  }
   *loglik = p->hresult[0];
   if (logdet) *logdet = p->hresult[1];
   if (dot) *dot = p->hresult[2];
+  return EGS_OK;
+}
+
+int egs_problem_set_graphs(egs_problem* p, int enable) {
+  if (!p) return EGS_ERR_INVALID;
+  p->graphs_enabled = enable != 0;
   return EGS_OK;
 }
 

@@ -140,16 +140,22 @@ __device__ __forceinline__ int perm_b(int r) {
   return (r & 1) | (((r >> 2) & 1) << 1) | (((r >> 1) & 1) << 3) | (((r >> 3) & 1) << 2);
 }
 
-struct GemmDesc {
-  int M, N, K;
-  int a_row0, a_col0, a_tcol;
-  int b_row0, b_col0, b_tcol;
-  int c_row0, c_col0;
-  int lower;
-  int MB, NB;
-  long long total;
-  int ts, nt, np;
-};
+template <bool kBatched>
+__device__ __forceinline__ const GemmDesc* locate_job(long long L, const GemmDesc& single, const GemmJobs& J,
+                                                      long long& local) {
+  if constexpr (!kBatched) {
+    local = L;
+    return &single;
+  } else {
+    int lo = 0, hi = J.njobs - 1;
+    while (lo < hi) {  // last job with begin <= L
+      const int mid = (lo + hi + 1) >> 1;
+      if (J.begin[mid] <= L) lo = mid; else hi = mid - 1;
+    }
+    local = L - J.begin[lo];
+    return J.jobs + lo;
+  }
+}
 
 // Raster: groups of GROUP block-columns; inside a group, block-rows outer,
 // block-columns inner, so a group's B panel stays in L2 while A streams once.
@@ -176,6 +182,7 @@ struct Cursor {
   long long L;
   int kt;
   bool valid;
+  const GemmDesc* d;
 };
 
 __device__ __forceinline__ void box_coords(int g0, int tcol, const GemmDesc& d, int2* out) {
@@ -186,19 +193,24 @@ __device__ __forceinline__ void box_coords(int g0, int tcol, const GemmDesc& d, 
     if (g < d.np) {
       const int ti = g / d.ts;
       x = g - ti * d.ts;
-      z = (int)tile_slot(ti, tcol, d.nt);
+      z = (int)(d.tile_base + tile_slot(ti, tcol, d.nt));
     }
     out[b] = make_int2(x, z);
   }
 }
 
-__device__ __forceinline__ void cursor_seek(Cursor& c, const GemmDesc& d, int2* coords) {
-  while (c.L < d.total) {
+template <bool kBatched>
+__device__ __forceinline__ void cursor_seek(Cursor& c, const GemmDesc& single, const GemmJobs& J, long long total,
+                                            int2* coords) {
+  while (c.L < total) {
+    long long local;
+    const GemmDesc& d = *locate_job<kBatched>(c.L, single, J, local);
     int mb, nb;
-    decode_block(c.L, d, mb, nb);
+    decode_block(local, d, mb, nb);
     if (!(d.lower && mb < nb)) {
       box_coords(d.a_row0 + mb * gemm::BM, d.a_tcol, d, coords);
       box_coords(d.b_row0 + nb * gemm::BN, d.b_tcol, d, coords + gemm::BM / gemm::BOX_ROWS);
+      c.d = &d;
       c.valid = true;
       return;
     }
@@ -208,8 +220,9 @@ __device__ __forceinline__ void cursor_seek(Cursor& c, const GemmDesc& d, int2* 
 }
 
 __device__ __forceinline__ void issue_stage(const CUtensorMap* tmap, uint8_t* smem, uint64_t* full, uint32_t s,
-                                            const Cursor& c, const GemmDesc& d, const int2* coords) {
+                                            const Cursor& c, const int2* coords) {
   using namespace gemm;
+  const GemmDesc& d = *c.d;
   mbar_expect_tx(&full[s], STAGE_BYTES);
   uint8_t* sa = smem + s * STAGE_BYTES;
   uint8_t* sb = sa + A_STAGE_BYTES;
@@ -226,9 +239,10 @@ __device__ __forceinline__ void issue_stage(const CUtensorMap* tmap, uint8_t* sm
   }
 }
 
+template <bool kBatched>
 __global__ void __launch_bounds__(gemm::THREADS, 1)
-dgemm_update_kernel(const __grid_constant__ CUtensorMap tmap, double* __restrict__ tiles, GemmDesc d,
-                    int* __restrict__ err) {
+dgemm_update_kernel(const __grid_constant__ CUtensorMap tmap, double* __restrict__ tiles, const __grid_constant__ GemmDesc single,
+                    GemmJobs J, int* __restrict__ err) {
   using namespace gemm;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   // 1024-byte aligned stage base (128B-swizzle atoms), kept as an offset into the
@@ -239,7 +253,7 @@ dgemm_update_kernel(const __grid_constant__ CUtensorMap tmap, double* __restrict
   uint64_t* empty = full + STAGES;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const bool producer = threadIdx.x == 0;
-  const int ksteps = d.K / BK;
+  const long long total = kBatched ? J.total : single.total;
   if (producer) {
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(&full[s], 1);
@@ -259,7 +273,8 @@ dgemm_update_kernel(const __grid_constant__ CUtensorMap tmap, double* __restrict
   cur.valid = false;
   uint32_t issued = 0;
   bool alive = true;
-  if (producer) cursor_seek(cur, d, coords);
+  cur.d = &single;
+  if (producer) cursor_seek<kBatched>(cur, single, J, total, coords);
   auto top_up = [&](uint32_t consumed) {
     // Keep up to STAGES-1 stages in flight ahead of the consumers.
     while (alive && cur.valid && issued < consumed + STAGES - 1) {
@@ -268,12 +283,12 @@ dgemm_update_kernel(const __grid_constant__ CUtensorMap tmap, double* __restrict
         alive = false;
         break;
       }
-      issue_stage(&tmap, smem, full, s, cur, d, coords);
+      issue_stage(&tmap, smem, full, s, cur, coords);
       ++issued;
-      if (++cur.kt == ksteps) {
+      if (++cur.kt == cur.d->K / BK) {
         cur.kt = 0;
         cur.L += gridDim.x;
-        cursor_seek(cur, d, coords);
+        cursor_seek<kBatched>(cur, single, J, total, coords);
       }
     }
   };
@@ -301,10 +316,13 @@ dgemm_update_kernel(const __grid_constant__ CUtensorMap tmap, double* __restrict
 
   uint32_t it = 0;
   bool ok = true;
-  for (long long L = blockIdx.x; L < d.total && ok; L += gridDim.x) {
+  for (long long L = blockIdx.x; L < total && ok; L += gridDim.x) {
+    long long local;
+    const GemmDesc& d = *locate_job<kBatched>(L, single, J, local);
     int mb, nb;
-    decode_block(L, d, mb, nb);
+    decode_block(local, d, mb, nb);
     if (d.lower && mb < nb) continue;
+    const int ksteps = d.K / BK;
     double acc[4][4][4];
 #pragma unroll
     for (int mi = 0; mi < 4; ++mi)
@@ -368,7 +386,8 @@ dgemm_update_kernel(const __grid_constant__ CUtensorMap tmap, double* __restrict
           const int gi = d.c_row0 + ml;
           const int ti = gi / ts, lr = gi - ti * ts;
           const bool ok_el = nl < d.N && ml < d.M && ti >= tj;
-          ptr[h][mi] = ok_el ? tiles + tile_slot(ti, tj, d.nt) * (long long)ts * ts + (long long)lc * ts + lr
+          ptr[h][mi] = ok_el ? tiles + (d.tile_base + tile_slot(ti, tj, d.nt)) * (long long)ts * ts +
+                                   (long long)lc * ts + lr
                              : nullptr;
           if (ok_el) ldg_v2f64(ptr[h][mi], cv[h][mi][0], cv[h][mi][1]);
         }
@@ -427,10 +446,17 @@ int gemm_num_sms() {
   return g_num_sms;
 }
 
-static int launch_desc(const void* tmap, double* tiles, GemmDesc& d, int* err, cudaStream_t st) {
+static void set_gemm_smem_attributes() {
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(dgemm_update_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, gemm::SMEM_BYTES);
+    cudaFuncSetAttribute(dgemm_update_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, gemm::SMEM_BYTES);
+    attr_set = true;
+  }
+}
+
+void finish_desc(GemmDesc& d) {
   using namespace gemm;
-  if (d.M <= 0 || d.N <= 0 || d.K <= 0) return EGS_OK;
-  if (d.K % BK != 0) return EGS_ERR_INVALID;
   d.MB = (d.M + BM - 1) / BM;
   d.NB = (d.N + BN - 1) / BN;
   long long total = 0;
@@ -439,14 +465,19 @@ static int launch_desc(const void* tmap, double* tiles, GemmDesc& d, int* err, c
     total += (long long)ge * (d.MB - (d.lower ? nb0 : 0));
   }
   d.total = total;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(dgemm_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-    attr_set = true;
-  }
+}
+
+static int launch_desc(const void* tmap, double* tiles, GemmDesc& d, int* err, cudaStream_t st) {
+  using namespace gemm;
+  if (d.M <= 0 || d.N <= 0 || d.K <= 0) return EGS_OK;
+  if (d.K % BK != 0) return EGS_ERR_INVALID;
+  finish_desc(d);
+  const long long total = d.total;
+  set_gemm_smem_attributes();
   const long long grid = total < gemm_num_sms() ? total : gemm_num_sms();
-  dgemm_update_kernel<<<(unsigned)grid, THREADS, SMEM_BYTES, st>>>(*reinterpret_cast<const CUtensorMap*>(tmap),
-                                                                    tiles, d, err);
+  GemmJobs none{nullptr, nullptr, 0, 0};
+  dgemm_update_kernel<false><<<(unsigned)grid, THREADS, SMEM_BYTES, st>>>(
+      *reinterpret_cast<const CUtensorMap*>(tmap), tiles, d, none, err);
   return cudaGetLastError() == cudaSuccess ? EGS_OK : EGS_ERR_CUDA;
 }
 
@@ -487,6 +518,25 @@ int launch_gemm_rows(const void* tmap, double* tiles, int ts, int nt, int M, int
   d.c_col0 = c_col0;
   d.lower = lower;
   return launch_desc(tmap, tiles, d, err, st);
+}
+
+}  // namespace egs
+
+namespace egs {
+
+// One launch over many jobs (one per problem of a batch); jobs and begin live in
+// device memory, begin[j] = number of blocks of jobs 0..j-1 (finish_desc totals).
+int launch_gemm_batched(const void* tmap, double* tiles, const GemmDesc* jobs, const long long* begin, int njobs,
+                        long long total, int* err, cudaStream_t st) {
+  using namespace gemm;
+  if (njobs <= 0 || total <= 0) return EGS_OK;
+  set_gemm_smem_attributes();
+  const long long grid = total < gemm_num_sms() ? total : gemm_num_sms();
+  GemmDesc none{};
+  GemmJobs J{jobs, begin, njobs, total};
+  dgemm_update_kernel<true><<<(unsigned)grid, THREADS, SMEM_BYTES, st>>>(
+      *reinterpret_cast<const CUtensorMap*>(tmap), tiles, none, J, err);
+  return cudaGetLastError() == cudaSuccess ? EGS_OK : EGS_ERR_CUDA;
 }
 
 }  // namespace egs

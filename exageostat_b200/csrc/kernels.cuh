@@ -31,6 +31,32 @@ void launch_gemv_t_block(const double* a, long long lda, int rows, int cols, con
                          cudaStream_t st);
 
 // FP64 tensor-core update C -= A * B^T over global row indices (dgemm_tma.cu).
+// Every operand row is a global row of one problem (tile row g / ts); A and B take
+// their K columns from one tile column starting at a local column offset; C is
+// addressed by (global row, global column), upper tiles never written.
+struct GemmDesc {
+  int M, N, K;
+  int a_row0, a_col0, a_tcol;
+  int b_row0, b_col0, b_tcol;
+  int c_row0, c_col0;
+  int lower;
+  int MB, NB;
+  long long total;
+  int ts, nt, np;
+  long long tile_base;  // slot of this problem's tile (0, 0) in a pool of problems
+};
+
+// Batched launches: blocks [begin[j], begin[j+1]) belong to job j.
+struct GemmJobs {
+  const GemmDesc* jobs;
+  const long long* begin;
+  int njobs;
+  long long total;
+};
+
+void finish_desc(GemmDesc& d);  // fills MB, NB, total
+int launch_gemm_batched(const void* tmap, double* tiles, const GemmDesc* jobs, const long long* begin, int njobs,
+                        long long total, int* err, cudaStream_t st);
 int gemm_init_tensor_map(void* tmap_storage, double* tiles, int ts, long long ntiles);
 int launch_gemm_trailing(const void* tmap, double* tiles, int ts, int nt, int k, int* err, cudaStream_t st);
 int launch_gemm_rows(const void* tmap, double* tiles, int ts, int nt, int M, int N, int K, int a_row0,

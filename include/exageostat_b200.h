@@ -193,6 +193,11 @@ EGS_API int egs_mle_eval_noalloc(int n, int dts, const double* x, const double* 
                                  const double* theta, double* work, long long work_doubles, double* loglik,
                                  void* cuda_stream);
 
+/* From its second evaluation on, egs_mle_eval replays the whole evaluation of a
+ * problem as one CUDA graph (captured once; disabled while profiling).  enable = 0
+ * turns replay off for this problem, 1 (the default) on. */
+EGS_API int egs_problem_set_graphs(egs_problem* p, int enable);
+
 /* ---- kernel plugin ------------------------------------------------------ */
 
 /* rows x cols column-major block (leading dimension lda) on caller device

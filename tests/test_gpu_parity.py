@@ -318,3 +318,23 @@ def test_diagonal_super_tile_needs_device_sized_tiles(goldens):
         p.set_band(1)
     assert ei.value.status == egs.EGS_ERR_INVALID
     p.set_band(0)
+
+
+
+def test_graph_replay_is_bit_identical_to_direct_launches():
+    x, y, z = synthetic(1600, 0, [1.0, 0.1, 0.5])
+    direct = egs.Problem(1600, 320)
+    direct.set_graphs(False)
+    replay = egs.Problem(1600, 320)
+    for p in (direct, replay):
+        p.set_locations(x, y)
+        p.set_observations(z)
+    thetas = ([1.0, 0.1, 0.5], [0.7, 0.2, 1.1], [1.3, 0.05, 0.6], [1.0, 0.1, 0.5])
+    for th in thetas:
+        assert replay.mle_eval(th) == direct.mle_eval(th)
+    # a change of factorisation recaptures the graph
+    replay.set_band(2)
+    direct.set_band(2)
+    for th in ([1.0, 0.02, 0.5], [1.0, 0.03, 0.8]):
+        a, b = replay.mle_eval(th), direct.mle_eval(th)
+        assert a == b
