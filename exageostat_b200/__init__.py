@@ -68,6 +68,11 @@ SIGNATURES = {
     "egs_mle_loglik_host": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _D]),
     "egs_predict_host": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _D, _D, _D,
                                         _D, _D]),
+    "egs_batch_create": (ctypes.c_int, [ctypes.POINTER(_P), ctypes.c_int, _I, ctypes.c_int, _D, _D, _D]),
+    "egs_batch_destroy": (ctypes.c_int, [_P]),
+    "egs_batch_info": (ctypes.c_int, [_P, _I, _I, _LL, _LL]),
+    "egs_batch_eval": (ctypes.c_int, [_P, _D, _D, _I]),
+    "egs_batch_autotune": (ctypes.c_int, [ctypes.c_int, _I, _D, _D, _D, _D, _I, ctypes.c_int, _I, _D]),
 }
 
 OBJECTIVE = ctypes.CFUNCTYPE(ctypes.c_double, ctypes.c_int, _D, ctypes.c_void_p)
@@ -298,3 +303,63 @@ def bobyqa_maximize(f, x0, lb, ub, ftol_abs: float, maxeval: int, rhobeg: float 
     if err:
         raise err[0]
     return x, fb.value, ne.value
+
+
+class Batch:
+    """Many independent problems evaluated together (``egs_batch``).
+
+    ``sizes[i]`` points of problem i; ``x``, ``y``, ``z`` are the problems'
+    arrays concatenated in order.  ``eval(theta)`` takes a (B, 3) array and
+    returns (loglik[B], status[B]); status[i] > 0 marks a problem whose
+    covariance was not positive definite (its loglik is not meaningful)."""
+
+    def __init__(self, sizes, x, y, z, dts: int):
+        self._lib = load_library()
+        self.sizes = np.ascontiguousarray(sizes, dtype=np.int32)
+        x, y, z = _f64(x), _f64(y), _f64(z)
+        if not (len(x) == len(y) == len(z) == int(self.sizes.sum())):
+            raise ValueError("x, y, z must hold sum(sizes) points")
+        self.B = len(self.sizes)
+        self._h = _P()
+        _check(self._lib.egs_batch_create(ctypes.byref(self._h), self.B, self.sizes.ctypes.data_as(_I), int(dts),
+                                          _dptr(x), _dptr(y), _dptr(z)), "egs_batch_create")
+
+    def info(self):
+        ts, ntm, nb, nl = ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong(), ctypes.c_longlong()
+        _check(self._lib.egs_batch_info(self._h, ctypes.byref(ts), ctypes.byref(ntm), ctypes.byref(nb),
+                                        ctypes.byref(nl)), "egs_batch_info")
+        return {"ts": ts.value, "nt_max": ntm.value, "bytes": nb.value, "launches_per_eval": nl.value}
+
+    def eval(self, theta):
+        th = _f64(np.broadcast_to(np.asarray(theta, dtype=np.float64), (self.B, 3)))
+        ll = np.empty(self.B)
+        st = np.zeros(self.B, dtype=np.int32)
+        rc = self._lib.egs_batch_eval(self._h, _dptr(th), _dptr(ll), st.ctypes.data_as(_I))
+        if rc not in (EGS_OK, EGS_ERR_STATE):
+            _check(rc, "egs_batch_eval")
+        return ll, st
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.egs_batch_destroy(self._h)
+            self._h = _P()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def batch_autotune(sizes, x, y, z, theta, candidates=(128, 192, 256, 320)):
+    """Fastest common tile size for a batch (one timed replay per candidate)."""
+    lib = load_library()
+    sizes = np.ascontiguousarray(sizes, dtype=np.int32)
+    B = len(sizes)
+    th = _f64(np.broadcast_to(np.asarray(theta, dtype=np.float64), (B, 3)))
+    cand = np.ascontiguousarray(candidates, dtype=np.int32)
+    best, ms = ctypes.c_int(), ctypes.c_double()
+    _check(lib.egs_batch_autotune(B, sizes.ctypes.data_as(_I), _dptr(_f64(x)), _dptr(_f64(y)), _dptr(_f64(z)),
+                                  _dptr(th), cand.ctypes.data_as(_I), len(cand), ctypes.byref(best),
+                                  ctypes.byref(ms)), "egs_batch_autotune")
+    return best.value, ms.value

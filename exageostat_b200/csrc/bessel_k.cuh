@@ -127,7 +127,31 @@ struct MaternParams {
   double mu;         // nu - n
   int n;             // floor(nu + 1/2)
   int kind;          // 0: nu == 1/2, 1: half-integer, 2: general
+  int table;         // 1: general nu <= kKtabMaxNu, evaluated through the Chebyshev table below
+  int pad_;
 };
+
+// K_nu(x) for kind 2 (general nu): Temme's series (x <= 2, unscaled) or Steed's
+// CF2 (x > 2, scaled by e^x, *scaled = true), then the upward recurrence.
+__device__ __forceinline__ double bessel_k_general(double x, const MaternParams& p, bool& scaled) {
+  double k0, k1;
+  if (x <= 2.0) {
+    k_temme_series(p.mu, x, k0, k1);
+    scaled = false;
+  } else {
+    k_steed_cf2_scaled(p.mu, x, k0, k1);
+    scaled = true;
+  }
+  if (p.n == 0) return k0;
+  double v = p.mu + 1.0;
+  for (int j = 1; j < p.n; ++j) {
+    const double k2 = k0 + (2.0 * v / x) * k1;
+    k0 = k1;
+    k1 = k2;
+    v += 1.0;
+  }
+  return k1;
+}
 
 // Matern covariance for scaled distance x = d / beta > 0:
 // con * x^nu * K_nu(x)   (UnivariateMaternStationary.cpp:61-62).
@@ -154,32 +178,82 @@ __device__ __forceinline__ double matern_positive(double x, const MaternParams& 
     // con * x^nu * sqrt(pi/2x) e^-x * rv
     return p.con * sqrt(M_PI / (2.0 * x)) * exp(p.nu * log(x) - x) * rv;
   }
-  double k0, k1;
   bool scaled;
-  if (x <= 2.0) {
-    k_temme_series(p.mu, x, k0, k1);
-    scaled = false;
-  } else {
-    k_steed_cf2_scaled(p.mu, x, k0, k1);
-    scaled = true;
-  }
-  double knu;
-  if (p.n == 0) {
-    knu = k0;
-  } else {
-    double v = p.mu + 1.0;
-    for (int j = 1; j < p.n; ++j) {
-      const double k2 = k0 + (2.0 * v / x) * k1;
-      k0 = k1;
-      k1 = k2;
-      v += 1.0;
-    }
-    knu = k1;
-  }
+  const double knu = bessel_k_general(x, p, scaled);
   if (scaled) {
     return p.con * exp(p.nu * log(x) - x) * knu;
   }
   return p.con * pow(x, p.nu) * knu;
+}
+
+// ---------------------------------------------------------------------------
+// Piecewise Chebyshev table of g(x) = e^x x^nu K_nu(x) for general nu.
+//
+// For one theta the generator evaluates the same K_nu at millions of distances;
+// the series/continued-fraction evaluation above costs thousands of FP64
+// operations per element (divisions, data-dependent trip counts that diverge
+// inside a warp).  Instead, per theta, g is interpolated on half-octave
+// intervals [2^e, 2^e sqrt2), [2^e sqrt2, 2^(e+1)) for 2^-20 <= x < 2^9 by
+// Chebyshev series of degree 15 whose coefficients come from the evaluation
+// above at the 16 Chebyshev points of each interval (one small launch per
+// theta).  g is analytic except for its branch point at 0, which lies
+// (3 + 2 sqrt2) half-widths from each interval's centre, so the series
+// converge like (5.83 + sqrt(5.83^2 - 1))^-k ~ 11.6^-k: the interpolant is
+// within a few 1e-15 (relative) of g for nu <= 8 (checked against 30-digit
+// values).  An element then costs one table lookup, a 16-term Clenshaw sum and
+// one exp.  Distances outside [2^-20, 2^9) and nu > 8 use the direct
+// evaluation.
+constexpr int kKtabDeg = 16;     // coefficients per interval
+constexpr int kKtabStride = 17;  // padded row: lanes reading different intervals hit different banks
+constexpr int kKtabELo = -20, kKtabEHi = 9;
+constexpr int kKtabIntervals = 2 * (kKtabEHi - kKtabELo);
+constexpr int kKtabDoubles = kKtabIntervals * kKtabStride;
+constexpr double kKtabMaxNu = 8.0;
+// t = x * 2^-e * S_h + C maps interval (e, h) onto [-1, 1]:
+// h = 0: S = 2 / (sqrt2 - 1) = 2 + 2 sqrt2; h = 1: S = 2 + sqrt2; C = -(3 + 2 sqrt2) for both.
+constexpr double kKtabS0 = 4.8284271247461900976, kKtabS1 = 3.4142135623730950488;
+constexpr double kKtabC = -5.8284271247461900976;
+constexpr long long kSqrt2Mantissa = 0x6A09E667F3BCDLL;  // fraction bits of fl(sqrt 2)
+
+// e^x x^nu K_nu(x) by the direct evaluation (kind 2).
+__device__ __forceinline__ double matern_g_direct(double x, const MaternParams& p) {
+  bool scaled;
+  const double knu = bessel_k_general(x, p, scaled);
+  if (scaled) return exp(p.nu * log(x)) * knu;
+  return exp(x) * pow(x, p.nu) * knu;
+}
+
+// Interval and local coordinate of x > 0; false outside the tabulated range.
+__device__ __forceinline__ bool ktab_locate(double x, int& idx, double& t) {
+  const long long bits = __double_as_longlong(x);
+  const int e = (int)(bits >> 52) - 1023;
+  if (e < kKtabELo || e >= kKtabEHi) return false;
+  const int h = (bits & 0xFFFFFFFFFFFFFLL) >= kSqrt2Mantissa ? 1 : 0;
+  idx = 2 * (e - kKtabELo) + h;
+  const double scale = __longlong_as_double((long long)(1023 - e) << 52);  // 2^-e, exact
+  t = fma(x, scale * (h ? kKtabS1 : kKtabS0), kKtabC);
+  return true;
+}
+
+// Node j (Chebyshev point of the first kind) of interval idx.
+__device__ __forceinline__ double ktab_node(int idx, int j) {
+  const int e = idx / 2 + kKtabELo, h = idx & 1;
+  const double t = cospi((j + 0.5) / kKtabDeg);
+  const double scale = __longlong_as_double((long long)(1023 + e) << 52);  // 2^e, exact
+  return (t - kKtabC) / (h ? kKtabS1 : kKtabS0) * scale;
+}
+
+// Clenshaw sum of one interval's Chebyshev series at t.
+__device__ __forceinline__ double ktab_sum(const double* __restrict__ c, double t) {
+  const double t2 = 2.0 * t;
+  double b1 = 0.0, b2 = 0.0;
+#pragma unroll
+  for (int k = kKtabDeg - 1; k >= 1; --k) {
+    const double b0 = fma(t2, b1, c[k] - b2);
+    b2 = b1;
+    b1 = b0;
+  }
+  return fma(t, b1, c[0] - b2);
 }
 
 // Euclidean distance sqrt(dx^2 + dy^2) with dx = x2 - x1, dy = y2 - y1, rounded
@@ -196,6 +270,18 @@ __device__ __forceinline__ double euclid_dist(double x1, double y1, double x2, d
 __device__ __forceinline__ double matern_from_dist(double dist, const MaternParams& p) {
   const double x = __ddiv_rn(dist, p.beta);
   return (x == 0.0) ? p.sigma2 : matern_positive(x, p);
+}
+
+// The same entry through the Chebyshev table tab (kKtabDoubles, any address
+// space) when p.table is set.
+__device__ __forceinline__ double matern_from_dist_tab(double dist, const MaternParams& p,
+                                                       const double* __restrict__ tab) {
+  const double x = __ddiv_rn(dist, p.beta);
+  if (x == 0.0) return p.sigma2;
+  int idx;
+  double t;
+  if (p.table && ktab_locate(x, idx, t)) return p.con * (ktab_sum(tab + idx * kKtabStride, t) * exp(-x));
+  return matern_positive(x, p);
 }
 
 }  // namespace egs

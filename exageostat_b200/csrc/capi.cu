@@ -45,6 +45,7 @@ struct egs_problem {
   double* result = nullptr;
   int* flags = nullptr;  // [0] potrf info, [1] device wait error
   MaternParams* dparams = nullptr;
+  double* ktab = nullptr;  // Chebyshev table of K_nu for the current theta (kKtabDoubles)
   // pinned host mirrors
   MaternParams* hparams = nullptr;
   double* hresult = nullptr;
@@ -161,6 +162,7 @@ void free_problem(egs_problem* p) {
   cudaFree(p->result);
   cudaFree(p->flags);
   cudaFree(p->dparams);
+  cudaFree(p->ktab);
   cudaFreeHost(p->hparams);
   cudaFreeHost(p->hresult);
   cudaFreeHost(p->hflags);
@@ -358,9 +360,9 @@ int enqueue_eval(egs_problem* p) {
   EGS_CUDA_TRY(cudaMemsetAsync(p->flags, 0, 2 * sizeof(int), st));
   EGS_CUDA_TRY(cudaMemcpyAsync(p->z, p->zcpy, p->np * sizeof(double), cudaMemcpyDeviceToDevice, st));
   int sp = span_begin(p, EGS_STAGE_GENERATE);
-  int rc = launch_matern_tiles(p->tiles, p->x, p->y, p->n, p->ts, p->nt, p->dparams, st);
+  int rc = launch_matern_tiles(p->tiles, p->x, p->y, p->n, p->ts, p->nt, p->dparams, p->ktab, st);
   if (rc != EGS_OK) return check_cuda("matern");
-  count_launches(p, EGS_STAGE_GENERATE, (lower_tiles(p->nt) + 65534) / 65535);
+  count_launches(p, EGS_STAGE_GENERATE, 1 + (lower_tiles(p->nt) + 65534) / 65535);
   span_end(p, sp, 0.0);
   rc = p->band > 0 ? enqueue_potrf_band(p) : enqueue_potrf(p);
   if (rc != EGS_OK) return rc;
@@ -468,7 +470,8 @@ int egs_problem_create(egs_problem** out, int n, int dts) {
       (rc = dev_alloc(&p->x, p->np, &p->bytes)) || (rc = dev_alloc(&p->y, p->np, &p->bytes)) ||
       (rc = dev_alloc(&p->z, p->np, &p->bytes)) || (rc = dev_alloc(&p->zcpy, p->np, &p->bytes)) ||
       (rc = dev_alloc(&p->partial, p->nt, &p->bytes)) || (rc = dev_alloc(&p->result, 4, &p->bytes)) ||
-      (rc = dev_alloc(&p->flags, 2, &p->bytes)) || (rc = dev_alloc(&p->dparams, 1, &p->bytes))) {
+      (rc = dev_alloc(&p->flags, 2, &p->bytes)) || (rc = dev_alloc(&p->dparams, 1, &p->bytes)) ||
+      (rc = dev_alloc(&p->ktab, kKtabDoubles, &p->bytes))) {
     free_problem(p);
     return rc;
   }
@@ -575,7 +578,7 @@ int egs_covariance_generate(egs_problem* p, const double* theta) {
   if (!p->have_locations) return EGS_ERR_STATE;
   int rc = set_params(p, theta);
   if (rc != EGS_OK) return rc;
-  rc = launch_matern_tiles(p->tiles, p->x, p->y, p->n, p->ts, p->nt, p->dparams, p->stream);
+  rc = launch_matern_tiles(p->tiles, p->x, p->y, p->n, p->ts, p->nt, p->dparams, p->ktab, p->stream);
   if (rc != EGS_OK) return check_cuda("egs_covariance_generate");
   EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
   return EGS_OK;
@@ -731,8 +734,10 @@ constexpr size_t kNoAllocPartialOff = 0;
 constexpr size_t kNoAllocResultOff = kNoAllocPartialOff + kNoAllocMaxTileRows * sizeof(double);
 constexpr size_t kNoAllocFlagsOff = kNoAllocResultOff + 4 * sizeof(double);
 constexpr size_t kNoAllocParamsOff = kNoAllocFlagsOff + 256;
-constexpr size_t kNoAllocScratchBytes = kNoAllocParamsOff + 256;
+constexpr size_t kNoAllocKtabOff = kNoAllocParamsOff + 256;
+constexpr size_t kNoAllocScratchBytes = kNoAllocKtabOff + kKtabDoubles * sizeof(double);
 constexpr int kNoAllocMaxDevices = 64;
+static_assert(sizeof(MaternParams) <= 256, "parameter slot of the static scratch");
 
 }  // namespace
 
@@ -810,6 +815,7 @@ int egs_mle_eval_noalloc(int n, int dts, const double* x, const double* y, const
   double* result = reinterpret_cast<double*>(scratch + kNoAllocResultOff);
   int* flags = reinterpret_cast<int*>(scratch + kNoAllocFlagsOff);
   MaternParams* dparams = reinterpret_cast<MaternParams*>(scratch + kNoAllocParamsOff);
+  double* ktab = reinterpret_cast<double*>(scratch + kNoAllocKtabOff);
 
   // A problem record on the stack that points at the caller's workspace and the
   // static scratch; it owns nothing.
@@ -828,6 +834,7 @@ int egs_mle_eval_noalloc(int n, int dts, const double* x, const double* y, const
   q.result = result;
   q.flags = flags;
   q.dparams = dparams;
+  q.ktab = ktab;
   q.stream = (cudaStream_t)cuda_stream;
   q.own_stream = false;
   if ((rc = gemm_init_tensor_map(q.tmap, q.tiles, q.ts, q.ntiles)) != EGS_OK) return rc;
@@ -844,7 +851,7 @@ int egs_mle_eval_noalloc(int n, int dts, const double* x, const double* y, const
     EGS_CUDA_TRY(cudaMemsetAsync(q.y + n, 0, pad, st));
     EGS_CUDA_TRY(cudaMemsetAsync(q.z + n, 0, pad, st));
   }
-  if ((rc = launch_matern_tiles(q.tiles, q.x, q.y, n, q.ts, q.nt, dparams, st)) != EGS_OK)
+  if ((rc = launch_matern_tiles(q.tiles, q.x, q.y, n, q.ts, q.nt, dparams, ktab, st)) != EGS_OK)
     return check_cuda("egs_mle_eval_noalloc/matern");
   if ((rc = enqueue_potrf(&q)) != EGS_OK) return rc;
   launch_logdet_partials(q.tiles, q.ts, q.nt, n, partial, st);

@@ -7,8 +7,12 @@
 namespace egs {
 
 int make_matern_params(const double* theta, MaternParams* out);
+// Builds the Chebyshev table of K_nu for theta (ktab: kKtabDoubles device
+// doubles), then generates every lower tile.
 int launch_matern_tiles(double* tiles, const double* x, const double* y, int n, int ts, int nt,
-                        const MaternParams* dparams, cudaStream_t st);
+                        const MaternParams* dparams, double* ktab, cudaStream_t st);
+// Chebyshev tables of nproblems parameter sets (tab: nproblems * kKtabDoubles).
+void launch_matern_ktab(const MaternParams* params, double* tab, int nproblems, cudaStream_t st);
 int launch_matern_block(double* a, int lda, int rows, int cols, const double* x1, const double* y1,
                         const double* x2, const double* y2, const MaternParams& p, cudaStream_t st);
 

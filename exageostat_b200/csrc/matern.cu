@@ -10,6 +10,7 @@
 #include "common.cuh"
 #include "bessel_k.cuh"
 #include "kernels.cuh"
+#include "matern_tile.cuh"
 
 namespace egs {
 
@@ -34,6 +35,8 @@ int make_matern_params(const double* theta, MaternParams* out) {
   } else {
     p.kind = 2;
   }
+  p.table = (p.kind == 2 && nu <= kKtabMaxNu) ? 1 : 0;
+  p.pad_ = 0;
   *out = p;
   return EGS_OK;
 }
@@ -51,40 +54,39 @@ __device__ __forceinline__ void slot_to_tile(long long s, int nt, int& ti, int& 
   ti = j + (int)(s - tile_slot(j, j, nt));
 }
 
-// One thread = rows (r, r+1) of column c of one lower tile.
-template <typename Real>
-__global__ void __launch_bounds__(256)
-matern_tiles_kernel(Real* __restrict__ tiles, const double* __restrict__ x, const double* __restrict__ y,
-                    int n, int ts, int nt, long long slot_begin, const MaternParams* __restrict__ pp) {
+// Chebyshev table of g(x) = e^x x^nu K_nu(x) for each problem whose nu needs one:
+// block (interval, problem), thread j evaluates g at node j, then computes
+// coefficient j of the interval's series (discrete cosine sum over the nodes).
+__global__ void __launch_bounds__(kKtabDeg)
+matern_ktab_kernel(const MaternParams* __restrict__ params, double* __restrict__ tab) {
+  const MaternParams p = params[blockIdx.y];
+  if (!p.table) return;
+  __shared__ double f[kKtabDeg];
+  const int idx = blockIdx.x, j = threadIdx.x;
+  f[j] = matern_g_direct(ktab_node(idx, j), p);
+  __syncthreads();
+  double c = 0.0;
+  for (int q = 0; q < kKtabDeg; ++q) c = fma(f[q], cospi((double)(j * (2 * q + 1)) / (2 * kKtabDeg)), c);
+  c *= (j == 0 ? 1.0 : 2.0) / kKtabDeg;
+  tab[blockIdx.y * (long long)kKtabDoubles + idx * kKtabStride + j] = c;
+}
+
+void launch_matern_ktab(const MaternParams* params, double* tab, int nproblems, cudaStream_t st) {
+  matern_ktab_kernel<<<dim3(kKtabIntervals, nproblems), kKtabDeg, 0, st>>>(params, tab);
+}
+
+__global__ void __launch_bounds__(kGenThreads)
+matern_tiles_kernel(double* __restrict__ tiles, const double* __restrict__ x, const double* __restrict__ y,
+                    int n, int ts, int nt, long long slot_begin, const MaternParams* __restrict__ pp,
+                    const double* __restrict__ tab) {
+  __shared__ double stab[kKtabDoubles];
   const MaternParams p = *pp;
+  stage_ktab(stab, tab, p);
   const long long slot = slot_begin + blockIdx.y;
   int ti, tj;
   slot_to_tile(slot, nt, ti, tj);
-  const long long pair = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long pairs_per_tile = (long long)ts * ts / 2;
-  if (pair >= pairs_per_tile) return;
-  const long long e = pair * 2;
-  const int c = (int)(e / ts);
-  const int r = (int)(e - (long long)c * ts);
-  const int gr = ti * ts + r;
-  const int gc = tj * ts + c;
-  const double xc = x[gc], yc = y[gc];
-  const double2 xr = *reinterpret_cast<const double2*>(x + gr);
-  const double2 yr = *reinterpret_cast<const double2*>(y + gr);
-  double v0, v1;
-  if (gc >= n) {
-    v0 = (gr == gc) ? 1.0 : 0.0;
-    v1 = (gr + 1 == gc) ? 1.0 : 0.0;
-  } else {
-    v0 = (gr < n) ? matern_from_dist(euclid_dist(xr.x, yr.x, xc, yc), p) : 0.0;
-    v1 = (gr + 1 < n) ? matern_from_dist(euclid_dist(xr.y, yr.y, xc, yc), p) : 0.0;
-  }
-  Real* dst = tiles + slot * (long long)ts * ts + e;
-  if constexpr (sizeof(Real) == 8) {
-    *reinterpret_cast<double2*>(dst) = make_double2(v0, v1);
-  } else {
-    *reinterpret_cast<float2*>(dst) = make_float2((float)v0, (float)v1);
-  }
+  matern_tile_pairs(tiles + slot * (long long)ts * ts, x, y, n, ts, ti, tj,
+                    (long long)blockIdx.x * kGenPairsPerBlock, p, stab);
 }
 
 // Generic rows x cols column-major block (leading dimension lda) at global
@@ -101,14 +103,14 @@ matern_block_kernel(double* __restrict__ a, int lda, int rows, int cols, const d
 }
 
 int launch_matern_tiles(double* tiles, const double* x, const double* y, int n, int ts, int nt,
-                        const MaternParams* p, cudaStream_t st) {
+                        const MaternParams* p, double* ktab, cudaStream_t st) {
+  launch_matern_ktab(p, ktab, 1, st);
   const long long pairs = (long long)ts * ts / 2;
-  const int threads = 256;
-  const unsigned gx = (unsigned)((pairs + threads - 1) / threads);
+  const unsigned gx = (unsigned)((pairs + kGenPairsPerBlock - 1) / kGenPairsPerBlock);
   const long long total = lower_tiles(nt);
   for (long long s0 = 0; s0 < total; s0 += 65535) {
     const unsigned gy = (unsigned)((total - s0) < 65535 ? (total - s0) : 65535);
-    matern_tiles_kernel<double><<<dim3(gx, gy), threads, 0, st>>>(tiles, x, y, n, ts, nt, s0, p);
+    matern_tiles_kernel<<<dim3(gx, gy), kGenThreads, 0, st>>>(tiles, x, y, n, ts, nt, s0, p, ktab);
   }
   return cudaGetLastError() == cudaSuccess ? EGS_OK : EGS_ERR_CUDA;
 }

@@ -1,0 +1,205 @@
+// Device bodies of the panel, solve and reduction kernels, shared by the
+// single-problem kernels (potrf.cu) and the batched kernels (batch.cu).  Each
+// body works on one tile (or one 64x64 block) given by pointers, so a kernel
+// only has to locate its tile.
+#pragma once
+#include "common.cuh"
+
+namespace egs {
+
+constexpr int kNB = 64;  // inner block width of the panel factorisation
+
+__device__ __forceinline__ double block_sum_256(double v, double* red) {
+  red[threadIdx.x] = v;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+    __syncthreads();
+  }
+  const double out = red[0];
+  __syncthreads();
+  return out;
+}
+
+// Cholesky of the 64x64 block at T (ld ts) by one warp.  The block sits in
+// shared memory; lane l owns rows l and l + 32.  Step j: every lane reads the
+// pivot (a broadcast), scales its entries of column j, and applies the rank-1
+// update to its rows, reading L[c][j] as broadcasts; only __syncwarp separates
+// the steps.  info records the 1-based global column (gcol0 + j + 1) of the
+// first pivot that is not positive (or NaN).
+__device__ __forceinline__ void potrf64_body(double* __restrict__ T, int ts, int gcol0, int* __restrict__ info) {
+  __shared__ double S[kNB][kNB + 1];
+  const int lane = threadIdx.x;
+  for (int c = 0; c < kNB; ++c) {
+    S[lane][c] = (lane >= c) ? T[(long long)c * ts + lane] : 0.0;
+    S[lane + 32][c] = T[(long long)c * ts + lane + 32];
+  }
+  __syncwarp();
+  const int r0 = lane, r1 = lane + 32;
+  for (int j = 0; j < kNB; ++j) {
+    const double d = S[j][j];
+    if (lane == 0 && !(d > 0.0)) atomicCAS(info, 0, gcol0 + j + 1);
+    const double ljj = sqrt(d);
+    const double inv = 1.0 / ljj;
+    const double l0 = (r0 > j) ? S[r0][j] * inv : 0.0;
+    const double l1 = (r1 > j) ? S[r1][j] * inv : 0.0;
+    __syncwarp();
+    if (r0 > j) S[r0][j] = l0;
+    if (r1 > j) S[r1][j] = l1;
+    if (r0 == j) S[r0][j] = ljj;
+    if (r1 == j) S[r1][j] = ljj;
+    __syncwarp();
+    // Independent columns: unrolled so their shared-memory latencies overlap.
+#pragma unroll 8
+    for (int c = j + 1; c < kNB; ++c) {
+      const double lcj = S[c][j];
+      if (r0 >= c) S[r0][c] = fma(-l0, lcj, S[r0][c]);
+      if (r1 >= c) S[r1][c] = fma(-l1, lcj, S[r1][c]);
+    }
+    __syncwarp();
+  }
+  for (int c = 0; c < kNB; ++c) {
+    if (lane >= c) T[(long long)c * ts + lane] = S[lane][c];
+    T[(long long)c * ts + lane + 32] = S[lane + 32][c];
+  }
+}
+
+// X := A * L^-T for the 64 columns [col0, col0+64) of row `row` of tile A
+// (ld ts); L is the factored 64x64 diagonal block at (col0, col0) of tile TL.
+// Called by every thread of a 128-thread block (rows past ts just return).
+__device__ __forceinline__ void trsm_rows_body(double* __restrict__ A, const double* __restrict__ TL, int ts,
+                                               int row, int col0) {
+  __shared__ __align__(16) double L[kNB][kNB];
+  __shared__ double invd[kNB];
+  for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
+    const int rr = e % kNB, c = e / kNB;
+    L[rr][c] = (rr >= c) ? TL[(long long)(col0 + c) * ts + col0 + rr] : 0.0;
+  }
+  __syncthreads();
+  if (threadIdx.x < kNB) invd[threadIdx.x] = 1.0 / L[threadIdx.x][threadIdx.x];
+  __syncthreads();
+  if (row >= ts) return;
+  double* a = A + (long long)col0 * ts + row;
+  double x[kNB];
+#pragma unroll
+  for (int c = 0; c < kNB; ++c) x[c] = a[(long long)c * ts];
+#pragma unroll
+  for (int c = 0; c < kNB; ++c) {
+    double s = x[c];
+#pragma unroll
+    for (int q = 0; q < c; q += 2) {
+      if (q + 1 < c) {
+        const double2 l2 = *reinterpret_cast<const double2*>(&L[c][q]);
+        s = fma(-x[q], l2.x, s);
+        s = fma(-x[q + 1], l2.y, s);
+      } else {
+        s = fma(-x[q], L[c][q], s);
+      }
+    }
+    x[c] = s * invd[c];
+  }
+#pragma unroll
+  for (int c = 0; c < kNB; ++c) a[(long long)c * ts] = x[c];
+}
+
+// Forward substitution on one diagonal tile T: zk := T^-1 zk (ts entries).
+// Dynamic shared memory: ts doubles.
+__device__ __forceinline__ void trsv_diag_body(const double* __restrict__ T, int ts, double* __restrict__ zk) {
+  extern __shared__ double zs[];  // ts
+  __shared__ double B[kNB][kNB + 1];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int r = tid; r < ts; r += blockDim.x) zs[r] = zk[r];
+  for (int kb = 0; kb < ts; kb += kNB) {
+    for (int e = tid; e < kNB * kNB; e += blockDim.x) {
+      const int rr = e % kNB, c = e / kNB;
+      B[rr][c] = (rr >= c) ? T[(long long)(kb + c) * ts + kb + rr] : 0.0;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      double z0 = zs[kb + lane], z1 = zs[kb + 32 + lane];
+      for (int c = 0; c < kNB; ++c) {
+        double zc;
+        if (c < 32) {
+          if (lane == c) z0 = z0 / B[c][c];
+          zc = __shfl_sync(0xffffffffu, z0, c);
+        } else {
+          if (lane == c - 32) z1 = z1 / B[c][c];
+          zc = __shfl_sync(0xffffffffu, z1, c - 32);
+        }
+        if (lane > c) z0 = fma(-B[lane][c], zc, z0);
+        if (lane + 32 > c) z1 = fma(-B[lane + 32][c], zc, z1);
+      }
+      zs[kb + lane] = z0;
+      zs[kb + 32 + lane] = z1;
+    }
+    __syncthreads();
+    for (int r = kb + kNB + tid; r < ts; r += blockDim.x) {
+      const double* col = T + (long long)kb * ts + r;
+      double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
+#pragma unroll 4
+      for (int c = 0; c < kNB; c += 4) {
+        acc0 = fma(col[(long long)c * ts], zs[kb + c], acc0);
+        acc1 = fma(col[(long long)(c + 1) * ts], zs[kb + c + 1], acc1);
+        acc2 = fma(col[(long long)(c + 2) * ts], zs[kb + c + 2], acc2);
+        acc3 = fma(col[(long long)(c + 3) * ts], zs[kb + c + 3], acc3);
+      }
+      zs[r] -= (acc0 + acc1) + (acc2 + acc3);
+    }
+    __syncthreads();
+  }
+  for (int r = tid; r < ts; r += blockDim.x) zk[r] = zs[r];
+}
+
+// zi -= T zk for the 64 rows of block rblk of tile T (256 threads = 64 rows x
+// 4 column groups, fixed reduction order).  Dynamic shared memory: ts doubles.
+__device__ __forceinline__ void gemv_panel_body(const double* __restrict__ T, int ts, const double* __restrict__ zk,
+                                                double* __restrict__ zi, int rblk) {
+  extern __shared__ double zks[];  // ts
+  __shared__ double red[4][kNB];
+  for (int c = threadIdx.x; c < ts; c += blockDim.x) zks[c] = zk[c];
+  __syncthreads();
+  const int rl = threadIdx.x % kNB, g = threadIdx.x / kNB;
+  const int r = rblk * kNB + rl;
+  double acc = 0.0;
+  if (r < ts) {
+    for (int c = g; c < ts; c += 4) acc = fma(T[(long long)c * ts + r], zks[c], acc);
+  }
+  red[g][rl] = acc;
+  __syncthreads();
+  if (g == 0 && r < ts) zi[r] -= ((red[0][rl] + red[1][rl]) + red[2][rl]) + red[3][rl];
+}
+
+// Sum over the first `rows` diagonal entries of tile T of log L_rr (L_rr > 0
+// only, dmdet-codelet.cpp:76-77); 256 threads.
+__device__ __forceinline__ double logdet_tile_body(const double* __restrict__ T, int ts, int rows) {
+  __shared__ double red[256];
+  double acc = 0.0;
+  for (int r = threadIdx.x; r < rows; r += blockDim.x) {
+    const double d = T[(long long)r * ts + r];
+    if (d > 0.0) acc += log(d);
+  }
+  return block_sum_256(acc, red);
+}
+
+// result[0..3] = (log-likelihood, log|C|, Z^T C^-1 Z, info) of one problem
+// (ChameleonImplementation.cpp:188-192, :257-265); 256 threads, fixed order.
+__device__ __forceinline__ void finalize_body(const double* __restrict__ partial, int nt, const double* __restrict__ z,
+                                              int n, double* __restrict__ result, const int* __restrict__ info) {
+  __shared__ double red[256];
+  double acc = 0.0;
+  for (int r = threadIdx.x; r < n; r += blockDim.x) acc = fma(z[r], z[r], acc);
+  const double dot = block_sum_256(acc, red);
+  if (threadIdx.x == 0) {
+    double det = 0.0;
+    for (int k = 0; k < nt; ++k) det += partial[k];
+    const double logdet = 2.0 * det;
+    const double pi = 3.141592653589793;
+    const double nn = (double)n;
+    result[0] = -0.5 * dot - 0.5 * logdet - (double)(nn / 2.0) * log(2.0 * pi);
+    result[1] = logdet;
+    result[2] = dot;
+    result[3] = (double)(info ? *info : 0);
+  }
+}
+
+}  // namespace egs

@@ -16,57 +16,15 @@
 #include <cmath>
 #include "common.cuh"
 #include "kernels.cuh"
+#include "panel_bodies.cuh"
 
 namespace egs {
 
-constexpr int kNB = 64;  // inner block width of the panel factorisation
-
-// ---------------------------------------------------------------------------
-// Cholesky of the 64x64 diagonal block at (off, off) of one tile by one warp.
-// The block sits in shared memory; lane l owns rows l and l + 32.  Step j:
-// every lane reads the pivot (a broadcast), scales its entries of column j, and
-// applies the rank-1 update to its rows, reading L[c][j] as broadcasts.  Only
-// __syncwarp separates the steps.  info records the 1-based global column of
-// the first pivot that is not positive (or NaN).
-// ---------------------------------------------------------------------------
+// Cholesky of the 64x64 diagonal block at (off, off) of one tile (potrf64_body).
 __global__ void __launch_bounds__(32)
 potrf_diag_block_kernel(double* __restrict__ tiles, int ts, long long slot, int off, int col_base,
                         int* __restrict__ info) {
-  __shared__ double S[kNB][kNB + 1];
-  double* T = tiles + slot * (long long)ts * ts + (long long)off * ts + off;  // block origin, ld = ts
-  const int lane = threadIdx.x;
-  for (int c = 0; c < kNB; ++c) {
-    S[lane][c] = (lane >= c) ? T[(long long)c * ts + lane] : 0.0;
-    S[lane + 32][c] = T[(long long)c * ts + lane + 32];
-  }
-  __syncwarp();
-  const int r0 = lane, r1 = lane + 32;
-  for (int j = 0; j < kNB; ++j) {
-    const double d = S[j][j];
-    if (lane == 0 && !(d > 0.0)) atomicCAS(info, 0, col_base + off + j + 1);
-    const double ljj = sqrt(d);
-    const double inv = 1.0 / ljj;
-    const double l0 = (r0 > j) ? S[r0][j] * inv : 0.0;
-    const double l1 = (r1 > j) ? S[r1][j] * inv : 0.0;
-    __syncwarp();
-    if (r0 > j) S[r0][j] = l0;
-    if (r1 > j) S[r1][j] = l1;
-    if (r0 == j) S[r0][j] = ljj;
-    if (r1 == j) S[r1][j] = ljj;
-    __syncwarp();
-    // Independent columns: unrolled so their shared-memory latencies overlap.
-#pragma unroll 8
-    for (int c = j + 1; c < kNB; ++c) {
-      const double lcj = S[c][j];
-      if (r0 >= c) S[r0][c] = fma(-l0, lcj, S[r0][c]);
-      if (r1 >= c) S[r1][c] = fma(-l1, lcj, S[r1][c]);
-    }
-    __syncwarp();
-  }
-  for (int c = 0; c < kNB; ++c) {
-    if (lane >= c) T[(long long)c * ts + lane] = S[lane][c];
-    T[(long long)c * ts + lane + 32] = S[lane + 32][c];
-  }
+  potrf64_body(tiles + slot * (long long)ts * ts + (long long)off * ts + off, ts, col_base + off, info);
 }
 
 void launch_potrf_diag_block(double* tiles, int ts, long long slot, int off, int col_base, int* info,
@@ -74,48 +32,14 @@ void launch_potrf_diag_block(double* tiles, int ts, long long slot, int off, int
   potrf_diag_block_kernel<<<1, 32, 0, st>>>(tiles, ts, slot, off, col_base, info);
 }
 
-// ---------------------------------------------------------------------------
 // X := A * L^-T for the 64-column block [col0, col0+64) of rows [row0, ts) of
 // ntiles consecutive tiles starting at slot0; L is the factored 64x64 diagonal
-// block at (col0, col0) of tile lslot.  One thread per row, L broadcast from
-// shared memory.
-// ---------------------------------------------------------------------------
+// block at (col0, col0) of tile lslot (trsm_rows_body).
 __global__ void __launch_bounds__(128)
 trsm_rows_kernel(double* __restrict__ tiles, int ts, long long slot0, int row0, int col0,
                  long long lslot) {
-  __shared__ __align__(16) double L[kNB][kNB];
-  __shared__ double invd[kNB];
-  const double* TL = tiles + lslot * (long long)ts * ts;
-  for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
-    const int rr = e % kNB, c = e / kNB;
-    L[rr][c] = (rr >= c) ? TL[(long long)(col0 + c) * ts + col0 + rr] : 0.0;
-  }
-  __syncthreads();
-  if (threadIdx.x < kNB) invd[threadIdx.x] = 1.0 / L[threadIdx.x][threadIdx.x];
-  __syncthreads();
-  const int row = row0 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (row >= ts) return;
-  double* A = tiles + (slot0 + blockIdx.y) * (long long)ts * ts + (long long)col0 * ts + row;
-  double x[kNB];
-#pragma unroll
-  for (int c = 0; c < kNB; ++c) x[c] = A[(long long)c * ts];
-#pragma unroll
-  for (int c = 0; c < kNB; ++c) {
-    double s = x[c];
-#pragma unroll
-    for (int q = 0; q < c; q += 2) {
-      if (q + 1 < c) {
-        const double2 l2 = *reinterpret_cast<const double2*>(&L[c][q]);
-        s = fma(-x[q], l2.x, s);
-        s = fma(-x[q + 1], l2.y, s);
-      } else {
-        s = fma(-x[q], L[c][q], s);
-      }
-    }
-    x[c] = s * invd[c];
-  }
-#pragma unroll
-  for (int c = 0; c < kNB; ++c) A[(long long)c * ts] = x[c];
+  trsm_rows_body(tiles + (slot0 + blockIdx.y) * (long long)ts * ts, tiles + lslot * (long long)ts * ts, ts,
+                 row0 + blockIdx.x * blockDim.x + threadIdx.x, col0);
 }
 
 void launch_trsm_rows(double* tiles, int ts, long long slot0, int ntiles, int row0, int col0,
@@ -127,79 +51,22 @@ void launch_trsm_rows(double* tiles, int ts, long long slot0, int ntiles, int ro
                                                                                     row0, col0, lslot);
 }
 
-// ---------------------------------------------------------------------------
-// Forward substitution on one diagonal tile: z_k := L_kk^-1 z_k.
-// ---------------------------------------------------------------------------
+// Forward substitution on one diagonal tile: z_k := L_kk^-1 z_k (trsv_diag_body).
 __global__ void __launch_bounds__(1024)
 trsv_diag_kernel(const double* __restrict__ tiles, int ts, long long slot, double* __restrict__ zk) {
-  extern __shared__ double zs[];  // ts
-  __shared__ double B[kNB][kNB + 1];
-  const double* T = tiles + slot * (long long)ts * ts;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int r = tid; r < ts; r += blockDim.x) zs[r] = zk[r];
-  for (int kb = 0; kb < ts; kb += kNB) {
-    for (int e = tid; e < kNB * kNB; e += blockDim.x) {
-      const int rr = e % kNB, c = e / kNB;
-      B[rr][c] = (rr >= c) ? T[(long long)(kb + c) * ts + kb + rr] : 0.0;
-    }
-    __syncthreads();
-    if (warp == 0) {
-      double z0 = zs[kb + lane], z1 = zs[kb + 32 + lane];
-      for (int c = 0; c < kNB; ++c) {
-        double zc;
-        if (c < 32) {
-          if (lane == c) z0 = z0 / B[c][c];
-          zc = __shfl_sync(0xffffffffu, z0, c);
-        } else {
-          if (lane == c - 32) z1 = z1 / B[c][c];
-          zc = __shfl_sync(0xffffffffu, z1, c - 32);
-        }
-        if (lane > c) z0 = fma(-B[lane][c], zc, z0);
-        if (lane + 32 > c) z1 = fma(-B[lane + 32][c], zc, z1);
-      }
-      zs[kb + lane] = z0;
-      zs[kb + 32 + lane] = z1;
-    }
-    __syncthreads();
-    for (int r = kb + kNB + tid; r < ts; r += blockDim.x) {
-      const double* col = T + (long long)kb * ts + r;
-      double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
-#pragma unroll 4
-      for (int c = 0; c < kNB; c += 4) {
-        acc0 = fma(col[(long long)c * ts], zs[kb + c], acc0);
-        acc1 = fma(col[(long long)(c + 1) * ts], zs[kb + c + 1], acc1);
-        acc2 = fma(col[(long long)(c + 2) * ts], zs[kb + c + 2], acc2);
-        acc3 = fma(col[(long long)(c + 3) * ts], zs[kb + c + 3], acc3);
-      }
-      zs[r] -= (acc0 + acc1) + (acc2 + acc3);
-    }
-    __syncthreads();
-  }
-  for (int r = tid; r < ts; r += blockDim.x) zk[r] = zs[r];
+  trsv_diag_body(tiles + slot * (long long)ts * ts, ts, zk);
 }
 
 void launch_trsv_diag(const double* tiles, int ts, long long slot, double* zk, cudaStream_t st) {
   trsv_diag_kernel<<<1, 1024, ts * sizeof(double), st>>>(tiles, ts, slot, zk);
 }
 
-// z_i -= L_ik z_k for every tile row i > k.  256 threads = 64 rows x 4 column groups.
+// z_i -= L_ik z_k for every tile row i > k (gemv_panel_body).
 __global__ void __launch_bounds__(256)
 gemv_panel_kernel(const double* __restrict__ tiles, int ts, int nt, int k, double* __restrict__ z) {
-  extern __shared__ double zks[];  // ts
-  __shared__ double red[4][kNB];
   const int i = k + 1 + blockIdx.y;
-  const double* T = tiles + tile_slot(i, k, nt) * (long long)ts * ts;
-  for (int c = threadIdx.x; c < ts; c += blockDim.x) zks[c] = z[(long long)k * ts + c];
-  __syncthreads();
-  const int rl = threadIdx.x % kNB, g = threadIdx.x / kNB;
-  const int r = blockIdx.x * kNB + rl;
-  double acc = 0.0;
-  if (r < ts) {
-    for (int c = g; c < ts; c += 4) acc = fma(T[(long long)c * ts + r], zks[c], acc);
-  }
-  red[g][rl] = acc;
-  __syncthreads();
-  if (g == 0 && r < ts) z[(long long)i * ts + r] -= ((red[0][rl] + red[1][rl]) + red[2][rl]) + red[3][rl];
+  gemv_panel_body(tiles + tile_slot(i, k, nt) * (long long)ts * ts, ts, z + (long long)k * ts,
+                  z + (long long)i * ts, blockIdx.x);
 }
 
 void launch_gemv_panel(const double* tiles, int ts, int nt, int k, double* z, cudaStream_t st) {
@@ -284,33 +151,12 @@ void launch_gemv_t_panel(const double* tiles, int ts, int nt, int k, double* z, 
 // ---------------------------------------------------------------------------
 // Deterministic reductions.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double block_sum_256(double v, double* red) {
-  red[threadIdx.x] = v;
-  __syncthreads();
-  for (int s = 128; s > 0; s >>= 1) {
-    if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
-    __syncthreads();
-  }
-  const double out = red[0];
-  __syncthreads();
-  return out;
-}
-
-// partial[k] = sum over the real rows of diagonal tile k of log L_rr (L_rr > 0 only,
-// dmdet-codelet.cpp:76-77).
+// partial[k] = sum over the real rows of diagonal tile k of log L_rr.
 __global__ void __launch_bounds__(256)
 logdet_partials_kernel(const double* __restrict__ tiles, int ts, int nt, int n, double* __restrict__ partial) {
-  __shared__ double red[256];
   const int k = blockIdx.x;
-  const double* T = tiles + tile_slot(k, k, nt) * (long long)ts * ts;
-  double acc = 0.0;
-  for (int r = threadIdx.x; r < ts; r += blockDim.x) {
-    if (k * ts + r < n) {
-      const double d = T[(long long)r * ts + r];
-      if (d > 0.0) acc += log(d);
-    }
-  }
-  const double s = block_sum_256(acc, red);
+  const int rows = min(ts, n - k * ts);
+  const double s = logdet_tile_body(tiles + tile_slot(k, k, nt) * (long long)ts * ts, ts, rows);
   if (threadIdx.x == 0) partial[k] = s;
 }
 
@@ -318,27 +164,11 @@ void launch_logdet_partials(const double* tiles, int ts, int nt, int n, double* 
   logdet_partials_kernel<<<nt, 256, 0, st>>>(tiles, ts, nt, n, partial);
 }
 
-// result[0] = log-likelihood, result[1] = log|C|, result[2] = Z^T C^-1 Z (after trsv),
-// following ChameleonImplementation.cpp:188-192 and :257-265:
-//   logdet = 2 * sum log L_kk,  loglik = -0.5 dot - 0.5 logdet - (n/2) log(2 pi).
+// result = (log-likelihood, log|C|, Z^T C^-1 Z after the solve, info) (finalize_body).
 __global__ void __launch_bounds__(256)
 finalize_kernel(const double* __restrict__ partial, int nt, const double* __restrict__ z, int n,
                 double* __restrict__ result, const int* __restrict__ info) {
-  __shared__ double red[256];
-  double acc = 0.0;
-  for (int r = threadIdx.x; r < n; r += blockDim.x) acc = fma(z[r], z[r], acc);
-  const double dot = block_sum_256(acc, red);
-  if (threadIdx.x == 0) {
-    double det = 0.0;
-    for (int k = 0; k < nt; ++k) det += partial[k];
-    const double logdet = 2.0 * det;
-    const double pi = 3.141592653589793;
-    const double nn = (double)n;
-    result[0] = -0.5 * dot - 0.5 * logdet - (double)(nn / 2.0) * log(2.0 * pi);
-    result[1] = logdet;
-    result[2] = dot;
-    result[3] = (double)(info ? *info : 0);
-  }
+  finalize_body(partial, nt, z, n, result, info);
 }
 
 void launch_finalize(const double* partial, int nt, const double* z, int n, double* result, const int* info,

@@ -182,7 +182,7 @@ EGS_API int egs_problem_stage_stats(egs_problem* p, double* ms, double* flops, l
  * memory, work is the 16-byte aligned device workspace (overwritten), and the
  * log-likelihood is written to the host double *loglik.  It calls no
  * cudaMalloc, cudaFree or other allocating routine: its small per-call state
- * lives in one static device array of about 33 KB that every GPU which loads
+ * lives in one static device array of about 41 KB that every GPU which loads
  * the library keeps until the process exits.  The first call on a device looks
  * up that array's device address, so make this first call before any stream
  * capture.  All calls share the array: calls whose work overlaps on the GPU
@@ -197,6 +197,40 @@ EGS_API int egs_mle_eval_noalloc(int n, int dts, const double* x, const double* 
  * problem as one CUDA graph (captured once; disabled while profiling).  enable = 0
  * turns replay off for this problem, 1 (the default) on. */
 EGS_API int egs_problem_set_graphs(egs_problem* p, int enable);
+
+/* ---- batched evaluation of many independent problems -------------------- */
+
+/* No counterpart in the reference, which evaluates one problem per call of
+ * ExaGeoStatMLETile (ChameleonImplementation.cpp:35-327).  A batch holds B
+ * independent problems (problem i: n[i] points, caller arrays concatenated in
+ * order in x, y, z, host memory) factored with one common tile size
+ * (round-up(dts, 64)).  Every stage runs once per batch: one tile pool and one
+ * TMA descriptor for all problems, the 64x64 potrf, row solves and
+ * tensor-core updates of all problems still active at step k in one launch
+ * each.  From the second egs_batch_eval on, the whole batched evaluation is one
+ * CUDA graph replay.  Results are the same formulas as egs_mle_eval per
+ * problem; the tile size can differ from a single-problem call with another dts,
+ * so results agree to rounding, not bit for bit. */
+typedef struct egs_batch egs_batch;
+EGS_API int egs_batch_create(egs_batch** out, int B, const int* n, int dts, const double* x, const double* y,
+                             const double* z);
+EGS_API int egs_batch_destroy(egs_batch* b);
+/* Common tile size, tile rows of the largest problem, device bytes held, and
+ * kernel launches of one evaluation (0 before the first). */
+EGS_API int egs_batch_info(const egs_batch* b, int* ts, int* nt_max, long long* bytes,
+                           long long* launches_per_eval);
+/* theta: 3*B host doubles (sigma^2, beta, nu of problem i at 3i); loglik: B
+ * host doubles; status (may be NULL): B ints, 0 or the potrf info of problem i
+ * (1-based column of the first non-positive pivot).  Returns EGS_OK, or
+ * EGS_ERR_STATE when at least one problem was not positive definite (the other
+ * problems' results are still valid). */
+EGS_API int egs_batch_eval(egs_batch* b, const double* theta, double* loglik, int* status);
+/* Times one graph-replayed evaluation for each candidate tile size and returns
+ * the fastest in *best_ts (device milliseconds of that evaluation in *best_ms,
+ * may be NULL). */
+EGS_API int egs_batch_autotune(int B, const int* n, const double* x, const double* y, const double* z,
+                               const double* theta, const int* candidates, int ncand, int* best_ts,
+                               double* best_ms);
 
 /* ---- kernel plugin ------------------------------------------------------ */
 
