@@ -73,6 +73,7 @@ SIGNATURES = {
     "egs_batch_info": (ctypes.c_int, [_P, _I, _I, _LL, _LL]),
     "egs_batch_eval": (ctypes.c_int, [_P, _D, _D, _I]),
     "egs_batch_autotune": (ctypes.c_int, [ctypes.c_int, _I, _D, _D, _D, _D, _I, ctypes.c_int, _I, _D]),
+    "egs_split_update": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P, _D]),
 }
 
 OBJECTIVE = ctypes.CFUNCTYPE(ctypes.c_double, ctypes.c_int, _D, ctypes.c_void_p)
@@ -363,3 +364,12 @@ def batch_autotune(sizes, x, y, z, theta, candidates=(128, 192, 256, 320)):
                                   _dptr(th), cand.ctypes.data_as(_I), len(cand), ctypes.byref(best),
                                   ctypes.byref(ms)), "egs_batch_autotune")
     return best.value, ms.value
+
+
+def split_update(ts: int, nt: int, band: int, k: int, panel_ptr: int, offband_ptr: int) -> float:
+    """egs_split_update on device pointers; returns the kernel's device milliseconds."""
+    lib = load_library()
+    ms = ctypes.c_double()
+    _check(lib.egs_split_update(int(ts), int(nt), int(band), int(k), _P(panel_ptr), _P(offband_ptr),
+                                ctypes.byref(ms)), "egs_split_update")
+    return ms.value

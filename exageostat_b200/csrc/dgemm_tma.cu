@@ -28,6 +28,7 @@
 #include <cstdint>
 #include "common.cuh"
 #include "kernels.cuh"
+#include "mbarrier.cuh"
 
 namespace egs {
 
@@ -50,65 +51,6 @@ constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 2 * STAGES * 8 + 1024;
 constexpr int GROUP = 8;                              // block-columns per raster group
 }  // namespace gemm
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-__device__ __forceinline__ uint64_t global_ns() {
-  uint64_t t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-// Bounded wait: gives up after kSpinLimit polls or about two seconds.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
-  long long n = 0;
-  uint64_t t0 = 0;
-  while (!mbar_try_wait(bar, parity)) {
-    ++n;
-    if ((n & 1023) == 0) {
-      const uint64_t now = global_ns();
-      if (t0 == 0) {
-        t0 = now;
-      } else if (now - t0 > 2000000000ull) {
-        atomicOr(err, 1);
-        return false;
-      }
-    }
-    if (n > kSpinLimit) {
-      atomicOr(err, 1);
-      return false;
-    }
-  }
-  return true;
-}
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y,
-                                            int z) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
-      "[%5];" ::"r"(smem_u32(dst)),
-      "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
-      : "memory");
-}
 __device__ __forceinline__ double lds_f64(uint32_t addr) {
   double v;
   asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(addr));
@@ -409,17 +351,25 @@ dgemm_update_kernel(const __grid_constant__ CUtensorMap tmap, double* __restrict
 
 static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 
-int gemm_init_tensor_map(void* tmap_storage, double* tiles, int ts, long long ntiles) {
+int tensor_map_encoder(void** fn_out) {
   if (!g_encode) {
     cudaDriverEntryPointQueryResult q;
     void* fn = nullptr;
     if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
         q != cudaDriverEntryPointSuccess || !fn) {
-      set_last_error("cuTensorMapEncodeTiled unavailable", "gemm_init_tensor_map");
+      cudaGetLastError();
+      set_last_error("cuTensorMapEncodeTiled unavailable", "tensor_map_encoder");
       return EGS_ERR_CUDA;
     }
     g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
   }
+  *fn_out = reinterpret_cast<void*>(g_encode);
+  return EGS_OK;
+}
+
+int gemm_init_tensor_map(void* tmap_storage, double* tiles, int ts, long long ntiles) {
+  void* fn = nullptr;
+  if (tensor_map_encoder(&fn) != EGS_OK) return EGS_ERR_CUDA;
   if (ts % 64 != 0 || ((uintptr_t)tiles & 15) != 0) return EGS_ERR_INVALID;
   cuuint64_t dims[3] = {(cuuint64_t)ts, (cuuint64_t)ts, (cuuint64_t)ntiles};
   cuuint64_t strides[2] = {(cuuint64_t)ts * 8, (cuuint64_t)ts * ts * 8};

@@ -62,6 +62,8 @@ void finish_desc(GemmDesc& d);  // fills MB, NB, total
 int launch_gemm_batched(const void* tmap, double* tiles, const GemmDesc* jobs, const long long* begin, int njobs,
                         long long total, int* err, cudaStream_t st);
 int gemm_init_tensor_map(void* tmap_storage, double* tiles, int ts, long long ntiles);
+// The driver's cuTensorMapEncodeTiled (looked up once).
+int tensor_map_encoder(void** fn);
 int launch_gemm_trailing(const void* tmap, double* tiles, int ts, int nt, int k, int* err, cudaStream_t st);
 int launch_gemm_rows(const void* tmap, double* tiles, int ts, int nt, int M, int N, int K, int a_row0,
                      int a_col0, int a_tcol, int b_row0, int b_col0, int b_tcol, int c_row0, int c_col0,

@@ -1,0 +1,483 @@
+// Off-band trailing update of the mixed-precision factorisation on the
+// 5th-generation tensor cores (tcgen05, sm_100a), with FP32 accuracy from
+// FP16 operands.
+//
+// At step k every off-band target tile (i, j), k < j, j + band < i, is updated
+// C_ij -= L_ik L_jk^T with C stored in FP32.  The solved panel column
+// (FP64) is first split per row into two FP16 parts after a power-of-two row
+// scaling s_r (max |s_r L_r.| in [2^13, 2^14)):
+//     hi = fp16(s L),  lo = fp16(s L - hi),   s L = hi + lo + O(2^-22 |s L|),
+// and the product is assembled from three FP16 tensor-core products with FP32
+// accumulation in tensor memory,
+//     (s_a a)(s_b b) ~ hi_a hi_b + hi_a lo_b + lo_a hi_b,
+// then unscaled exactly (powers of two) in the epilogue.  The dropped lo*lo
+// term is O(2^-22) relative, so the update has FP32-level accuracy while it
+// runs on the FP16 tensor path (kind::f16).  Per-row scaling keeps the FP16
+// parts in range whatever the magnitude of the factor's rows.
+//
+// Kernel structure (one CTA per SM, persistent over 128 x 256 output tiles):
+//   warp 0    TMA producer: per 64-wide K stage, the A rows (hi, lo) and B rows
+//             (hi, lo) of the tile, 128B-swizzled, into a 2-stage ring;
+//   warp 1    allocates 512 TMEM columns (two 128 x 256 FP32 accumulators) and
+//             issues the tcgen05.mma instructions from one thread; commits
+//             release the ring stage and, after the last stage, hand the
+//             accumulator to the epilogue;
+//   warps 2-5 epilogue: tcgen05.ld of the accumulator (thread = tile row),
+//             C -= acc * inv_s_row * inv_s_col, coalesced along each column.
+// The two accumulators let the MMAs of tile t+1 overlap the epilogue of tile t.
+// Every mbarrier wait is bounded; a timed-out CTA records the error, stops, and
+// still frees its tensor memory.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_fp16.h>
+#include <cstdint>
+#include "common.cuh"
+#include "kernels.cuh"
+#include "mbarrier.cuh"
+
+namespace egs {
+
+namespace sg {
+constexpr int BM = 128, BN = 256, BK = 64, STAGES = 2;
+constexpr int BOX_ROWS = 128;                      // TMA box: 64 fp16 (128 B) x 128 rows
+constexpr int A_BYTES = BM * BK * 2;               // 16 KB
+constexpr int B_BYTES = BN * BK * 2;               // 32 KB
+constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+constexpr int THREADS = 192;
+constexpr int SMEM_BYTES = 1024 + STAGES * STAGE_BYTES + 256;
+constexpr uint32_t TMEM_COLS = 512;
+// Instruction descriptor of kind::f16: D F32 (bits 4-5 = 1), A and B F16 (0),
+// both K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28.
+constexpr uint32_t IDESC = (1u << 4) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+}  // namespace sg
+
+// ---------------------------------------------------------------------------
+// Row scaling and FP16 split of a solved panel
+// ---------------------------------------------------------------------------
+
+// Power-of-two scale of row r of panel tile t: inv_scale = 2^(e - 13) with
+// 2^e <= max_c |W(r, c)| < 2^(e+1); rows whose maximum is 0 (or below 2^-120)
+// get inv_scale 0 and split to zeros.  W: column-major ts x ts tiles.
+__global__ void __launch_bounds__(256)
+panel_rowscale_kernel(const double* __restrict__ W, int ts, int t0, int row_tile0, float* __restrict__ inv_scale) {
+  __shared__ double red[4][64];
+  const int t = t0 + blockIdx.y;
+  const int rl = threadIdx.x & 63, g = threadIdx.x >> 6;
+  const int r = blockIdx.x * 64 + rl;
+  const double* col = W + (long long)t * ts * ts + r;
+  double m = 0.0;
+  for (int c = g; c < ts; c += 4) m = fmax(m, fabs(col[(long long)c * ts]));
+  red[g][rl] = m;
+  __syncthreads();
+  if (g == 0) {
+    m = fmax(fmax(red[0][rl], red[1][rl]), fmax(red[2][rl], red[3][rl]));
+    const long long bits = __double_as_longlong(m);
+    const int e = (int)((bits >> 52) & 0x7FF) - 1023;
+    float inv;
+    if (e == 1024) {
+      inv = __int_as_float(0x7fc00000);  // NaN or Inf in the row: propagate
+    } else if (!(m > 0.0) || e < -120) {
+      inv = 0.0f;
+    } else {
+      inv = __int_as_float((e - 13 + 127) << 23);  // 2^(e-13), e <= 1023 - 13 keeps it finite for e <= 140
+    }
+    inv_scale[(long long)(row_tile0 + t) * ts + r] = inv;
+  }
+}
+
+// hi/lo FP16 parts of 64 x 64 blocks of panel tiles, transposed to row-major
+// (K contiguous) rows of Ph / Pl (row stride ts).
+__global__ void __launch_bounds__(256)
+panel_split_kernel(const double* __restrict__ W, int ts, int t0, int row_tile0, const float* __restrict__ inv_scale,
+                   __half* __restrict__ Ph, __half* __restrict__ Pl) {
+  __shared__ double S[64][65];
+  const int t = t0 + blockIdx.z;
+  const int r0 = blockIdx.x * 64, c0 = blockIdx.y * 64;
+  const double* src = W + (long long)t * ts * ts;
+  for (int e = threadIdx.x; e < 64 * 64; e += 256) {
+    const int r = e & 63, c = e >> 6;
+    S[r][c] = src[(long long)(c0 + c) * ts + r0 + r];
+  }
+  __syncthreads();
+  const long long grow0 = (long long)(row_tile0 + t) * ts + r0;
+  for (int e = threadIdx.x; e < 64 * 32; e += 256) {
+    const int r = e >> 5, c = (e & 31) * 2;
+    const float inv = inv_scale[grow0 + r];
+    const double s = (inv > 0.0f) ? 1.0 / (double)inv : 0.0;  // exact: inv is a power of two
+    const double v0 = S[r][c] * s, v1 = S[r][c + 1] * s;
+    const __half h0 = __double2half(v0), h1 = __double2half(v1);
+    const __half l0 = __double2half(v0 - (double)__half2float(h0));
+    const __half l1 = __double2half(v1 - (double)__half2float(h1));
+    const long long off = (grow0 + r) * ts + c0 + c;
+    *reinterpret_cast<__half2*>(Ph + off) = __halves2half2(h0, h1);
+    *reinterpret_cast<__half2*>(Pl + off) = __halves2half2(l0, l1);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// tcgen05 helpers
+// ---------------------------------------------------------------------------
+
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row atoms of
+// 1024 bytes stacked contiguously (stride byte offset 1024), sm_100 version 1.
+__device__ __forceinline__ uint64_t sdesc_sw128(uint32_t addr) {
+  uint64_t d = (uint64_t)((addr & 0x3FFFF) >> 4);
+  d |= (uint64_t)1 << 16;             // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(1024 >> 4) << 32;   // stride byte offset
+  d |= (uint64_t)1 << 46;             // descriptor version
+  d |= (uint64_t)2 << 61;             // SWIZZLE_128B
+  return d;
+}
+__device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(sg::IDESC), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_u32(dst)),
+      "l"((uint64_t)map), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+// 32 consecutive FP32 columns of this warp's 32 TMEM lanes.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Target tile of work item L at step k: targets are enumerated column by column
+// (j = k+1, ...; i = j+band+1 .. nt-1), each split into (ts/BM) x (ts/BN) CTA
+// tiles with the row block fastest.
+struct SplitStep {
+  int ts, nt, band, k;
+  int mblocks, nblocks;
+  long long total;
+  float* c_pool;            // off-band FP32 tiles: slot(i, j) = tile_slot(i - band - 1, j, nt - band - 1)
+  const float* inv_scale;   // per global row
+  int* err;
+};
+
+__device__ __forceinline__ void decode_item(const SplitStep& P, long long L, int& i, int& j, int& mb, int& nb) {
+  const long long per = (long long)P.mblocks * P.nblocks;
+  long long q = L / per;
+  const int w = (int)(L - q * per);
+  nb = w / P.mblocks;
+  mb = w - nb * P.mblocks;
+  j = P.k + 1;
+  long long cnt = P.nt - j - P.band - 1;
+  while (q >= cnt) {
+    q -= cnt;
+    ++j;
+    --cnt;
+  }
+  i = j + P.band + 1 + (int)q;
+}
+
+__global__ void __launch_bounds__(sg::THREADS, 1)
+split_gemm_kernel(const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo,
+                  const __grid_constant__ SplitStep P) {
+  using namespace sg;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
+  uint64_t* empty = full + STAGES;
+  uint64_t* acc_full = empty + STAGES;
+  uint64_t* acc_empty = acc_full + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 2);
+  __shared__ int bail_flag;
+  volatile int& bail = bail_flag;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&acc_full[b], 1);
+      mbar_init(&acc_empty[b], 4);
+    }
+    bail = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+  const int ksteps = P.ts / BK;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      uint32_t it = 0;
+      for (long long L = blockIdx.x; L < P.total && !bail; L += gridDim.x) {
+        int i, j, mb, nb;
+        decode_item(P, L, i, j, mb, nb);
+        const int arow = i * P.ts + mb * BM, brow = j * P.ts + nb * BN;
+        for (int kt = 0; kt < ksteps; ++kt, ++it) {
+          const uint32_t s = it % STAGES;
+          if (it >= (uint32_t)STAGES && !mbar_wait(&empty[s], ((it / STAGES) & 1) ^ 1, P.err)) {
+            bail = 1;
+            break;
+          }
+          uint8_t* st = smem + s * STAGE_BYTES;
+          mbar_expect_tx(&full[s], STAGE_BYTES);
+          const int x = kt * BK;
+          tma_load_2d(st, &tm_hi, &full[s], x, arow);
+          tma_load_2d(st + A_BYTES, &tm_lo, &full[s], x, arow);
+          tma_load_2d(st + 2 * A_BYTES, &tm_hi, &full[s], x, brow);
+          tma_load_2d(st + 2 * A_BYTES + BOX_ROWS * 128, &tm_hi, &full[s], x, brow + BOX_ROWS);
+          tma_load_2d(st + 2 * A_BYTES + B_BYTES, &tm_lo, &full[s], x, brow);
+          tma_load_2d(st + 2 * A_BYTES + B_BYTES + BOX_ROWS * 128, &tm_lo, &full[s], x, brow + BOX_ROWS);
+        }
+      }
+      // drain: the stages issued last must land before the CTA may exit
+      const uint32_t first = it > (uint32_t)STAGES ? it - STAGES : 0;
+      for (uint32_t q = first; q < it; ++q) mbar_wait(&full[q % STAGES], (q / STAGES) & 1, P.err);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      uint32_t it = 0, tcount = 0;
+      for (long long L = blockIdx.x; L < P.total && !bail; L += gridDim.x, ++tcount) {
+        const uint32_t ab = tcount & 1;
+        if (tcount >= 2 && !mbar_wait(&acc_empty[ab], ((tcount >> 1) & 1) ^ 1, P.err)) {
+          bail = 1;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t dcol = tmem_base + ab * BN;
+        bool ok = true;
+        for (int kt = 0; kt < ksteps; ++kt, ++it) {
+          const uint32_t s = it % STAGES;
+          if (!mbar_wait(&full[s], (it / STAGES) & 1, P.err)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t sa = smem_u32(smem + s * STAGE_BYTES);
+          const uint32_t sal = sa + A_BYTES, sbh = sa + 2 * A_BYTES, sbl = sbh + B_BYTES;
+#pragma unroll
+          for (int kk = 0; kk < BK / 16; ++kk) {
+            const uint32_t off = kk * 32;
+            const uint32_t acc = (kt > 0 || kk > 0) ? 1u : 0u;
+            umma_f16(dcol, sdesc_sw128(sa + off), sdesc_sw128(sbh + off), acc);
+            umma_f16(dcol, sdesc_sw128(sa + off), sdesc_sw128(sbl + off), 1u);
+            umma_f16(dcol, sdesc_sw128(sal + off), sdesc_sw128(sbh + off), 1u);
+          }
+          umma_commit(&empty[s]);
+        }
+        if (!ok) {
+          bail = 1;
+          break;
+        }
+        umma_commit(&acc_full[ab]);
+      }
+    }
+  } else {
+    // epilogue warps 2..5: TMEM lane quarter = warp % 4
+    const int quarter = warp & 3;
+    const int row = quarter * 32 + lane;
+    uint32_t tcount = 0;
+    for (long long L = blockIdx.x; L < P.total; L += gridDim.x, ++tcount) {
+      const uint32_t ab = tcount & 1;
+      // one lane waits, the warp follows it uniformly (tcgen05.ld needs the whole warp)
+      int ok = 1;
+      if (lane == 0) ok = mbar_wait(&acc_full[ab], (tcount >> 1) & 1, P.err) ? 1 : 0;
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!ok) {
+        bail = 1;
+        break;
+      }
+      tc_fence_after();
+      int i, j, mb, nb;
+      decode_item(P, L, i, j, mb, nb);
+      const int mm = P.nt - P.band - 1;
+      float* C = P.c_pool + tile_slot(i - P.band - 1, j, mm) * (long long)P.ts * P.ts;
+      const int r = mb * BM + row;
+      const float inv_r = P.inv_scale[(long long)i * P.ts + r];
+      const float* inv_c = P.inv_scale + (long long)j * P.ts + nb * BN;
+      float* cp = C + (long long)(nb * BN) * P.ts + r;
+      const long long ld = P.ts;
+      // 32 columns per chunk; the C loads of the next chunk are issued before the
+      // current chunk is finished, so about 64 independent loads are in flight.
+      float cv[32], cn[32];
+#pragma unroll
+      for (int c = 0; c < 32; ++c) cv[c] = __ldcg(cp + c * ld);
+#pragma unroll 1
+      for (int c0 = 0; c0 < BN; c0 += 32) {
+        if (c0 + 32 < BN) {
+#pragma unroll
+          for (int c = 0; c < 32; ++c) cn[c] = __ldcg(cp + (c0 + 32 + c) * ld);
+        }
+        float v[32];
+        tmem_ld32(tmem_base + ((uint32_t)(quarter * 32) << 16) + ab * BN + c0, v);
+#pragma unroll
+        for (int c = 0; c < 32; ++c) __stcg(cp + (c0 + c) * ld, fmaf(-(v[c] * inv_r), __ldg(inv_c + c0 + c), cv[c]));
+#pragma unroll
+        for (int c = 0; c < 32; ++c) cv[c] = cn[c];
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acc_empty[ab]);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    __syncwarp();
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS) : "memory");
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+
+int split_tensor_map(void* storage, const __half* base, int ts, long long rows) {
+  void* fn = nullptr;
+  if (tensor_map_encoder(&fn) != EGS_OK) return EGS_ERR_CUDA;
+  if (ts % 64 != 0 || ((uintptr_t)base & 15) != 0) return EGS_ERR_INVALID;
+  auto encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  cuuint64_t dims[2] = {(cuuint64_t)ts, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)ts * 2};
+  cuuint32_t box[2] = {sg::BK, sg::BOX_ROWS};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = encode(reinterpret_cast<CUtensorMap*>(storage), CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2,
+                      const_cast<__half*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                      CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_last_error("cuTensorMapEncodeTiled failed", "split_tensor_map");
+    return EGS_ERR_CUDA;
+  }
+  return EGS_OK;
+}
+
+void launch_panel_split(const double* W, int ts, int t0, int ntiles, int row_tile0, float* inv_scale, __half* Ph,
+                        __half* Pl, cudaStream_t st) {
+  if (ntiles <= 0) return;
+  panel_rowscale_kernel<<<dim3(ts / 64, ntiles), 256, 0, st>>>(W, ts, t0, row_tile0, inv_scale);
+  panel_split_kernel<<<dim3(ts / 64, ts / 64, ntiles), 256, 0, st>>>(W, ts, t0, row_tile0, inv_scale, Ph, Pl);
+}
+
+// Number of off-band target tiles at step k.
+long long split_targets(int nt, int band, int k) {
+  long long n = 0;
+  for (int j = k + 1; j < nt; ++j) {
+    const int c = nt - j - band - 1;
+    if (c > 0) n += c;
+  }
+  return n;
+}
+
+int launch_split_update(const void* tm_hi, const void* tm_lo, int ts, int nt, int band, int k, float* c_pool,
+                        const float* inv_scale, int* err, cudaStream_t st) {
+  using namespace sg;
+  if (ts % BN != 0) return EGS_ERR_INVALID;
+  const long long targets = split_targets(nt, band, k);
+  if (targets == 0) return EGS_OK;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(split_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    attr = true;
+  }
+  SplitStep P;
+  P.ts = ts;
+  P.nt = nt;
+  P.band = band;
+  P.k = k;
+  P.mblocks = ts / BM;
+  P.nblocks = ts / BN;
+  P.total = targets * P.mblocks * P.nblocks;
+  P.c_pool = c_pool;
+  P.inv_scale = inv_scale;
+  P.err = err;
+  const long long grid = P.total < gemm_num_sms() ? P.total : gemm_num_sms();
+  split_gemm_kernel<<<(unsigned)grid, THREADS, SMEM_BYTES, st>>>(*reinterpret_cast<const CUtensorMap*>(tm_hi),
+                                                                 *reinterpret_cast<const CUtensorMap*>(tm_lo), P);
+  return cudaGetLastError() == cudaSuccess ? EGS_OK : EGS_ERR_CUDA;
+}
+
+}  // namespace egs
+
+using namespace egs;
+
+extern "C" int egs_split_update(int ts, int nt, int band, int k, const double* panel, float* offband, double* ms) {
+  if (ts <= 0 || ts % sg::BN != 0 || nt <= 0 || band < 0 || k < -1 || k >= nt || !panel || !offband)
+    return EGS_ERR_INVALID;
+  const long long rows = (long long)nt * ts;
+  __half *ph = nullptr, *pl = nullptr;
+  float* inv = nullptr;
+  int* err = nullptr;
+  alignas(64) unsigned char tmh[128], tml[128];
+  int rc = EGS_OK;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaMalloc(&ph, rows * ts * sizeof(__half)) || cudaMalloc(&pl, rows * ts * sizeof(__half)) ||
+      cudaMalloc(&inv, rows * sizeof(float)) || cudaMalloc(&err, sizeof(int))) {
+    cudaGetLastError();
+    rc = EGS_ERR_OOM;
+    goto done;
+  }
+  cudaMemset(err, 0, sizeof(int));
+  cudaMemset(inv, 0, rows * sizeof(float));
+  cudaMemset(ph, 0, rows * ts * sizeof(__half));
+  cudaMemset(pl, 0, rows * ts * sizeof(__half));
+  if ((rc = split_tensor_map(tmh, ph, ts, rows)) != EGS_OK || (rc = split_tensor_map(tml, pl, ts, rows)) != EGS_OK)
+    goto done;
+  launch_panel_split(panel, ts, k + 1, nt - k - 1, 0, inv, ph, pl, 0);
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, 0);
+  if ((rc = launch_split_update(tmh, tml, ts, nt, band, k, offband, inv, err, 0)) != EGS_OK) goto done;
+  cudaEventRecord(e1, 0);
+  if (cudaDeviceSynchronize() != cudaSuccess) {
+    rc = EGS_ERR_CUDA;
+    set_last_error(cudaGetErrorString(cudaGetLastError()), "egs_split_update");
+    goto done;
+  }
+  {
+    int h = 0;
+    cudaMemcpy(&h, err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (h) {
+      set_last_error("a device-side wait exceeded its limit", "egs_split_update");
+      rc = EGS_ERR_TIMEOUT;
+    }
+    float t = 0.f;
+    cudaEventElapsedTime(&t, e0, e1);
+    if (ms) *ms = t;
+  }
+done:
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(ph);
+  cudaFree(pl);
+  cudaFree(inv);
+  cudaFree(err);
+  return rc;
+}

@@ -232,6 +232,20 @@ EGS_API int egs_batch_autotune(int B, const int* n, const double* x, const doubl
                                const double* theta, const int* candidates, int ncand, int* best_ts,
                                double* best_ms);
 
+/* ---- mixed-precision building block --------------------------------------- */
+
+/* No counterpart in the reference.  One step k of the off-band trailing update
+ * of the mixed-precision factorisation, on caller device memory: panel holds nt
+ * column-major ts x ts FP64 tiles (tile t = rows t*ts.. of the solved panel
+ * column; tiles <= k are not read), offband the FP32 off-band tiles
+ * (i, j), i - j > band, in lower-tile order over nt - band - 1 tile rows.  Every
+ * target (i, j) with k < j, j + band < i < nt gets C -= P_i P_j^T computed from
+ * a per-row scaled two-part FP16 split of the panel on the tcgen05 tensor cores
+ * (FP32 accumulation; about 2^-22 relative).  ts must be a multiple of 256;
+ * k = -1 updates every off-band tile.  *ms (may be NULL) receives the device
+ * time of the update kernel.  Allocates and frees its scratch per call. */
+EGS_API int egs_split_update(int ts, int nt, int band, int k, const double* panel, float* offband, double* ms);
+
 /* ---- kernel plugin ------------------------------------------------------ */
 
 /* rows x cols column-major block (leading dimension lda) on caller device
