@@ -22,6 +22,8 @@ EGS_ERR_NO_DEVICE = -3
 EGS_ERR_OOM = -4
 EGS_ERR_TIMEOUT = -5
 EGS_ERR_STATE = -6
+EGS_PRECISION_DOUBLE = 1
+EGS_PRECISION_MIXED = 2
 
 STAGES = ("generate", "panel", "update", "solve", "reduce")
 NUM_STAGES = len(STAGES)
@@ -43,6 +45,7 @@ SIGNATURES = {
     "egs_problem_set_stream": (ctypes.c_int, [_P, _P]),
     "egs_problem_set_band": (ctypes.c_int, [_P, ctypes.c_int]),
     "egs_problem_set_graphs": (ctypes.c_int, [_P, ctypes.c_int]),
+    "egs_problem_set_precision": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int]),
     "egs_problem_set_locations": (ctypes.c_int, [_P, _D, _D]),
     "egs_problem_set_locations_device": (ctypes.c_int, [_P, _P, _P]),
     "egs_problem_set_observations": (ctypes.c_int, [_P, _D]),
@@ -227,6 +230,13 @@ class Problem:
         ln = (ctypes.c_longlong * NUM_STAGES)()
         _check(self._lib.egs_problem_stage_stats(self._h, _dptr(ms), _dptr(fl), ln), "stage_stats")
         return ms, fl, np.array(list(ln), dtype=np.int64)
+
+    def set_precision(self, precision: int, band_tiles: int = 0) -> None:
+        """EGS_PRECISION_DOUBLE or EGS_PRECISION_MIXED (FP64 band of band_tiles tile rows)."""
+        _check(self._lib.egs_problem_set_precision(self._h, int(precision), int(band_tiles)), "set_precision")
+        nn, ts, nt, nb = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()
+        self._lib.egs_problem_info(self._h, ctypes.byref(nn), ctypes.byref(ts), ctypes.byref(nt), ctypes.byref(nb))
+        self.ts, self.nt, self.bytes = ts.value, nt.value, nb.value
 
     def set_stream(self, cuda_stream_handle) -> None:
         _check(self._lib.egs_problem_set_stream(self._h, _P(cuda_stream_handle)), "set_stream")

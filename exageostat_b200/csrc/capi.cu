@@ -76,11 +76,37 @@ struct egs_problem {
   double stage_ms[EGS_NUM_STAGES] = {};
   double stage_flops[EGS_NUM_STAGES] = {};
   long long stage_launches[EGS_NUM_STAGES] = {};
+  // Mixed precision (precision == EGS_PRECISION_MIXED): FP64 band of mband tile
+  // rows below the diagonal, FP32 off-band tiles; see mixed.cu for the layout.
+  int precision = EGS_PRECISION_DOUBLE;
+  int mband = 0;
+  double* band_pool = nullptr;
+  float* off_pool = nullptr;
+  double* W = nullptr;        // one FP64 tile column (panel workspace)
+  __half* ph = nullptr;       // FP16 split of the solved panel rows (hi, lo)
+  __half* pl = nullptr;
+  float* inv_scale = nullptr; // per panel row
+  double* w = nullptr;        // refinement vector
+  double* res_scratch = nullptr;
+  int4* gen_tiles = nullptr;  // (i, j, pool, slot) of every generated tile
+  long long ngen = 0;
+  GemmDesc* band_jobs = nullptr;
+  long long* band_begin = nullptr;
+  struct JobLaunch {
+    long long job_off, begin_off;
+    int njobs;
+    long long total;
+  };
+  std::vector<JobLaunch> band_launch;  // per step k
+  alignas(64) unsigned char tmapW[128];
+  alignas(64) unsigned char tm_hi[128];
+  alignas(64) unsigned char tm_lo[128];
 };
 
 namespace {
 
 constexpr int kInnerBlock = 64;
+constexpr int kPrecisionBroken = -1;  // egs_problem_set_precision failed part-way
 
 int round_tile(int dts) {
   int ts = dts < kInnerBlock ? kInnerBlock : dts;
@@ -150,6 +176,23 @@ int dev_alloc(T** p, size_t count, long long* bytes) {
   return EGS_OK;
 }
 
+void free_mixed(egs_problem* p) {
+  void* bufs[] = {p->band_pool, p->off_pool, p->W, p->ph, p->pl, p->inv_scale, p->w, p->res_scratch,
+                  p->gen_tiles, p->band_jobs, p->band_begin};
+  for (void* b : bufs) cudaFree(b);
+  p->band_pool = nullptr;
+  p->off_pool = nullptr;
+  p->W = nullptr;
+  p->ph = p->pl = nullptr;
+  p->inv_scale = nullptr;
+  p->w = p->res_scratch = nullptr;
+  p->gen_tiles = nullptr;
+  p->band_jobs = nullptr;
+  p->band_begin = nullptr;
+  p->band_launch.clear();
+  p->ngen = 0;
+}
+
 void free_problem(egs_problem* p) {
   if (!p) return;
   if (p->stream) cudaStreamSynchronize(p->stream);
@@ -163,6 +206,7 @@ void free_problem(egs_problem* p) {
   cudaFree(p->flags);
   cudaFree(p->dparams);
   cudaFree(p->ktab);
+  free_mixed(p);
   cudaFreeHost(p->hparams);
   cudaFreeHost(p->hresult);
   cudaFreeHost(p->hflags);
@@ -355,7 +399,10 @@ int sync_flags(egs_problem* p, bool want_result) {
 // Device work of one evaluation after the parameter record is on the device:
 // Z <- Zcpy, generation, factorisation, log-det, solve, assembly, and the copy
 // of the result record and status words to the pinned host mirrors.
+int enqueue_eval_mixed(egs_problem* p);
+
 int enqueue_eval(egs_problem* p) {
+  if (p->precision == EGS_PRECISION_MIXED) return enqueue_eval_mixed(p);
   cudaStream_t st = p->stream;
   EGS_CUDA_TRY(cudaMemsetAsync(p->flags, 0, 2 * sizeof(int), st));
   EGS_CUDA_TRY(cudaMemcpyAsync(p->z, p->zcpy, p->np * sizeof(double), cudaMemcpyDeviceToDevice, st));
@@ -378,6 +425,210 @@ int enqueue_eval(egs_problem* p) {
   EGS_CUDA_TRY(cudaMemcpyAsync(p->hflags, p->flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
   EGS_CUDA_TRY(cudaMemcpyAsync(p->hresult, p->result, 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
   return check_cuda("egs_mle_eval");
+}
+
+// Mixed-precision evaluation.  Step k: gather tile column k into the FP64
+// workspace W, factor and solve it there (the FP64 panel kernels with W as a
+// one-column problem), scatter it back (off-band tiles rounded to FP32), split
+// its rows for the FP16 tensor-core update, then update the band targets with
+// FP64 DMMA and the off-band targets with the split tcgen05 kernel.  After the
+// factorisation: log-det from the FP64 diagonal tiles, v = (L L^T)^-1 z, one
+// refinement step with the FP64 residual z - C v, and the assembly with
+// z^T (v + w).
+int enqueue_eval_mixed(egs_problem* p) {
+  cudaStream_t st = p->stream;
+  const int ts = p->ts, nt = p->nt, n = p->n, b = p->mband;
+  int* info = p->flags;
+  int* err = p->flags + 1;
+  EGS_CUDA_TRY(cudaMemsetAsync(p->flags, 0, 2 * sizeof(int), st));
+  EGS_CUDA_TRY(cudaMemcpyAsync(p->z, p->zcpy, p->np * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  int sp = span_begin(p, EGS_STAGE_GENERATE);
+  launch_matern_mixed(p->band_pool, p->off_pool, p->x, p->y, n, ts, p->gen_tiles, p->ngen, p->dparams, p->ktab, st);
+  count_launches(p, EGS_STAGE_GENERATE, 1 + (p->ngen + 65534) / 65535);
+  span_end(p, sp, 0.0);
+  for (int k = 0; k < nt; ++k) {
+    const int ntp = nt - k;
+    sp = span_begin(p, EGS_STAGE_PANEL);
+    launch_gather_column(p->band_pool, p->off_pool, p->W, ts, nt, b, k, st);
+    long long nl = 1;
+    for (int kb = 0; kb < ts; kb += kInnerBlock) {
+      launch_potrf_diag_block(p->W, ts, 0, kb, k * ts, info, st);
+      ++nl;
+      if (kb + kInnerBlock < ts) {
+        const int r0 = kb + kInnerBlock, m = ts - kb - kInnerBlock;
+        launch_trsm_rows(p->W, ts, 0, 1, r0, kb, 0, st);
+        int rc = launch_gemm_rows(p->tmapW, p->W, ts, ntp, m, m, kInnerBlock, r0, kb, 0, r0, kb, 0, r0, r0, 1, err, st);
+        if (rc != EGS_OK) return rc;
+        nl += 2;
+      }
+    }
+    if (ntp > 1) {
+      for (int kb = 0; kb < ts; kb += kInnerBlock) {
+        launch_trsm_rows(p->W, ts, 1, ntp - 1, 0, kb, 0, st);
+        ++nl;
+        if (kb + kInnerBlock < ts) {
+          const int brow = kb + kInnerBlock;
+          int rc = launch_gemm_rows(p->tmapW, p->W, ts, ntp, (ntp - 1) * ts, ts - brow, kInnerBlock, ts, kb, 0,
+                                    brow, kb, 0, ts, brow, 0, err, st);
+          if (rc != EGS_OK) return rc;
+          ++nl;
+        }
+      }
+    }
+    launch_scatter_column(p->W, p->band_pool, p->off_pool, ts, nt, b, k, st);
+    ++nl;
+    if (ntp > 1) {
+      launch_panel_split(p->W, ts, 1, ntp - 1, k, p->inv_scale, p->ph, p->pl, st);
+      nl += 2;
+    }
+    count_launches(p, EGS_STAGE_PANEL, nl);
+    {
+      const double wd = (double)std::min(ts, n - k * ts);
+      const double below = (double)std::max(0, n - (k + 1) * ts);
+      span_end(p, sp, wd * wd * wd / 3.0 + wd * wd / 2.0 + wd / 6.0 + below * wd * wd);
+    }
+    if (ntp > 1) {
+      sp = span_begin(p, EGS_STAGE_UPDATE);
+      const egs_problem::JobLaunch& L = p->band_launch[k];
+      if (L.njobs > 0 && L.total > 0) {
+        int rc = launch_gemm_batched(p->tmapW, p->band_pool, p->band_jobs + L.job_off, p->band_begin + L.begin_off,
+                                     L.njobs, L.total, err, st);
+        if (rc != EGS_OK) return rc;
+        count_launches(p, EGS_STAGE_UPDATE, 1);
+      }
+      if (split_targets(nt, b, k) > 0) {
+        int rc = launch_split_update(p->tm_hi, p->tm_lo, ts, nt, b, k, p->off_pool, p->inv_scale, err, st);
+        if (rc != EGS_OK) return rc;
+        count_launches(p, EGS_STAGE_UPDATE, 1);
+      }
+      const double m = (double)std::max(0, n - (k + 1) * ts);
+      span_end(p, sp, m * (m + 1.0) * (double)ts);
+    }
+  }
+  sp = span_begin(p, EGS_STAGE_REDUCE);
+  launch_logdet_band(p->band_pool, ts, nt, b, n, p->partial, st);
+  count_launches(p, EGS_STAGE_REDUCE, 1);
+  span_end(p, sp, 0.0);
+  sp = span_begin(p, EGS_STAGE_SOLVE);
+  long long ns = 0;
+  launch_mixed_solve(p->band_pool, p->off_pool, ts, nt, b, p->z, st, &ns);
+  launch_matern_residual(p->x, p->y, p->zcpy, p->z, n, p->np, p->dparams, p->ktab, p->res_scratch, p->w, st);
+  launch_mixed_solve(p->band_pool, p->off_pool, ts, nt, b, p->w, st, &ns);
+  count_launches(p, EGS_STAGE_SOLVE, ns + 2);
+  span_end(p, sp, 6.0 * (double)n * (double)n);
+  sp = span_begin(p, EGS_STAGE_REDUCE);
+  launch_finalize_mixed(p->partial, nt, p->zcpy, p->z, p->w, n, p->result, p->flags, st);
+  count_launches(p, EGS_STAGE_REDUCE, 1);
+  span_end(p, sp, 0.0);
+  EGS_CUDA_TRY(cudaMemcpyAsync(p->hflags, p->flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+  EGS_CUDA_TRY(cudaMemcpyAsync(p->hresult, p->result, 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  return check_cuda("egs_mle_eval (mixed)");
+}
+
+// Re-lays a problem out for mixed precision: device tile rounded up to a
+// multiple of 256 (the FP16 update's tile), FP64 band of b tile rows, FP32
+// off-band tiles, workspaces, the generator's tile table and the band update's
+// job tables.
+int setup_mixed(egs_problem* p, int b) {
+  free_mixed(p);
+  cudaFree(p->tiles);
+  cudaFree(p->x);
+  cudaFree(p->y);
+  cudaFree(p->z);
+  cudaFree(p->zcpy);
+  cudaFree(p->partial);
+  p->tiles = p->x = p->y = p->z = p->zcpy = p->partial = nullptr;
+  p->bytes = (long long)(sizeof(MaternParams) + kKtabDoubles * sizeof(double) + 2 * sizeof(int) + 4 * sizeof(double));
+  const int ts = ((std::max(p->dts, 256) + 255) / 256) * 256;
+  p->ts = ts;
+  p->nt = (p->n + ts - 1) / ts;
+  p->np = p->nt * ts;
+  p->ntiles = 0;
+  p->mband = b;
+  const int nt = p->nt;
+  const int m = std::max(0, nt - b - 1);
+  const size_t ts2 = (size_t)ts * ts;
+  int rc = EGS_OK;
+  if ((rc = dev_alloc(&p->x, p->np, &p->bytes)) || (rc = dev_alloc(&p->y, p->np, &p->bytes)) ||
+      (rc = dev_alloc(&p->z, p->np, &p->bytes)) || (rc = dev_alloc(&p->zcpy, p->np, &p->bytes)) ||
+      (rc = dev_alloc(&p->partial, p->nt, &p->bytes)) ||
+      (rc = dev_alloc(&p->band_pool, (size_t)nt * (b + 1) * ts2, &p->bytes)) ||
+      (rc = dev_alloc(&p->off_pool, std::max<size_t>(1, (size_t)lower_tiles(m) * ts2), &p->bytes)) ||
+      (rc = dev_alloc(&p->W, (size_t)nt * ts2, &p->bytes)) || (rc = dev_alloc(&p->ph, (size_t)p->np * ts, &p->bytes)) ||
+      (rc = dev_alloc(&p->pl, (size_t)p->np * ts, &p->bytes)) ||
+      (rc = dev_alloc(&p->inv_scale, (size_t)p->np, &p->bytes)) || (rc = dev_alloc(&p->w, p->np, &p->bytes)) ||
+      (rc = dev_alloc(&p->res_scratch, (size_t)residual_scratch_doubles(p->n), &p->bytes)))
+    return rc;
+  std::vector<int4> gen;
+  for (int j = 0; j < nt; ++j)
+    for (int i = j; i < nt; ++i)
+      gen.push_back(i - j <= b ? make_int4(i, j, 0, (int)((long long)j * (b + 1) + (i - j)))
+                               : make_int4(i, j, 1, (int)tile_slot(i - b - 1, j, m)));
+  p->ngen = (long long)gen.size();
+  if ((rc = dev_alloc(&p->gen_tiles, gen.size(), &p->bytes))) return rc;
+  EGS_CUDA_TRY(cudaMemcpy(p->gen_tiles, gen.data(), gen.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  // FP64 band update of step k: one job per target tile column j > k, rows of
+  // tiles j .. min(nt-1, j+b), all operands W-relative (W[t] = tile (k+t, k)).
+  std::vector<GemmDesc> jobs;
+  std::vector<long long> begin;
+  p->band_launch.clear();
+  for (int k = 0; k < nt; ++k) {
+    egs_problem::JobLaunch L{(long long)jobs.size(), (long long)begin.size(), 0, 0};
+    long long acc = 0;
+    for (int j = k + 1; j < nt; ++j) {
+      const int t = j - k;
+      GemmDesc d{};
+      d.M = (std::min(nt - 1, j + b) - j + 1) * ts;
+      d.N = ts;
+      d.K = ts;
+      d.a_row0 = d.b_row0 = d.c_row0 = d.c_col0 = t * ts;
+      d.lower = 1;
+      d.ts = ts;
+      d.nt = nt - k;
+      d.np = (nt - k) * ts;
+      d.c_mode = 1;
+      d.c_band = b;
+      d.c_tile_off = k;
+      finish_desc(d);
+      jobs.push_back(d);
+      begin.push_back(acc);
+      acc += d.total;
+      ++L.njobs;
+    }
+    begin.push_back(acc);
+    L.total = acc;
+    p->band_launch.push_back(L);
+  }
+  if ((rc = dev_alloc(&p->band_jobs, std::max<size_t>(1, jobs.size()), &p->bytes)) ||
+      (rc = dev_alloc(&p->band_begin, std::max<size_t>(1, begin.size()), &p->bytes)))
+    return rc;
+  if (!jobs.empty())
+    EGS_CUDA_TRY(cudaMemcpy(p->band_jobs, jobs.data(), jobs.size() * sizeof(GemmDesc), cudaMemcpyHostToDevice));
+  EGS_CUDA_TRY(cudaMemcpy(p->band_begin, begin.data(), begin.size() * sizeof(long long), cudaMemcpyHostToDevice));
+  if ((rc = gemm_init_tensor_map(p->tmapW, p->W, ts, nt)) != EGS_OK ||
+      (rc = split_tensor_map(p->tm_hi, p->ph, ts, p->np)) != EGS_OK ||
+      (rc = split_tensor_map(p->tm_lo, p->pl, ts, p->np)) != EGS_OK)
+    return rc;
+  EGS_CUDA_TRY(cudaMemset(p->x, 0, p->np * sizeof(double)));
+  EGS_CUDA_TRY(cudaMemset(p->y, 0, p->np * sizeof(double)));
+  EGS_CUDA_TRY(cudaMemset(p->z, 0, p->np * sizeof(double)));
+  EGS_CUDA_TRY(cudaMemset(p->zcpy, 0, p->np * sizeof(double)));
+  EGS_CUDA_TRY(cudaMemset(p->w, 0, p->np * sizeof(double)));
+  EGS_CUDA_TRY(cudaMemset(p->inv_scale, 0, p->np * sizeof(float)));
+  EGS_CUDA_TRY(cudaMemset(p->ph, 0, (size_t)p->np * ts * sizeof(__half)));
+  EGS_CUDA_TRY(cudaMemset(p->pl, 0, (size_t)p->np * ts * sizeof(__half)));
+  p->precision = EGS_PRECISION_MIXED;
+  return EGS_OK;
+}
+
+int reject_mixed(const egs_problem* p, const char* where) {
+  if (p->precision == EGS_PRECISION_DOUBLE) return EGS_OK;
+  if (p->precision == kPrecisionBroken) {
+    set_last_error("the problem's mixed-precision layout could not be built", where);
+    return EGS_ERR_STATE;
+  }
+  set_last_error("not available for a mixed-precision problem (use egs_mle_eval)", where);
+  return EGS_ERR_STATE;
 }
 
 // Capture the parameter upload and enqueue_eval into a graph.  Capture problems
@@ -519,6 +770,7 @@ int egs_problem_info(const egs_problem* p, int* n, int* ts, int* nt, long long* 
 
 int egs_problem_set_band(egs_problem* p, int band) {
   if (!p || band < 0) return EGS_ERR_INVALID;
+  if (int rc = reject_mixed(p, "egs_problem_set_band")) return rc;
   if (band > 0 && p->dts != p->ts) {
     // The approximation is defined on the caller's tiles; merging them into a
     // larger device tile would change the result.
@@ -527,6 +779,37 @@ int egs_problem_set_band(egs_problem* p, int band) {
   }
   p->band = band;
   return EGS_OK;
+}
+
+int egs_problem_set_precision(egs_problem* p, int precision, int band_tiles) {
+  if (!p || band_tiles < 0) return EGS_ERR_INVALID;
+  if (precision != EGS_PRECISION_DOUBLE && precision != EGS_PRECISION_MIXED) return EGS_ERR_INVALID;
+  if (precision == p->precision && (precision == EGS_PRECISION_DOUBLE || band_tiles == p->mband)) return EGS_OK;
+  if (p->have_locations || p->have_observations) {
+    set_last_error("set the precision before locations and observations", "egs_problem_set_precision");
+    return EGS_ERR_STATE;
+  }
+  if (precision == EGS_PRECISION_DOUBLE) {
+    set_last_error("a mixed-precision problem cannot return to FP64; create a new problem",
+                   "egs_problem_set_precision");
+    return EGS_ERR_STATE;
+  }
+  if (p->band > 0) {
+    set_last_error("the band approximation and mixed precision are exclusive", "egs_problem_set_precision");
+    return EGS_ERR_STATE;
+  }
+  EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  if (p->graph_exec) cudaGraphExecDestroy(p->graph_exec);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  p->graph_exec = nullptr;
+  p->graph = nullptr;
+  const int rc = setup_mixed(p, band_tiles);
+  if (rc != EGS_OK) {
+    // leave a problem that reports the failure instead of a half-built layout
+    free_mixed(p);
+    p->precision = kPrecisionBroken;
+  }
+  return rc;
 }
 
 int egs_problem_set_stream(egs_problem* p, void* cuda_stream) {
@@ -545,6 +828,7 @@ int egs_problem_set_stream(egs_problem* p, void* cuda_stream) {
 
 static int set_locs(egs_problem* p, const double* x, const double* y, cudaMemcpyKind kind) {
   if (!p || !x || !y) return EGS_ERR_INVALID;
+  if (p->precision == kPrecisionBroken) return EGS_ERR_STATE;
   EGS_CUDA_TRY(cudaMemcpyAsync(p->x, x, p->n * sizeof(double), kind, p->stream));
   EGS_CUDA_TRY(cudaMemcpyAsync(p->y, y, p->n * sizeof(double), kind, p->stream));
   EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
@@ -561,6 +845,7 @@ int egs_problem_set_locations_device(egs_problem* p, const double* x, const doub
 
 static int set_obs(egs_problem* p, const double* z, cudaMemcpyKind kind) {
   if (!p || !z) return EGS_ERR_INVALID;
+  if (p->precision == kPrecisionBroken) return EGS_ERR_STATE;
   EGS_CUDA_TRY(cudaMemcpyAsync(p->zcpy, z, p->n * sizeof(double), kind, p->stream));
   EGS_CUDA_TRY(cudaMemcpyAsync(p->z, p->zcpy, p->np * sizeof(double), cudaMemcpyDeviceToDevice, p->stream));
   EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
@@ -575,6 +860,7 @@ int egs_problem_set_observations_device(egs_problem* p, const double* z) {
 
 int egs_covariance_generate(egs_problem* p, const double* theta) {
   if (!p) return EGS_ERR_INVALID;
+  if (int rc = reject_mixed(p, "egs_covariance_generate")) return rc;
   if (!p->have_locations) return EGS_ERR_STATE;
   int rc = set_params(p, theta);
   if (rc != EGS_OK) return rc;
@@ -586,6 +872,7 @@ int egs_covariance_generate(egs_problem* p, const double* theta) {
 
 int egs_potrf(egs_problem* p) {
   if (!p) return EGS_ERR_INVALID;
+  if (int rc = reject_mixed(p, "egs_potrf")) return rc;
   EGS_CUDA_TRY(cudaMemsetAsync(p->flags, 0, 2 * sizeof(int), p->stream));
   int rc = p->band > 0 ? enqueue_potrf_band(p) : enqueue_potrf(p);
   if (rc != EGS_OK) return rc;
@@ -602,6 +889,7 @@ int egs_restore_observations(egs_problem* p) {
 
 int egs_trsv(egs_problem* p) {
   if (!p) return EGS_ERR_INVALID;
+  if (int rc = reject_mixed(p, "egs_trsv")) return rc;
   enqueue_trsv(p);
   int rc = check_cuda("egs_trsv");
   if (rc != EGS_OK) return rc;
@@ -611,6 +899,7 @@ int egs_trsv(egs_problem* p) {
 
 int egs_loglik_parts(egs_problem* p, double* loglik, double* logdet, double* dot) {
   if (!p) return EGS_ERR_INVALID;
+  if (int rc = reject_mixed(p, "egs_loglik_parts")) return rc;
   launch_logdet_partials(p->tiles, p->ts, p->nt, p->n, p->partial, p->stream);
   launch_finalize(p->partial, p->nt, p->z, p->n, p->result, nullptr, p->stream);
   int rc = check_cuda("egs_loglik_parts");
@@ -625,6 +914,7 @@ int egs_loglik_parts(egs_problem* p, double* loglik, double* logdet, double* dot
 
 int egs_get_tile(egs_problem* p, int i, int j, double* host_out) {
   if (!p || !host_out || i < j || i >= p->nt || j < 0) return EGS_ERR_INVALID;
+  if (int rc = reject_mixed(p, "egs_get_tile")) return rc;
   const size_t ts2 = (size_t)p->ts * p->ts;
   EGS_CUDA_TRY(cudaMemcpyAsync(host_out, p->tiles + tile_slot(i, j, p->nt) * ts2, ts2 * sizeof(double),
                                cudaMemcpyDeviceToHost, p->stream));
@@ -688,6 +978,7 @@ int egs_problem_set_graphs(egs_problem* p, int enable) {
 
 int egs_generate_observations(egs_problem* p, const double* theta, int seed, double* z_out) {
   if (!p || !theta || seed < 0 || seed > 4095) return EGS_ERR_INVALID;
+  if (int rc = reject_mixed(p, "egs_generate_observations")) return rc;
   if (!p->have_locations) return EGS_ERR_STATE;
   if (lower_tiles(p->nt) > 65535) return EGS_ERR_INVALID;
   std::vector<double> e(p->np, 0.0);

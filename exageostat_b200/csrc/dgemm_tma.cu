@@ -327,10 +327,10 @@ dgemm_update_kernel(const __grid_constant__ CUtensorMap tmap, double* __restrict
           const int ml = mb * BM + wm * 64 + mi * 16 + row_in_box;
           const int gi = d.c_row0 + ml;
           const int ti = gi / ts, lr = gi - ti * ts;
-          const bool ok_el = nl < d.N && ml < d.M && ti >= tj;
-          ptr[h][mi] = ok_el ? tiles + (d.tile_base + tile_slot(ti, tj, d.nt)) * (long long)ts * ts +
-                                   (long long)lc * ts + lr
-                             : nullptr;
+          const bool ok_el = nl < d.N && ml < d.M && ti >= tj && (d.c_mode == 0 || ti - tj <= d.c_band);
+          const long long cslot = d.c_mode == 0 ? d.tile_base + tile_slot(ti, tj, d.nt)
+                                                : (long long)(d.c_tile_off + tj) * (d.c_band + 1) + (ti - tj);
+          ptr[h][mi] = ok_el ? tiles + cslot * (long long)ts * ts + (long long)lc * ts + lr : nullptr;
           if (ok_el) ldg_v2f64(ptr[h][mi], cv[h][mi][0], cv[h][mi][1]);
         }
       }

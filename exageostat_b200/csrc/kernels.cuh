@@ -1,6 +1,7 @@
 // Launch helpers shared by the translation units of the B200 path.
 #pragma once
 #include <cuda_runtime.h>
+#include <cuda_fp16.h>
 #include "common.cuh"
 #include "bessel_k.cuh"
 
@@ -48,6 +49,10 @@ struct GemmDesc {
   long long total;
   int ts, nt, np;
   long long tile_base;  // slot of this problem's tile (0, 0) in a pool of problems
+  // C addressing: c_mode 0 = lower-tile pool (tile_base + tile_slot(ti, tj, nt));
+  // c_mode 1 = FP64 band pool of a mixed-precision problem: only tiles with
+  // ti - tj <= c_band are written, at slot (c_tile_off + tj) * (c_band + 1) + (ti - tj).
+  int c_mode, c_band, c_tile_off;
 };
 
 // Batched launches: blocks [begin[j], begin[j+1]) belong to job j.
@@ -69,5 +74,29 @@ int launch_gemm_rows(const void* tmap, double* tiles, int ts, int nt, int M, int
                      int a_col0, int a_tcol, int b_row0, int b_col0, int b_tcol, int c_row0, int c_col0,
                      int lower, int* err, cudaStream_t st);
 int gemm_num_sms();
+
+// Mixed-precision evaluation (mixed.cu, split_gemm.cu).
+void launch_matern_mixed(double* band, float* off, const double* x, const double* y, int n, int ts,
+                         const int4* tinfo, long long ntiles, const MaternParams* params, double* ktab,
+                         cudaStream_t st);
+void launch_gather_column(const double* band, const float* off, double* W, int ts, int nt, int b, int k,
+                          cudaStream_t st);
+void launch_scatter_column(const double* W, double* band, float* off, int ts, int nt, int b, int k,
+                           cudaStream_t st);
+void launch_logdet_band(const double* band, int ts, int nt, int b, int n, double* partial, cudaStream_t st);
+void launch_mixed_solve(const double* band, const float* off, int ts, int nt, int b, double* v, cudaStream_t st,
+                        long long* launches);
+long long residual_scratch_doubles(int n);
+void launch_matern_residual(const double* x, const double* y, const double* z, const double* v, int n, int np,
+                            const MaternParams* params, const double* ktab, double* scratch, double* r,
+                            cudaStream_t st);
+void launch_finalize_mixed(const double* partial, int nt, const double* z, const double* v, const double* w, int n,
+                           double* result, const int* info, cudaStream_t st);
+int split_tensor_map(void* storage, const __half* base, int ts, long long rows);
+void launch_panel_split(const double* W, int ts, int t0, int ntiles, int row_tile0, float* inv_scale, __half* Ph,
+                        __half* Pl, cudaStream_t st);
+long long split_targets(int nt, int band, int k);
+int launch_split_update(const void* tm_hi, const void* tm_lo, int ts, int nt, int band, int k, float* c_pool,
+                        const float* inv_scale, int* err, cudaStream_t st);
 
 }  // namespace egs

@@ -21,10 +21,12 @@ __device__ __forceinline__ void stage_ktab(double* __restrict__ stab, const doub
 
 // Pairs [pair0, pair0 + kGenPairsPerBlock) of tile (ti, tj), column-major with
 // ld ts: thread t writes rows (r, r+1) of column c for pair = pair0 + i*256 + t,
-// e = 2*pair = c*ts + r, with one 16-byte store (a warp stores 512 contiguous
-// bytes).  Rows/columns past n are padding: identity on the diagonal, 0
-// elsewhere.  x and y hold the problem's padded locations (nt*ts entries).
-__device__ __forceinline__ void matern_tile_pairs(double* __restrict__ tile, const double* __restrict__ x,
+// e = 2*pair = c*ts + r, with one vector store (FP64 tiles: a warp stores 512
+// contiguous bytes; FP32 tiles, rounded from the FP64 value: 256 bytes).
+// Rows/columns past n are padding: identity on the diagonal, 0 elsewhere.  x and
+// y hold the problem's padded locations (nt*ts entries).
+template <typename Out>
+__device__ __forceinline__ void matern_tile_pairs(Out* __restrict__ tile, const double* __restrict__ x,
                                                   const double* __restrict__ y, int n, int ts, int ti, int tj,
                                                   long long pair0, const MaternParams& p,
                                                   const double* __restrict__ tab) {
@@ -49,7 +51,11 @@ __device__ __forceinline__ void matern_tile_pairs(double* __restrict__ tile, con
       v0 = (gr < n) ? matern_from_dist_tab(euclid_dist(xr.x, yr.x, xc, yc), p, tab) : 0.0;
       v1 = (gr + 1 < n) ? matern_from_dist_tab(euclid_dist(xr.y, yr.y, xc, yc), p, tab) : 0.0;
     }
-    *reinterpret_cast<double2*>(tile + e) = make_double2(v0, v1);
+    if constexpr (sizeof(Out) == 8) {
+      *reinterpret_cast<double2*>(tile + e) = make_double2(v0, v1);
+    } else {
+      *reinterpret_cast<float2*>(tile + e) = make_float2((float)v0, (float)v1);
+    }
   }
 }
 

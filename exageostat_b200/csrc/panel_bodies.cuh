@@ -151,8 +151,10 @@ __device__ __forceinline__ void trsv_diag_body(const double* __restrict__ T, int
 }
 
 // zi -= T zk for the 64 rows of block rblk of tile T (256 threads = 64 rows x
-// 4 column groups, fixed reduction order).  Dynamic shared memory: ts doubles.
-__device__ __forceinline__ void gemv_panel_body(const double* __restrict__ T, int ts, const double* __restrict__ zk,
+// 4 column groups, fixed reduction order, FP64 arithmetic whatever the tile's
+// storage type).  Dynamic shared memory: ts doubles.
+template <typename Tile>
+__device__ __forceinline__ void gemv_panel_body(const Tile* __restrict__ T, int ts, const double* __restrict__ zk,
                                                 double* __restrict__ zi, int rblk) {
   extern __shared__ double zks[];  // ts
   __shared__ double red[4][kNB];
@@ -162,7 +164,7 @@ __device__ __forceinline__ void gemv_panel_body(const double* __restrict__ T, in
   const int r = rblk * kNB + rl;
   double acc = 0.0;
   if (r < ts) {
-    for (int c = g; c < ts; c += 4) acc = fma(T[(long long)c * ts + r], zks[c], acc);
+    for (int c = g; c < ts; c += 4) acc = fma((double)T[(long long)c * ts + r], zks[c], acc);
   }
   red[g][rl] = acc;
   __syncthreads();

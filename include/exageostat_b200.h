@@ -72,6 +72,25 @@ EGS_API int egs_problem_set_stream(egs_problem* p, void* cuda_stream);
  * tile); other sizes return EGS_ERR_INVALID. */
 EGS_API int egs_problem_set_band(egs_problem* p, int band);
 
+/* Precision of the factorisation, the reference's Precision enum
+ * (inst/include/common/Definitions.hpp:258-262, Configurations --precision). */
+#define EGS_PRECISION_DOUBLE 1
+#define EGS_PRECISION_MIXED 2
+
+/* Select the precision before locations and observations are set.
+ * EGS_PRECISION_DOUBLE (default) is the exact FP64 path.  EGS_PRECISION_MIXED
+ * keeps the diagonal tiles and band_tiles tile rows below them in FP64 and
+ * stores every other tile in FP32: the diagonal potrf, the panel solves, the
+ * band updates, the log-determinant and the dot product run in FP64; off-band
+ * updates run on FP16 tensor cores from a per-row scaled two-part split of the
+ * panel (FP32-level accuracy), and the quadratic form gets one iterative
+ * refinement step against the FP64 covariance.  The device tile becomes dts
+ * rounded up to a multiple of 256.  Only egs_mle_eval (and the info, stream,
+ * profiling and observation calls) is available on a mixed problem; a mixed
+ * problem cannot return to FP64.  The reference declares the option but its
+ * dense path has no mixed implementation. */
+EGS_API int egs_problem_set_precision(egs_problem* p, int precision, int band_tiles);
+
 /* Copy n locations from host memory (Locations<T> SoA x[], y[],
  * src/data-units/Locations.cpp:94-118). */
 EGS_API int egs_problem_set_locations(egs_problem* p, const double* x, const double* y);

