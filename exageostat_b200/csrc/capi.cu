@@ -101,6 +101,8 @@ struct egs_problem {
   alignas(64) unsigned char tmapW[128];
   alignas(64) unsigned char tm_hi[128];
   alignas(64) unsigned char tm_lo[128];
+  alignas(64) unsigned char tm_c[128];
+  alignas(64) unsigned char tm_cr[128];
 };
 
 namespace {
@@ -497,7 +499,8 @@ int enqueue_eval_mixed(egs_problem* p) {
         count_launches(p, EGS_STAGE_UPDATE, 1);
       }
       if (split_targets(nt, b, k) > 0) {
-        int rc = launch_split_update(p->tm_hi, p->tm_lo, ts, nt, b, k, p->off_pool, p->inv_scale, err, st);
+        int rc = launch_split_update(p->tm_hi, p->tm_lo, p->tm_c, p->tm_cr, ts, nt, b, k, p->off_pool, p->inv_scale,
+                                     err, st);
         if (rc != EGS_OK) return rc;
         count_launches(p, EGS_STAGE_UPDATE, 1);
       }
@@ -607,7 +610,8 @@ int setup_mixed(egs_problem* p, int b) {
   EGS_CUDA_TRY(cudaMemcpy(p->band_begin, begin.data(), begin.size() * sizeof(long long), cudaMemcpyHostToDevice));
   if ((rc = gemm_init_tensor_map(p->tmapW, p->W, ts, nt)) != EGS_OK ||
       (rc = split_tensor_map(p->tm_hi, p->ph, ts, p->np)) != EGS_OK ||
-      (rc = split_tensor_map(p->tm_lo, p->pl, ts, p->np)) != EGS_OK)
+      (rc = split_tensor_map(p->tm_lo, p->pl, ts, p->np)) != EGS_OK ||
+      (rc = split_c_maps(p->tm_c, p->tm_cr, p->off_pool, ts, lower_tiles(m))) != EGS_OK)
     return rc;
   EGS_CUDA_TRY(cudaMemset(p->x, 0, p->np * sizeof(double)));
   EGS_CUDA_TRY(cudaMemset(p->y, 0, p->np * sizeof(double)));

@@ -93,10 +93,12 @@ void launch_matern_residual(const double* x, const double* y, const double* z, c
 void launch_finalize_mixed(const double* partial, int nt, const double* z, const double* v, const double* w, int n,
                            double* result, const int* info, cudaStream_t st);
 int split_tensor_map(void* storage, const __half* base, int ts, long long rows);
+int split_c_maps(void* tm_c, void* tm_cr, const float* c_pool, int ts, long long nslots);
 void launch_panel_split(const double* W, int ts, int t0, int ntiles, int row_tile0, float* inv_scale, __half* Ph,
                         __half* Pl, cudaStream_t st);
 long long split_targets(int nt, int band, int k);
-int launch_split_update(const void* tm_hi, const void* tm_lo, int ts, int nt, int band, int k, float* c_pool,
+int launch_split_update(const void* tm_hi, const void* tm_lo, const void* tm_c, const void* tm_cr, int ts, int nt,
+                        int band, int k, float* c_pool,
                         const float* inv_scale, int* err, cudaStream_t st);
 
 }  // namespace egs

@@ -15,22 +15,37 @@
 // runs on the FP16 tensor path (kind::f16).  Per-row scaling keeps the FP16
 // parts in range whatever the magnitude of the factor's rows.
 //
+// Promotion.  The tensor core's FP32 accumulation does not round to nearest:
+// sums of same-sign products come out systematically short (about 8e-6
+// relative after K = 1024, i.e. ~1 ulp per instruction).  The Cholesky
+// updates of a positively correlated covariance are such sums, and the bias
+// reaches the log-determinant at first order.  So each 64-wide K stage is
+// accumulated from zero in tensor memory -- the two small correction products
+// first, the main hi*hi product last, so at most four instructions add into a
+// full-size accumulator -- and the epilogue adds the stage's partial sum into
+// FP32 registers with round-to-nearest.  The bias drops to that of four
+// instructions (~2e-7 relative), the same order as plain FP32 rounding.
+//
 // Kernel structure (one CTA per SM, persistent over 128 x 256 output tiles):
 //   warp 0    TMA producer: per 64-wide K stage, the A rows (hi, lo) and B rows
-//             (hi, lo) of the tile, 128B-swizzled, into a 2-stage ring;
-//   warp 1    allocates 512 TMEM columns (two 128 x 256 FP32 accumulators) and
-//             issues the tcgen05.mma instructions from one thread; commits
-//             release the ring stage and, after the last stage, hand the
+//             (hi, lo) of the tile, 128B-swizzled, into a 2-stage ring; a few
+//             stages before a tile ends it prefetches the tile's C block to L2;
+//   warp 1    allocates 512 TMEM columns (two 128 x 256 FP32 stage
+//             accumulators) and issues the tcgen05.mma instructions from one
+//             thread; commits release the ring stage and hand the stage
 //             accumulator to the epilogue;
-//   warps 2-5 epilogue: tcgen05.ld of the accumulator (thread = tile row),
+//   warps 2-9 epilogue: warp w reads TMEM lanes 32 (w % 4) .. +32 (thread =
+//             tile row) and one half of the columns, adds every stage into 128
+//             FP32 registers, and after the last stage applies
 //             C -= acc * inv_s_row * inv_s_col, coalesced along each column.
-// The two accumulators let the MMAs of tile t+1 overlap the epilogue of tile t.
-// Every mbarrier wait is bounded; a timed-out CTA records the error, stops, and
-// still frees its tensor memory.
+// The two stage accumulators let the MMAs of stage s+1 overlap the draining of
+// stage s.  Every mbarrier wait is bounded; a timed-out CTA records the error,
+// stops, and still frees its tensor memory.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_fp16.h>
 #include <cstdint>
+#include <cstring>
 #include "common.cuh"
 #include "kernels.cuh"
 #include "mbarrier.cuh"
@@ -43,8 +58,17 @@ constexpr int BOX_ROWS = 128;                      // TMA box: 64 fp16 (128 B) x
 constexpr int A_BYTES = BM * BK * 2;               // 16 KB
 constexpr int B_BYTES = BN * BK * 2;               // 32 KB
 constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
-constexpr int THREADS = 192;
-constexpr int SMEM_BYTES = 1024 + STAGES * STAGE_BYTES + 256;
+constexpr int EPI_WARPS = 8;                       // two per TMEM lane quarter
+constexpr int THREADS = 64 + 32 * EPI_WARPS;       // producer, MMA issuer, epilogue
+constexpr int HALF_COLS = BN / 2;                  // accumulator columns per epilogue thread
+constexpr int PF_AHEAD = 6;                        // stages before a tile's end at which C is prefetched
+// Epilogue staging for the TMA reduce-add of C: per epilogue warp two buffers of
+// 32 rows x RED_COLS columns (column-major, one 128-byte row segment per column).
+constexpr int RED_COLS = 16;
+constexpr int RED_BYTES = 32 * RED_COLS * 4;       // 2 KB
+constexpr int STAGING_BYTES = EPI_WARPS * 2 * RED_BYTES;
+constexpr int SMEM_BYTES = 1024 + STAGES * STAGE_BYTES + STAGING_BYTES + 256;
+static_assert(SMEM_BYTES <= 232448, "shared memory per CTA");
 constexpr uint32_t TMEM_COLS = 512;
 // Instruction descriptor of kind::f16: D F32 (bits 4-5 = 1), A and B F16 (0),
 // both K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28.
@@ -149,6 +173,19 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
       "l"((uint64_t)map), "r"(x), "r"(y), "r"(smem_u32(bar))
       : "memory");
 }
+// out[box at (x, y)] += smem (FP32 add performed at L2), tracked in this thread's bulk group.
+__device__ __forceinline__ void tma_reduce_add_2d(const CUtensorMap* map, const void* src, int x, int y) {
+  asm volatile("cp.reduce.async.bulk.tensor.2d.global.shared::cta.add.bulk_group [%0, {%2, %3}], [%1];" ::"l"(
+                   (uint64_t)map),
+               "r"(smem_u32(src)), "r"(x), "r"(y)
+               : "memory");
+}
+// L2 prefetch of one box of a tiled tensor (no shared memory, no completion).
+__device__ __forceinline__ void tma_prefetch_l2_2d(const CUtensorMap* map, int x, int y) {
+  asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];" ::"l"((uint64_t)map), "r"(x),
+               "r"(y)
+               : "memory");
+}
 // 32 consecutive FP32 columns of this warp's 32 TMEM lanes.
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
   uint32_t r[32];
@@ -163,6 +200,20 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// 16 consecutive FP32 columns of this warp's 32 TMEM lanes.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
 // Target tile of work item L at step k: targets are enumerated column by column
@@ -195,11 +246,13 @@ __device__ __forceinline__ void decode_item(const SplitStep& P, long long L, int
 
 __global__ void __launch_bounds__(sg::THREADS, 1)
 split_gemm_kernel(const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo,
+                  const __grid_constant__ CUtensorMap tm_c, const __grid_constant__ CUtensorMap tm_cr,
                   const __grid_constant__ SplitStep P) {
   using namespace sg;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
+  float* staging = reinterpret_cast<float*>(smem + STAGES * STAGE_BYTES);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES + STAGING_BYTES);
   uint64_t* empty = full + STAGES;
   uint64_t* acc_full = empty + STAGES;
   uint64_t* acc_empty = acc_full + 2;
@@ -215,7 +268,7 @@ split_gemm_kernel(const __grid_constant__ CUtensorMap tm_hi, const __grid_consta
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&acc_full[b], 1);
-      mbar_init(&acc_empty[b], 4);
+      mbar_init(&acc_empty[b], EPI_WARPS);
     }
     bail = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -231,10 +284,12 @@ split_gemm_kernel(const __grid_constant__ CUtensorMap tm_hi, const __grid_consta
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
   const int ksteps = P.ts / BK;
+  const int pf_kt = ksteps > PF_AHEAD ? ksteps - PF_AHEAD : 0;
 
   if (warp == 0) {
     if (lane == 0) {
       uint32_t it = 0;
+      const int mm = P.nt - P.band - 1;
       for (long long L = blockIdx.x; L < P.total && !bail; L += gridDim.x) {
         int i, j, mb, nb;
         decode_item(P, L, i, j, mb, nb);
@@ -254,6 +309,11 @@ split_gemm_kernel(const __grid_constant__ CUtensorMap tm_hi, const __grid_consta
           tma_load_2d(st + 2 * A_BYTES + BOX_ROWS * 128, &tm_hi, &full[s], x, brow + BOX_ROWS);
           tma_load_2d(st + 2 * A_BYTES + B_BYTES, &tm_lo, &full[s], x, brow);
           tma_load_2d(st + 2 * A_BYTES + B_BYTES + BOX_ROWS * 128, &tm_lo, &full[s], x, brow + BOX_ROWS);
+          if (kt == pf_kt) {
+            // the tile's C block (BM rows x BN columns of an FP32 tile) into L2
+            const long long slot = tile_slot(i - P.band - 1, j, mm);
+            tma_prefetch_l2_2d(&tm_c, mb * BM, (int)(slot * P.ts + nb * BN));
+          }
         }
       }
       // drain: the stages issued last must land before the CTA may exit
@@ -262,89 +322,110 @@ split_gemm_kernel(const __grid_constant__ CUtensorMap tm_hi, const __grid_consta
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      uint32_t it = 0, tcount = 0;
-      for (long long L = blockIdx.x; L < P.total && !bail; L += gridDim.x, ++tcount) {
-        const uint32_t ab = tcount & 1;
-        if (tcount >= 2 && !mbar_wait(&acc_empty[ab], ((tcount >> 1) & 1) ^ 1, P.err)) {
-          bail = 1;
-          break;
-        }
-        tc_fence_after();
-        const uint32_t dcol = tmem_base + ab * BN;
-        bool ok = true;
+      uint32_t it = 0;
+      bool ok = true;
+      for (long long L = blockIdx.x; L < P.total && ok && !bail; L += gridDim.x) {
         for (int kt = 0; kt < ksteps; ++kt, ++it) {
-          const uint32_t s = it % STAGES;
+          // stage it accumulates into buffer it & 1 from zero
+          const uint32_t ab = it & 1, s = it % STAGES;
+          if (it >= 2 && !mbar_wait(&acc_empty[ab], ((it >> 1) & 1) ^ 1, P.err)) {
+            ok = false;
+            break;
+          }
           if (!mbar_wait(&full[s], (it / STAGES) & 1, P.err)) {
             ok = false;
             break;
           }
           tc_fence_after();
+          const uint32_t dcol = tmem_base + ab * BN;
           const uint32_t sa = smem_u32(smem + s * STAGE_BYTES);
           const uint32_t sal = sa + A_BYTES, sbh = sa + 2 * A_BYTES, sbl = sbh + B_BYTES;
+          // corrections first (small partial sums), the main product last
 #pragma unroll
           for (int kk = 0; kk < BK / 16; ++kk) {
             const uint32_t off = kk * 32;
-            const uint32_t acc = (kt > 0 || kk > 0) ? 1u : 0u;
-            umma_f16(dcol, sdesc_sw128(sa + off), sdesc_sw128(sbh + off), acc);
-            umma_f16(dcol, sdesc_sw128(sa + off), sdesc_sw128(sbl + off), 1u);
+            umma_f16(dcol, sdesc_sw128(sa + off), sdesc_sw128(sbl + off), kk > 0 ? 1u : 0u);
             umma_f16(dcol, sdesc_sw128(sal + off), sdesc_sw128(sbh + off), 1u);
           }
+#pragma unroll
+          for (int kk = 0; kk < BK / 16; ++kk) {
+            const uint32_t off = kk * 32;
+            umma_f16(dcol, sdesc_sw128(sa + off), sdesc_sw128(sbh + off), 1u);
+          }
           umma_commit(&empty[s]);
+          umma_commit(&acc_full[ab]);
         }
-        if (!ok) {
-          bail = 1;
-          break;
-        }
-        umma_commit(&acc_full[ab]);
       }
+      if (!ok) bail = 1;
     }
   } else {
-    // epilogue warps 2..5: TMEM lane quarter = warp % 4
-    const int quarter = warp & 3;
-    const int row = quarter * 32 + lane;
-    uint32_t tcount = 0;
-    for (long long L = blockIdx.x; L < P.total; L += gridDim.x, ++tcount) {
-      const uint32_t ab = tcount & 1;
-      // one lane waits, the warp follows it uniformly (tcgen05.ld needs the whole warp)
-      int ok = 1;
-      if (lane == 0) ok = mbar_wait(&acc_full[ab], (tcount >> 1) & 1, P.err) ? 1 : 0;
-      ok = __shfl_sync(0xffffffffu, ok, 0);
-      if (!ok) {
-        bail = 1;
-        break;
+    // epilogue warps 2..9: TMEM lane quarter = warp % 4, column half by warp group
+    const int quarter = warp & 3, half = (warp - 2) >> 2;
+    const uint32_t tl = tmem_base + ((uint32_t)(quarter * 32) << 16) + half * HALF_COLS;
+    uint32_t it = 0, red_count = 0;
+    bool ok = true;
+    for (long long L = blockIdx.x; L < P.total && ok; L += gridDim.x) {
+      float acc[HALF_COLS];  // zero plus the first stage is that stage's value
+#pragma unroll
+      for (int c = 0; c < HALF_COLS; ++c) acc[c] = 0.f;
+      for (int kt = 0; kt < ksteps; ++kt, ++it) {
+        const uint32_t ab = it & 1;
+        // one lane waits, the warp follows it uniformly (tcgen05.ld needs the whole warp)
+        int w = 1;
+        if (lane == 0) w = mbar_wait(&acc_full[ab], (it >> 1) & 1, P.err) ? 1 : 0;
+        w = __shfl_sync(0xffffffffu, w, 0);
+        if (!w) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+#pragma unroll
+        for (int g = 0; g < HALF_COLS / 16; ++g) {
+          float v[16];
+          tmem_ld16(tl + ab * BN + g * 16, v);
+#pragma unroll
+          for (int c = 0; c < 16; ++c) acc[g * 16 + c] += v[c];
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&acc_empty[ab]);
       }
-      tc_fence_after();
+      if (!ok) break;
+      // C -= acc * inv_r * inv_c: the scaled update goes through this warp's
+      // staging buffers to TMA reduce-adds of 32 rows x RED_COLS columns, so the
+      // epilogue never waits for C to be read.
       int i, j, mb, nb;
       decode_item(P, L, i, j, mb, nb);
       const int mm = P.nt - P.band - 1;
-      float* C = P.c_pool + tile_slot(i - P.band - 1, j, mm) * (long long)P.ts * P.ts;
-      const int r = mb * BM + row;
-      const float inv_r = P.inv_scale[(long long)i * P.ts + r];
-      const float* inv_c = P.inv_scale + (long long)j * P.ts + nb * BN;
-      float* cp = C + (long long)(nb * BN) * P.ts + r;
-      const long long ld = P.ts;
-      // 32 columns per chunk; the C loads of the next chunk are issued before the
-      // current chunk is finished, so about 64 independent loads are in flight.
-      float cv[32], cn[32];
+      const long long slot = tile_slot(i - P.band - 1, j, mm);
+      const int r0 = mb * BM + quarter * 32;
+      const int c0 = nb * BN + half * HALF_COLS;
+      const float inv_r = P.inv_scale[(long long)i * P.ts + r0 + lane];
+      const float* inv_c = P.inv_scale + (long long)j * P.ts + c0;
+      float* stage_w = staging + (warp - 2) * 2 * (RED_BYTES / 4);
 #pragma unroll
-      for (int c = 0; c < 32; ++c) cv[c] = __ldcg(cp + c * ld);
-#pragma unroll 1
-      for (int c0 = 0; c0 < BN; c0 += 32) {
-        if (c0 + 32 < BN) {
-#pragma unroll
-          for (int c = 0; c < 32; ++c) cn[c] = __ldcg(cp + (c0 + 32 + c) * ld);
+      for (int g = 0; g < HALF_COLS / RED_COLS; ++g, ++red_count) {
+        float* buf = stage_w + (red_count & 1) * (RED_BYTES / 4);
+        if (red_count >= 2) {
+          // the reduce issued two groups ago has finished reading this buffer
+          if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+          __syncwarp();
         }
-        float v[32];
-        tmem_ld32(tmem_base + ((uint32_t)(quarter * 32) << 16) + ab * BN + c0, v);
 #pragma unroll
-        for (int c = 0; c < 32; ++c) __stcg(cp + (c0 + c) * ld, fmaf(-(v[c] * inv_r), __ldg(inv_c + c0 + c), cv[c]));
-#pragma unroll
-        for (int c = 0; c < 32; ++c) cv[c] = cn[c];
+        for (int c = 0; c < RED_COLS; ++c)
+          buf[c * 32 + lane] = -(acc[g * RED_COLS + c] * inv_r) * __ldg(inv_c + g * RED_COLS + c);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) {
+          tma_reduce_add_2d(&tm_cr, buf, r0, (int)(slot * P.ts + c0 + g * RED_COLS));
+          asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+        }
       }
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&acc_empty[ab]);
     }
+    // every reduce-add of this thread is complete before the CTA exits
+    if (lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+    __syncwarp();
+    if (!ok) bail = 1;
   }
   tc_fence_before();
   __syncthreads();
@@ -379,6 +460,37 @@ int split_tensor_map(void* storage, const __half* base, int ts, long long rows) 
   return EGS_OK;
 }
 
+// The off-band FP32 pool as a 2-D tensor (tile rows fastest, then every column
+// of every slot).  Two maps per pool: BM x BN boxes, the C block of a CTA tile
+// prefetched to L2, and 32 x RED_COLS boxes, the epilogue's reduce-adds.
+int split_c_tensor_map(void* storage, const float* c_pool, int ts, long long nslots, int box_rows, int box_cols);
+int split_c_maps(void* tm_c, void* tm_cr, const float* c_pool, int ts, long long nslots) {
+  int rc = split_c_tensor_map(tm_c, c_pool, ts, nslots, sg::BM, sg::BN);
+  if (rc == EGS_OK) rc = split_c_tensor_map(tm_cr, c_pool, ts, nslots, 32, sg::RED_COLS);
+  return rc;
+}
+int split_c_tensor_map(void* storage, const float* c_pool, int ts, long long nslots, int box_rows, int box_cols) {
+  std::memset(storage, 0, 128);
+  if (nslots <= 0) return EGS_OK;  // no off-band tile, no update launches
+  void* fn = nullptr;
+  if (tensor_map_encoder(&fn) != EGS_OK) return EGS_ERR_CUDA;
+  if (ts % sg::BN != 0 || ((uintptr_t)c_pool & 15) != 0) return EGS_ERR_INVALID;
+  auto encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  cuuint64_t dims[2] = {(cuuint64_t)ts, (cuuint64_t)(nslots * ts)};
+  cuuint64_t strides[1] = {(cuuint64_t)ts * 4};
+  cuuint32_t box[2] = {(cuuint32_t)box_rows, (cuuint32_t)box_cols};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = encode(reinterpret_cast<CUtensorMap*>(storage), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                      const_cast<float*>(c_pool), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_last_error("cuTensorMapEncodeTiled failed", "split_c_tensor_map");
+    return EGS_ERR_CUDA;
+  }
+  return EGS_OK;
+}
+
 void launch_panel_split(const double* W, int ts, int t0, int ntiles, int row_tile0, float* inv_scale, __half* Ph,
                         __half* Pl, cudaStream_t st) {
   if (ntiles <= 0) return;
@@ -396,8 +508,8 @@ long long split_targets(int nt, int band, int k) {
   return n;
 }
 
-int launch_split_update(const void* tm_hi, const void* tm_lo, int ts, int nt, int band, int k, float* c_pool,
-                        const float* inv_scale, int* err, cudaStream_t st) {
+int launch_split_update(const void* tm_hi, const void* tm_lo, const void* tm_c, const void* tm_cr, int ts, int nt,
+                        int band, int k, float* c_pool, const float* inv_scale, int* err, cudaStream_t st) {
   using namespace sg;
   if (ts % BN != 0) return EGS_ERR_INVALID;
   const long long targets = split_targets(nt, band, k);
@@ -420,7 +532,9 @@ int launch_split_update(const void* tm_hi, const void* tm_lo, int ts, int nt, in
   P.err = err;
   const long long grid = P.total < gemm_num_sms() ? P.total : gemm_num_sms();
   split_gemm_kernel<<<(unsigned)grid, THREADS, SMEM_BYTES, st>>>(*reinterpret_cast<const CUtensorMap*>(tm_hi),
-                                                                 *reinterpret_cast<const CUtensorMap*>(tm_lo), P);
+                                                                 *reinterpret_cast<const CUtensorMap*>(tm_lo),
+                                                                 *reinterpret_cast<const CUtensorMap*>(tm_c),
+                                                                 *reinterpret_cast<const CUtensorMap*>(tm_cr), P);
   return cudaGetLastError() == cudaSuccess ? EGS_OK : EGS_ERR_CUDA;
 }
 
@@ -435,7 +549,8 @@ extern "C" int egs_split_update(int ts, int nt, int band, int k, const double* p
   __half *ph = nullptr, *pl = nullptr;
   float* inv = nullptr;
   int* err = nullptr;
-  alignas(64) unsigned char tmh[128], tml[128];
+  alignas(64) unsigned char tmh[128], tml[128], tmc[128], tmcr[128];
+  const long long mm = nt - band - 1 > 0 ? nt - band - 1 : 0;
   int rc = EGS_OK;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (cudaMalloc(&ph, rows * ts * sizeof(__half)) || cudaMalloc(&pl, rows * ts * sizeof(__half)) ||
@@ -448,13 +563,14 @@ extern "C" int egs_split_update(int ts, int nt, int band, int k, const double* p
   cudaMemset(inv, 0, rows * sizeof(float));
   cudaMemset(ph, 0, rows * ts * sizeof(__half));
   cudaMemset(pl, 0, rows * ts * sizeof(__half));
-  if ((rc = split_tensor_map(tmh, ph, ts, rows)) != EGS_OK || (rc = split_tensor_map(tml, pl, ts, rows)) != EGS_OK)
+  if ((rc = split_tensor_map(tmh, ph, ts, rows)) != EGS_OK || (rc = split_tensor_map(tml, pl, ts, rows)) != EGS_OK ||
+      (rc = split_c_maps(tmc, tmcr, offband, ts, mm * (mm + 1) / 2)) != EGS_OK)
     goto done;
   launch_panel_split(panel, ts, k + 1, nt - k - 1, 0, inv, ph, pl, 0);
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   cudaEventRecord(e0, 0);
-  if ((rc = launch_split_update(tmh, tml, ts, nt, band, k, offband, inv, err, 0)) != EGS_OK) goto done;
+  if ((rc = launch_split_update(tmh, tml, tmc, tmcr, ts, nt, band, k, offband, inv, err, 0)) != EGS_OK) goto done;
   cudaEventRecord(e1, 0);
   if (cudaDeviceSynchronize() != cudaSuccess) {
     rc = EGS_ERR_CUDA;
