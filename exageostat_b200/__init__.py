@@ -25,7 +25,7 @@ EGS_ERR_STATE = -6
 EGS_PRECISION_DOUBLE = 1
 EGS_PRECISION_MIXED = 2
 
-STAGES = ("generate", "panel", "update", "solve", "reduce")
+STAGES = ("generate", "panel", "update", "solve", "reduce", "update_low")
 NUM_STAGES = len(STAGES)
 
 _D = ctypes.POINTER(ctypes.c_double)

@@ -81,11 +81,11 @@ void launch_matern_mixed(double* band, float* off, const double* x, const double
                          cudaStream_t st);
 void launch_gather_column(const double* band, const float* off, double* W, int ts, int nt, int b, int k,
                           cudaStream_t st);
-void launch_scatter_column(const double* W, double* band, float* off, int ts, int nt, int b, int k,
+void launch_scatter_column(const double* W, double* band, float* off, double* inv, int ts, int nt, int b, int k,
                            cudaStream_t st);
 void launch_logdet_band(const double* band, int ts, int nt, int b, int n, double* partial, cudaStream_t st);
-void launch_mixed_solve(const double* band, const float* off, int ts, int nt, int b, double* v, cudaStream_t st,
-                        long long* launches);
+void launch_mixed_solve(const double* band, const float* off, const double* inv, int ts, int nt, int b, double* v,
+                        double* tmp, cudaStream_t st, long long* launches);
 long long residual_scratch_doubles(int n);
 void launch_matern_residual(const double* x, const double* y, const double* z, const double* v, int n, int np,
                             const MaternParams* params, const double* ktab, double* scratch, double* r,

@@ -4,14 +4,18 @@
 // Storage of one problem (nt tile rows of ts, band b >= 0 tile rows kept FP64):
 //   band pool  FP64 tiles (i, j), 0 <= i - j <= b, at slot j*(b+1) + (i-j);
 //   off pool   FP32 tiles (i, j), i - j > b, at tile_slot(i-b-1, j, nt-b-1);
-//   W          FP64 workspace of one tile column: W[t] = tile (k+t, k).
+//   W          FP64 workspace of one tile column: W[t] = tile (k+t, k), plus
+//              W[nt-k] = identity, which the panel solve turns into L_kk^-T;
+//   inv pool   FP64 L_kk^-T of every diagonal tile (upper triangular).
 // The step-k host sequence (capi.cu) gathers column k into W (FP32 tiles
 // widened), factors and solves it there with the FP64 kernels, scatters it back
 // (off-band tiles rounded to FP32), splits it for the FP16 tensor-core update
 // (split_gemm.cu) and runs the FP64 band update with the DMMA kernel.
 //
-// Solves: forward and backward substitution read the band tiles in FP64 and
-// the off-band tiles in FP32 with FP64 arithmetic; one step of iterative
+// Solves: the diagonal blocks are applied through their explicit inverses
+// (a many-block matrix-vector product instead of a sequential substitution),
+// the off-diagonal tiles are read in FP64 (band) or FP32 (off-band) with FP64
+// arithmetic; one step of iterative
 // refinement uses the residual r = z - C v with C regenerated on the fly in
 // FP64 (matern_residual_kernel), so the quadratic form z^T C^-1 z keeps FP64
 // accuracy up to the factor's conditioning.
@@ -69,7 +73,11 @@ gather_column_kernel(const double* __restrict__ band, const float* __restrict__ 
   const long long e = ((long long)blockIdx.x * 256 + threadIdx.x) * 2;
   if (e >= (long long)ts * ts) return;
   double2 v;
-  if (t <= b) {
+  if (t == nt - k) {
+    // identity tile below the column: the panel solve makes it L_kk^-T
+    const long long c = e / ts, r = e - c * ts;
+    v = make_double2(r == c ? 1.0 : 0.0, r + 1 == c ? 1.0 : 0.0);
+  } else if (t <= b) {
     v = *reinterpret_cast<const double2*>(band + band_slot(k + t, k, b) * ts * ts + e);
   } else {
     const float2 f = *reinterpret_cast<const float2*>(off + off_slot(k + t, k, nt, b) * ts * ts + e);
@@ -79,29 +87,34 @@ gather_column_kernel(const double* __restrict__ band, const float* __restrict__ 
 }
 
 __global__ void __launch_bounds__(256)
-scatter_column_kernel(const double* __restrict__ W, double* __restrict__ band, float* __restrict__ off, int ts,
-                      int nt, int b, int k) {
+scatter_column_kernel(const double* __restrict__ W, double* __restrict__ band, float* __restrict__ off,
+                      double* __restrict__ inv, int ts, int nt, int b, int k) {
   const int t = blockIdx.y;
   const long long e = ((long long)blockIdx.x * 256 + threadIdx.x) * 2;
   if (e >= (long long)ts * ts) return;
   const double2 v = *reinterpret_cast<const double2*>(W + (long long)t * ts * ts + e);
-  if (t <= b) {
+  if (t == nt - k) {
+    *reinterpret_cast<double2*>(inv + (long long)k * ts * ts + e) = v;
+  } else if (t <= b) {
     *reinterpret_cast<double2*>(band + band_slot(k + t, k, b) * ts * ts + e) = v;
   } else {
     *reinterpret_cast<float2*>(off + off_slot(k + t, k, nt, b) * ts * ts + e) = make_float2((float)v.x, (float)v.y);
   }
 }
 
+// W[0 .. nt-k-1] = tile column k (FP32 tiles widened), W[nt-k] = identity.
 void launch_gather_column(const double* band, const float* off, double* W, int ts, int nt, int b, int k,
                           cudaStream_t st) {
   const unsigned gx = (unsigned)(((long long)ts * ts / 2 + 255) / 256);
-  gather_column_kernel<<<dim3(gx, nt - k), 256, 0, st>>>(band, off, W, ts, nt, b, k);
+  gather_column_kernel<<<dim3(gx, nt - k + 1), 256, 0, st>>>(band, off, W, ts, nt, b, k);
 }
 
-void launch_scatter_column(const double* W, double* band, float* off, int ts, int nt, int b, int k,
+// Tile column k back to the pools (off-band tiles rounded to FP32) and
+// W[nt-k] = L_kk^-T to inv slot k.
+void launch_scatter_column(const double* W, double* band, float* off, double* inv, int ts, int nt, int b, int k,
                            cudaStream_t st) {
   const unsigned gx = (unsigned)(((long long)ts * ts / 2 + 255) / 256);
-  scatter_column_kernel<<<dim3(gx, nt - k), 256, 0, st>>>(W, band, off, ts, nt, b, k);
+  scatter_column_kernel<<<dim3(gx, nt - k + 1), 256, 0, st>>>(W, band, off, inv, ts, nt, b, k);
 }
 
 // ---------------------------------------------------------------------------
@@ -119,13 +132,17 @@ void launch_logdet_band(const double* band, int ts, int nt, int b, int n, double
   logdet_band_kernel<<<nt, 256, 0, st>>>(band, ts, b, n, partial);
 }
 
-// z_i -= L_ik z_k for every tile row i > k.
+// z_i -= L_ik z_k for every tile row i > k, with z_k read from zk; blocks of
+// the first target row also store zk into z (the solved segment k).
 __global__ void __launch_bounds__(256)
 gemv_mixed_kernel(const double* __restrict__ band, const float* __restrict__ off, int ts, int nt, int b, int k,
-                  double* __restrict__ z) {
+                  const double* __restrict__ zk, double* __restrict__ z) {
   const int i = k + 1 + blockIdx.y;
-  const double* zk = z + (long long)k * ts;
   double* zi = z + (long long)i * ts;
+  if (blockIdx.y == 0) {
+    const int r = blockIdx.x * kNB + threadIdx.x;
+    if (threadIdx.x < kNB && r < ts) z[(long long)k * ts + r] = zk[r];
+  }
   if (i - k <= b) {
     gemv_panel_body(band + band_slot(i, k, b) * (long long)ts * ts, ts, zk, zi, blockIdx.x);
   } else {
@@ -146,12 +163,12 @@ __device__ __forceinline__ double col_dot(const Tile* __restrict__ col, const do
 
 __global__ void __launch_bounds__(256)
 gemv_t_mixed_kernel(const double* __restrict__ band, const float* __restrict__ off, int ts, int nt, int b, int k,
-                    double* __restrict__ z) {
+                    const double* __restrict__ zk, double* __restrict__ z) {
   const int i = blockIdx.y;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int c = blockIdx.x * 8 + warp;
   if (c >= ts) return;
-  const double* zk = z + (long long)k * ts;
+  if (i == 0 && lane == 0) z[(long long)k * ts + c] = zk[c];
   double acc;
   if (k - i <= b) {
     acc = col_dot(band + band_slot(k, i, b) * (long long)ts * ts + (long long)c * ts, zk, ts, lane);
@@ -161,25 +178,69 @@ gemv_t_mixed_kernel(const double* __restrict__ band, const float* __restrict__ o
   if (lane == 0) z[(long long)i * ts + c] -= acc;
 }
 
-// v := (L L^T)^-1 v with the mixed factor.
-void launch_mixed_solve(const double* band, const float* off, int ts, int nt, int b, double* v, cudaStream_t st,
-                        long long* launches) {
+// out = L_kk^-1 in = X^T in with X = L_kk^-T (upper triangular, column-major):
+// out[i] = sum_{j <= i} X[j, i] in[j]; one warp per output (a contiguous column).
+__global__ void __launch_bounds__(256)
+inv_apply_t_kernel(const double* __restrict__ X, int ts, const double* __restrict__ in, double* __restrict__ out) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i = blockIdx.x * 8 + warp;
+  if (i >= ts) return;
+  const double* col = X + (long long)i * ts;
+  double acc = 0.0;
+  for (int j = lane; j <= i; j += 32) acc = fma(col[j], in[j], acc);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0) out[i] = acc;
+}
+
+// out = L_kk^-T in = X in: out[i] = sum_{j >= i} X[i, j] in[j]; 64 rows x 4
+// column groups per block, fixed reduction order.  Dynamic shared memory: ts doubles.
+__global__ void __launch_bounds__(256)
+inv_apply_kernel(const double* __restrict__ X, int ts, const double* __restrict__ in, double* __restrict__ out) {
+  extern __shared__ double ins[];
+  __shared__ double red[4][kNB];
+  for (int c = threadIdx.x; c < ts; c += blockDim.x) ins[c] = in[c];
+  __syncthreads();
+  const int rl = threadIdx.x & (kNB - 1), g = threadIdx.x / kNB;
+  const int i = blockIdx.x * kNB + rl;
+  double acc = 0.0;
+  if (i < ts) {
+    for (int j = blockIdx.x * kNB + g; j < ts; j += 4)
+      if (j >= i) acc = fma(X[i + (long long)j * ts], ins[j], acc);
+  }
+  red[g][rl] = acc;
+  __syncthreads();
+  if (g == 0 && i < ts) out[i] = ((red[0][rl] + red[1][rl]) + red[2][rl]) + red[3][rl];
+}
+
+__global__ void copy_segment_kernel(const double* __restrict__ src, double* __restrict__ dst, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = src[i];
+}
+
+// v := (L L^T)^-1 v with the mixed factor; tmp holds ts doubles.
+void launch_mixed_solve(const double* band, const float* off, const double* inv, int ts, int nt, int b, double* v,
+                        double* tmp, cudaStream_t st, long long* launches) {
+  const long long ts2 = (long long)ts * ts;
   for (int k = 0; k < nt; ++k) {
-    launch_trsv_diag(band, ts, band_slot(k, k, b), v + (long long)k * ts, st);
-    ++*launches;
+    inv_apply_t_kernel<<<(ts + 7) / 8, 256, 0, st>>>(inv + k * ts2, ts, v + (long long)k * ts, tmp);
     if (k < nt - 1) {
       gemv_mixed_kernel<<<dim3((ts + kNB - 1) / kNB, nt - 1 - k), 256, ts * sizeof(double), st>>>(band, off, ts, nt,
-                                                                                                 b, k, v);
-      ++*launches;
+                                                                                                 b, k, tmp, v);
+    } else {
+      copy_segment_kernel<<<(ts + 255) / 256, 256, 0, st>>>(tmp, v + (long long)k * ts, ts);
     }
+    *launches += 2;
   }
   for (int k = nt - 1; k >= 0; --k) {
-    launch_trsv_t_diag(band, ts, band_slot(k, k, b), v + (long long)k * ts, st);
-    ++*launches;
+    inv_apply_kernel<<<(ts + kNB - 1) / kNB, 256, ts * sizeof(double), st>>>(inv + k * ts2, ts, v + (long long)k * ts,
+                                                                               tmp);
     if (k > 0) {
-      gemv_t_mixed_kernel<<<dim3((ts + 7) / 8, k), 256, 0, st>>>(band, off, ts, nt, b, k, v);
-      ++*launches;
+      gemv_t_mixed_kernel<<<dim3((ts + 7) / 8, k), 256, 0, st>>>(band, off, ts, nt, b, k, tmp, v);
+    } else {
+      copy_segment_kernel<<<(ts + 255) / 256, 256, 0, st>>>(tmp, v, ts);
     }
+    *launches += 2;
   }
 }
 
