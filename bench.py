@@ -1,14 +1,19 @@
 #!/usr/bin/env python3
-"""Log-likelihood evaluations per second of the plain-FP64 B200 path.
+"""Log-likelihood evaluations per second of the mixed-precision B200 path beside
+the plain-FP64 B200 path, at the stated relative error.
 
-Workload (the reference's N = 40,000 plain-FP64 configuration): 41,000 synthetic
-locations from the reference generator (jittered 203 x 203 grid, Morton sorted,
-16-bit quantised, srand(0)), observations Z = L e at theta_true = (1, 0.05, 0.8)
-with e = DLARNV(3, {0,0,0,1}), 1,000 points held out at random, and the
-log-likelihood of the remaining N = 40,000 evaluated at theta_true with tile 960.
-One step = one full evaluation (Matern generation, tiled Cholesky, log-det,
-triangular solve, dot, assembly) with the inputs resident in HBM.  The tile
-storage is 6.6 GB, far larger than the 126 MB L2, so no flush is needed.
+Workload (the mixed-precision configuration): N = 102,400 synthetic locations
+from the reference generator (jittered 320 x 320 grid, Morton sorted, 16-bit
+quantised, srand(0)), observations Z = L e at theta = (1, 0.1, 0.5) with
+e = DLARNV(3, {0,0,0,1}) generated on the device, tile 1024.  The mixed form
+keeps the diagonal tile and 2 tiles below it in FP64 and stores the other 4,753
+tiles in FP32 with split-FP16 tensor-core updates; the plain form is the exact
+FP64 path.  One step = one full evaluation (Matern generation, tiled Cholesky,
+log-det, triangular solves with one refinement step, assembly) with the
+inputs resident in HBM.  The tile storage (22 GB mixed, 42 GB FP64) is far
+larger than the 126 MB L2, so no flush is needed.  The relative error is the
+mixed log-likelihood against the plain FP64 path at the same N (itself within
+1e-10 of the CPU oracle in the tests).
 
 ``python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]``
 Under torchrun each rank evaluates its own replica (a single evaluation does not
@@ -28,34 +33,22 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-N_TOTAL = 41000
-N_MISS = 1000
-DTS = 960
-THETA = (1.0, 0.05, 0.8)
+N = 102400
+DTS = 1024
+BAND = 2
+THETA = (1.0, 0.1, 0.5)
 SEED = 0
-METRIC = "loglik evals/s (plain FP64, N=40000 Matern, tile 960)"
+METRIC = "loglik evals/s mixed vs plain FP64 on B200 at stated rel. error; p50/p99 ms"
 UNIT = "evals/s"
 CONFIG = {
-    "workload": "MLE log-likelihood evaluation, N=40000 (41000 generated, 1000 held out), 2-D Matern, "
-                "theta=(1,0.05,0.8), tile 960, plain FP64",
-    "n": N_TOTAL - N_MISS, "tile": DTS, "theta": list(THETA), "precision": "fp64",
-    "l2": "inputs larger than L2 (6.6 GB tile storage vs 126 MB L2); no flush",
+    "workload": "MLE log-likelihood evaluation, N=102400 (320x320 jittered grid), 2-D Matern, theta=(1,0.1,0.5), "
+                "tile 1024; mixed precision: FP64 diagonal + band of 2 tiles, FP32 off-band tiles with split-FP16 "
+                "tcgen05 updates, one refinement step; beside it the plain FP64 path at the same N",
+    "n": N, "tile": DTS, "band_tiles": BAND, "theta": list(THETA), "precision": "mixed (value) / fp64 (plain_fp64)",
+    "l2": "inputs larger than L2 (22 GB mixed / 42 GB FP64 tile storage vs 126 MB L2); no flush",
 }
-# DRAM bytes per updated C element of the trailing-update kernel, from one ncu
-# capture of a full trailing update (N = 8,000, tile 960: 571 MB for 1,830
-# 128 x 128 blocks; profiles/dgemm_update_kernel_n8000.md).  The per-launch
-# traffic of this workload is that figure times each launch's block count.
-UPDATE_DRAM_BYTES_PER_C_ELEMENT = 571.28e6 / (1830 * 128 * 128)
-
-
-def update_traffic_per_launch(n: int, ts: int) -> float:
-    """Mean DRAM bytes of one trailing-update launch at (n, ts), scaled from the capture."""
-    nt = -(-n // ts)
-    per = []
-    for k in range(nt - 1):
-        mb = -(-((nt - k - 1) * ts) // 128)
-        per.append(mb * (mb + 1) // 2 * 128 * 128 * UPDATE_DRAM_BYTES_PER_C_ELEMENT)
-    return sum(per) / max(len(per), 1)
+# Secondary line item: the reference's plain-FP64 GPU configuration.
+N40_TOTAL, N40_MISS, N40_DTS, N40_THETA = 41000, 1000, 960, (1.0, 0.05, 0.8)
 
 
 def env_rank():
@@ -64,16 +57,34 @@ def env_rank():
 
 
 def workload_data(egs):
-    """Locations, Z (generated on the device), and the 40,000-point training split."""
-    import numpy as np
-    x, y = egs.generate_locations(N_TOTAL, SEED)
-    gen = egs.Problem(N_TOTAL, DTS)
+    """Locations and Z = L e at theta, generated on the device (FP64 path)."""
+    x, y = egs.generate_locations(N, SEED)
+    gen = egs.Problem(N, DTS)
     gen.set_locations(x, y)
     z = gen.generate_observations(THETA, SEED)
     gen.close()
-    perm = np.random.default_rng(SEED).permutation(N_TOTAL)
-    train = np.sort(perm[N_MISS:])
+    return x, y, z
+
+
+def workload_n40000(egs):
+    """The 40,000-point training split of the 41,000-point plain-FP64 configuration."""
+    import numpy as np
+    x, y = egs.generate_locations(N40_TOTAL, SEED)
+    gen = egs.Problem(N40_TOTAL, N40_DTS)
+    gen.set_locations(x, y)
+    z = gen.generate_observations(N40_THETA, SEED)
+    gen.close()
+    perm = np.random.default_rng(SEED).permutation(N40_TOTAL)
+    train = np.sort(perm[N40_MISS:])
     return x[train].copy(), y[train].copy(), z[train].copy()
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
 
 
 class ClockSampler:
@@ -178,7 +189,7 @@ def cpu_sample(x, y, z, target_s: float = 12.0):
     value = C.scaled_evals_per_s(st, ns, n_target)
     return value, {
         "cores": C.threads(), "n_sample": ns, "stage_s": {k: round(v, 4) for k, v in st.items()},
-        "sample": f"one full evaluation at N={ns} (first {ns} training points, theta={THETA}); "
+        "sample": f"one full FP64 evaluation at N={ns} (first {ns} of the workload's points, theta={THETA}); "
                   f"generation and solve scaled by (N/{ns})^2, potrf by (N/{ns})^3 to N={n_target}"}
 
 
@@ -189,16 +200,13 @@ def run_reference(args):
     import numpy as np
     from oracle import cpu_baseline as C
     from oracle import oracle as O
-    # Same inputs as the B200 arm, produced on the host by the oracle's generator.
-    # Z for the sampled subset only (a 41,000-point CPU Cholesky would dominate).
+    # Same locations as the B200 arm, produced on the host by the oracle's
+    # generator; the CPU path is the reference's FP64 dense evaluation.  Z for
+    # the sampled subset only (its cost does not depend on the values).
     t0 = time.perf_counter()
-    x, y = O.generate_locations(N_TOTAL, O.GlibcRand(SEED))
-    perm = np.random.default_rng(SEED).permutation(N_TOTAL)
-    train = np.sort(perm[N_MISS:])
-    x, y = x[train], y[train]
-    n_target = len(x)
+    x, y = O.generate_locations(N, O.GlibcRand(SEED))
     ns = 6000
-    z = O.dlarnv_normal(SEED, ns)  # any standard-normal observations: cost does not depend on Z
+    z = O.dlarnv_normal(SEED, ns)
     _, st = C.timed_eval(x[:ns], y[:ns], z, THETA)
     per_step = 4.0
     grow = (per_step / max(sum(st.values()), 1e-3)) ** (1.0 / 3.0)
@@ -211,7 +219,7 @@ def run_reference(args):
     lat = []
     for _ in range(args.steps):
         _, st = C.timed_eval(x[:ns], y[:ns], z, THETA, a)
-        scaled.append(1.0 / C.scaled_evals_per_s(st, ns, n_target))
+        scaled.append(1.0 / C.scaled_evals_per_s(st, ns, N))
         lat.append(sum(st.values()))
     total = sum(scaled)
     value = args.steps / total
@@ -221,33 +229,168 @@ def run_reference(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (reference generator semantics)",
         "config": CONFIG,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": C.threads(), "kind": "port",
-                         "sample": f"each step one full evaluation at N={ns} on all host threads "
+                         "sample": f"each step one full FP64 evaluation at N={ns} on all host threads "
                                    f"(Matern in C/pthreads, LAPACK dpotrf/dtrtrs via OpenBLAS), scaled to "
-                                   f"N={n_target} by n^2 (generation, solve) and n^3 (potrf)"},
+                                   f"N={N} by n^2 (generation, solve) and n^3 (potrf)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "p50_ms": 1e3 * statistics.median(scaled), "p99_ms": 1e3 * float(np.percentile(scaled, 99)),
         "sample_step_s_p50": statistics.median(lat), "wall_s": time.perf_counter() - t0,
     }
     print(json.dumps(line), flush=True)
     return 0
 
 
+def timed_evals(torch, p, stream, theta, steps, dist=None):
+    """Device time (ms, max over ranks) of `steps` evaluations, host latencies (ms) and the last result."""
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    lat = []
+    e0.record(stream)
+    for _ in range(steps):
+        t = time.perf_counter()
+        r = p.mle_eval(theta)
+        lat.append(1e3 * (time.perf_counter() - t))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        tt = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    return ms, lat, r
+
+
+def plain_n40000(egs, torch, steps, peak):
+    """The plain-FP64 path at the reference's N = 40,000 GPU configuration (tile 960)."""
+    x, y, z = workload_n40000(egs)
+    stream = torch.cuda.Stream()
+    p = egs.Problem(len(z), N40_DTS)
+    p.set_stream(stream.cuda_stream)
+    p.set_locations(x, y)
+    p.set_observations(z)
+    for _ in range(3):
+        p.mle_eval(N40_THETA)
+    p.set_profiling(True)
+    ms, _, r = timed_evals(torch, p, stream, N40_THETA, steps)
+    st_ms, st_fl, _ = p.stage_stats()
+    p.close()
+    up = egs.STAGES.index("update")
+    ach = st_fl[up] / (st_ms[up] * 1e-3) / 1e12
+    return {"config": "plain FP64, N=40000 (41000 generated, 1000 held out), theta=(1,0.05,0.8), tile 960",
+            "evals_per_s": steps / (ms * 1e-3), "ms_per_eval": ms / steps, "loglik": r[0],
+            "trailing_update_tflops": ach, "trailing_update_frac_of_dgemm": ach / peak}
+
+
+def run_serving(args):
+    """Open-loop Poisson request stream through the serving loop, rate swept.
+
+    Mix: 35% log-likelihood, 35% fit (BOBYQA, at most --serve-fit-evals
+    evaluations), 30% predict (500 targets); N log-uniform in [1,000, 60,000]
+    on jittered grids, theta drawn as sigma^2 ~ U[0.5, 2], beta ~ U[0.02, 0.3],
+    nu ~ U[0.3, 2.5]; observations are i.i.d. N(0, 1) (the cost does not depend
+    on their values).  HBM admission budget 160 GB.  Reports p50/p99 latency
+    (submission to completion) and evaluations/s per rate, for the plain and the
+    mixed form (FP64 band of 2 tiles)."""
+    import numpy as np
+    import torch
+    import exageostat_b200 as egs
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(12345)
+    pool = []
+    for i in range(24):
+        n = int(round(math.exp(rng.uniform(math.log(1000), math.log(60000)))))
+        x, y = egs.generate_locations(n, i % 4096)
+        z = rng.standard_normal(n)
+        pool.append((x, y, z))
+    xm_all, ym_all = rng.random(500), rng.random(500)
+    lines = []
+    for rate in args.serve_rates:
+        # one arrival sequence per rate, replayed for both forms
+        g = np.random.default_rng(int(rate * 1000) + 7)
+        arr = []
+        t = 0.0
+        while True:
+            t += g.exponential(1.0 / rate)
+            if t > args.serve_seconds:
+                break
+            arr.append(t)
+        picks = []
+        for a in arr:
+            u = g.random()
+            kind = egs.EGS_REQ_LOGLIK if u < 0.35 else (egs.EGS_REQ_FIT if u < 0.70 else egs.EGS_REQ_PREDICT)
+            theta = (g.uniform(0.5, 2.0), g.uniform(0.02, 0.3), g.uniform(0.3, 2.5))
+            picks.append((a, int(g.integers(len(pool))), kind, theta))
+        for precision, label in ((egs.EGS_PRECISION_DOUBLE, "plain"), (egs.EGS_PRECISION_MIXED, "mixed")):
+            reqs = []
+            for a, idx, kind, theta in picks:
+                x, y, z = pool[idx]
+                dts = 512 if len(z) < 8000 else 1024
+                r = dict(kind=kind, x=x, y=y, z=z, dts=dts, theta=theta, precision=precision,
+                         band_tiles=2 if precision == egs.EGS_PRECISION_MIXED else 0,
+                         max_evals=args.serve_fit_evals, ftol_abs=1e-9)
+                if kind == egs.EGS_REQ_PREDICT:
+                    r["x_miss"], r["y_miss"] = xm_all, ym_all
+                reqs.append((a, r))
+            with egs.Server(hbm_budget=160 * 10**9, max_active=args.serve_slots) as srv:
+                t0 = time.perf_counter()
+                tickets = []
+                for a, r in reqs:
+                    d = a - (time.perf_counter() - t0)
+                    if d > 0:
+                        time.sleep(d)
+                    tickets.append(srv.submit(**r))
+                res = [srv.wait(tk)[0] for tk in tickets]
+                span = time.perf_counter() - t0
+                st = srv.stats()
+            lat = np.array([r.latency_ms for r in res])
+            kinds = {egs.EGS_REQ_LOGLIK: "loglik", egs.EGS_REQ_FIT: "fit", egs.EGS_REQ_PREDICT: "predict"}
+            per = {}
+            for k, name in kinds.items():
+                lk = np.array([r.latency_ms for r in res if r.kind == k])
+                if len(lk):
+                    per[name] = {"n": int(len(lk)), "p50_ms": float(np.percentile(lk, 50)),
+                                 "p99_ms": float(np.percentile(lk, 99))}
+            lines.append({"form": label, "rate_per_s": rate, "requests": len(res),
+                          "failed": int(sum(r.status != 0 for r in res)),
+                          "failed_not_positive_definite": int(sum(r.status > 0 for r in res)),
+                          "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                          "evals_per_s": st["evals"] / span, "span_s": span, "per_kind": per,
+                          "peak_active": st["peak_active"], "peak_reserved_gb": st["peak_reserved"] / 1e9})
+            print(json.dumps(lines[-1]), flush=True)
+    print(json.dumps({"metric": METRIC, "workload": "serving", "unit": UNIT, "slots": args.serve_slots,
+                      "hbm_budget_gb": 160, "fit_max_evals": args.serve_fit_evals, "sweep": lines}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain-steps", type=int, default=2, help="timed plain-FP64 evaluations at N=102400")
     ap.add_argument("--profile-eval", action="store_true",
-                    help="one evaluation between cudaProfilerStart/Stop (for ncu --profile-from-start off)")
+                    help="one mixed evaluation between cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     ap.add_argument("--profile-n", type=int, default=0,
-                    help="with --profile-eval: evaluate this many of the workload's locations with "
-                         "DLARNV observations instead of the full workload (small ncu captures)")
+                    help="with --profile-eval: evaluate this many points of a jittered grid with DLARNV "
+                         "observations instead of the full workload (small ncu captures)")
+    ap.add_argument("--profile-plain", action="store_true", help="with --profile-eval: the plain FP64 path")
+    ap.add_argument("--workload", default="eval", choices=["eval", "serving"])
+    ap.add_argument("--serve-rates", type=float, nargs="+", default=[0.25, 0.5, 1.0])
+    ap.add_argument("--serve-seconds", type=float, default=30.0)
+    ap.add_argument("--serve-slots", type=int, default=6)
+    ap.add_argument("--serve-fit-evals", type=int, default=10)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "serving":
+        return run_serving(args)
 
     import numpy as np
     import torch
@@ -259,7 +402,7 @@ def main():
         import datetime
         import torch.distributed as dist
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     else:
         torch.cuda.set_device(0)
     dev = torch.cuda.current_device()
@@ -277,6 +420,8 @@ def main():
         else:
             x, y, z = workload_data(egs)
         p = egs.Problem(len(z), DTS)
+        if not args.profile_plain:
+            p.set_precision(egs.EGS_PRECISION_MIXED, BAND)
         p.set_locations(x, y)
         p.set_observations(z)
         p.mle_eval(THETA)
@@ -288,95 +433,119 @@ def main():
         p.close()
         return 0
 
-    peak = fp64_dgemm_peak_tflops(torch)
+    peaks = load_peaks()
+    fp64_peak = fp64_dgemm_peak_tflops(torch)
     x, y, z = workload_data(egs)
-    n = len(z)
 
+    # --- mixed precision: the headline -------------------------------------------------
     stream = torch.cuda.Stream()
-    p = egs.Problem(n, DTS)
-    p.set_stream(stream.cuda_stream)
-    p.set_locations(x, y)
-    p.set_observations(z)
+    q = egs.Problem(N, DTS)
+    q.set_precision(egs.EGS_PRECISION_MIXED, BAND)
+    q.set_stream(stream.cuda_stream)
+    q.set_locations(x, y)
+    q.set_observations(z)
     for _ in range(args.warmup):
-        p.mle_eval(THETA)
-    p.set_profiling(True)
-
+        q.mle_eval(THETA)
+    q.set_profiling(True)
     clocks = ClockSampler(bus)
     clocks.start()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    lat = []
-    e0.record(stream)
-    for _ in range(args.steps):
-        t = time.perf_counter()
-        ll, logdet, dot = p.mle_eval(THETA)
-        lat.append(1e3 * (time.perf_counter() - t))
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
+    ms, lat, (ll, logdet, dot) = timed_evals(torch, q, stream, THETA, args.steps, dist)
     clk = clocks.stop()
-    if dist:
-        tt = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
-    stage_ms, stage_flops, stage_launches = p.stage_stats()
-    p.set_profiling(False)
+    stage_ms, stage_flops, stage_launches = q.stage_stats()
+    q.set_profiling(False)
     value = world * args.steps / (ms * 1e-3)
 
-    # end to end through the host-buffer C ABI, pinned host inputs, copies in the timed region
+    # end to end through the C ABI with host buffers: locations and observations
+    # uploaded from pinned host memory every step, the result read back
     pin = [torch.from_numpy(a).pin_memory() for a in (x, y, z)]
     xh, yh, zh = (t.numpy() for t in pin)
-    egs.mle_loglik_host(xh, yh, zh, THETA, DTS)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        ll_e2e = egs.mle_loglik_host(xh, yh, zh, THETA, DTS)
+        q.set_locations(xh, yh)
+        q.set_observations(zh)
+        ll_e2e = q.mle_eval(THETA)[0]
     e2e_s = time.perf_counter() - t0
     if dist:
         tt = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e2e_s = float(tt.item())
-    e2e = {"value": world * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 3 * n * 8 + 64,
-           "d2h_bytes_per_step": 8 + 32, "api": "egs_mle_loglik_host (C ABI, host buffers)"}
+    e2e = {"value": world * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 3 * N * 8 + 64,
+           "d2h_bytes_per_step": 4 * 8 + 8,
+           "api": "egs_problem_set_locations + egs_problem_set_observations + egs_mle_eval "
+                  "(C ABI, pinned host buffers, mixed precision)"}
+    q.close()
 
+    # --- plain FP64 at the same N: speed and the accuracy reference ----------------------
+    ps = torch.cuda.Stream()
+    p = egs.Problem(N, DTS)
+    p.set_stream(ps.cuda_stream)
+    p.set_locations(x, y)
+    p.set_observations(z)
+    p.mle_eval(THETA)
+    p.set_profiling(True)
+    pms, plat, (pll, plogdet, pdot) = timed_evals(torch, p, ps, THETA, args.plain_steps, dist)
+    p_ms, p_fl, p_ln = p.stage_stats()
+    p.close()
+    plain_value = world * args.plain_steps / (pms * 1e-3)
     up = egs.STAGES.index("update")
-    achieved = stage_flops[up] / (stage_ms[up] * 1e-3) / 1e12 if stage_ms[up] > 0 else None
-    n_up = int(stage_launches[up])
-    roof = {"bound": "tensor", "kernel": "dgemm_update_kernel (trailing syrk/gemm, FP64 DMMA)",
-            "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-            "frac": (achieved / peak) if achieved else None,
-            "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor; MEASURED_PEAKS.json has no FP64 entry)",
-            "traffic": update_traffic_per_launch(n, DTS),
-            "traffic_note": "DRAM bytes per launch: 19.0 B per updated C element (ncu, N=8000 trailing update) "
-                            "times the mean block count of this workload's launches",
-            "launches": n_up,
-            "flops_per_launch": stage_flops[up] / max(n_up, 1)}
-    eval_flops = n ** 3 / 3.0 + n ** 2 / 2.0 + n / 6.0 + n ** 2
-    small = small_problem_rate(egs, torch)
+    plain_update = p_fl[up] / (p_ms[up] * 1e-3) / 1e12
+    plain = {"value": plain_value, "unit": UNIT, "ms_per_eval": pms / args.plain_steps,
+             "p50_ms": statistics.median(plat), "loglik": pll, "logdet": plogdet, "dot": pdot,
+             "trailing_update_tflops": plain_update, "trailing_update_frac_of_dgemm": plain_update / fp64_peak,
+             "stages_ms_per_eval": {s: float(p_ms[i]) / args.plain_steps for i, s in enumerate(egs.STAGES)},
+             "steps": args.plain_steps, "warmup": 1}
+    rel = {"loglik": abs(ll - pll) / abs(pll), "logdet": abs(logdet - plogdet) / abs(plogdet),
+           "dot": abs(dot - pdot) / abs(pdot), "against": "plain FP64 B200 path at the same N"}
+
+    # --- rooflines of the update kernels (CUDA events around every launch) ---------------
+    lo = egs.STAGES.index("update_low")
+    bf16_peak = peaks.get("bf16_tflops_sustained") or 1386.0
+    roofs = []
+    if stage_ms[lo] > 0:
+        a = stage_flops[lo] / (stage_ms[lo] * 1e-3) / 1e12
+        n_l = int(stage_launches[lo])
+        roofs.append({"bound": "tensor", "kernel": "split_gemm_kernel (off-band C -= P_i P_j^T, split-FP16 tcgen05, "
+                                                   "FP32-accurate)",
+                      "achieved": a, "peak": bf16_peak, "unit": "TFLOP/s", "frac": a / bf16_peak,
+                      "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)",
+                      "executed_tflops": 3.0 * a, "frac_executed": 3.0 * a / bf16_peak,
+                      "note": "achieved counts the algorithmic 2*ts^3 flops per target tile; the kernel executes "
+                              "three FP16 products per tile (hi*hi, hi*lo, lo*hi)",
+                      "traffic": None, "launches": n_l, "ms_per_eval": float(stage_ms[lo]) / args.steps,
+                      "flops_per_launch": stage_flops[lo] / max(n_l, 1)})
+    if stage_ms[up] > 0:
+        a = stage_flops[up] / (stage_ms[up] * 1e-3) / 1e12
+        n_u = int(stage_launches[up])
+        roofs.append({"bound": "tensor", "kernel": "dgemm_update_kernel (FP64 band update, DMMA)",
+                      "achieved": a, "peak": fp64_peak, "unit": "TFLOP/s", "frac": a / fp64_peak,
+                      "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 entry)",
+                      "traffic": None, "launches": n_u, "ms_per_eval": float(stage_ms[up]) / args.steps,
+                      "flops_per_launch": stage_flops[up] / max(n_u, 1)})
+    roofs.sort(key=lambda r: -r["ms_per_eval"])
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (reference generator semantics, generated on device)",
+        "vs_baseline": None, "dtype": "f16/f32/f64 (mixed)",
+        "data": "synthetic (reference generator semantics, generated on device)",
         "config": dict(CONFIG, parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
-        "loglik": ll, "loglik_e2e": ll_e2e,
+        "loglik": ll, "loglik_e2e": ll_e2e, "logdet": logdet, "dot": dot,
         "p50_ms": statistics.median(lat), "p99_ms": float(np.percentile(lat, 99)),
-        "eval_tflops": eval_flops * world * args.steps / (ms * 1e-3) / 1e12,
+        "plain_fp64": plain, "speedup_vs_plain": value / plain_value, "rel_error": rel,
         "stages_ms_per_eval": {s: float(stage_ms[i]) / args.steps for i, s in enumerate(egs.STAGES)},
-        "roofline": roof, "e2e": e2e,
+        "roofline": roofs[0] if roofs else None, "roofline_other": roofs[1:],
+        "e2e": e2e,
         "gpu_launches": int(stage_launches.sum()),
-        "small_n": small,
         "clocks": clk,
     }
+    line["plain_n40000"] = plain_n40000(egs, torch, 3, fp64_peak)
+    line["small_n"] = small_problem_rate(egs, torch)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, info = cpu_sample(x, y, z)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": info["cores"], "kind": "port",
                                 "sample": info["sample"], "stage_s": info["stage_s"]}
-    p.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

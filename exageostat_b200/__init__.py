@@ -24,6 +24,9 @@ EGS_ERR_TIMEOUT = -5
 EGS_ERR_STATE = -6
 EGS_PRECISION_DOUBLE = 1
 EGS_PRECISION_MIXED = 2
+EGS_REQ_LOGLIK = 1
+EGS_REQ_FIT = 2
+EGS_REQ_PREDICT = 3
 
 STAGES = ("generate", "panel", "update", "solve", "reduce", "update_low")
 NUM_STAGES = len(STAGES)
@@ -77,7 +80,35 @@ SIGNATURES = {
     "egs_batch_eval": (ctypes.c_int, [_P, _D, _D, _I]),
     "egs_batch_autotune": (ctypes.c_int, [ctypes.c_int, _I, _D, _D, _D, _D, _I, ctypes.c_int, _I, _D]),
     "egs_split_update": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P, _D]),
+    "egs_problem_create_ex": (ctypes.c_int, [ctypes.POINTER(_P), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_int]),
+    "egs_problem_footprint": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _LL]),
+    "egs_problem_predict": (ctypes.c_int, [_P, _D, ctypes.c_int, _D, _D, _D]),
 }
+
+
+class Request(ctypes.Structure):
+    """egs_request of the serving API."""
+    _fields_ = [("kind", ctypes.c_int), ("n", ctypes.c_int), ("dts", ctypes.c_int), ("precision", ctypes.c_int),
+                ("band_tiles", ctypes.c_int), ("x", _D), ("y", _D), ("z", _D), ("theta", ctypes.c_double * 3),
+                ("lb", ctypes.c_double * 3), ("ub", ctypes.c_double * 3), ("ftol_abs", ctypes.c_double),
+                ("max_evals", ctypes.c_int), ("n_miss", ctypes.c_int), ("x_miss", _D), ("y_miss", _D)]
+
+
+class Result(ctypes.Structure):
+    """egs_result of the serving API."""
+    _fields_ = [("status", ctypes.c_int), ("kind", ctypes.c_int), ("loglik", ctypes.c_double),
+                ("theta", ctypes.c_double * 3), ("evals", ctypes.c_int), ("queue_ms", ctypes.c_double),
+                ("latency_ms", ctypes.c_double), ("footprint", ctypes.c_longlong)]
+
+
+SIGNATURES.update({
+    "egs_server_create": (ctypes.c_int, [ctypes.POINTER(_P), ctypes.c_int, ctypes.c_longlong, ctypes.c_int]),
+    "egs_server_submit": (ctypes.c_int, [_P, ctypes.POINTER(Request), _LL]),
+    "egs_server_wait": (ctypes.c_int, [_P, ctypes.c_longlong, ctypes.POINTER(Result), _D]),
+    "egs_server_stats": (ctypes.c_int, [_P, _I, _I, _LL, _I, _LL, _LL, _LL]),
+    "egs_server_destroy": (ctypes.c_int, [_P]),
+})
 
 OBJECTIVE = ctypes.CFUNCTYPE(ctypes.c_double, ctypes.c_int, _D, ctypes.c_void_p)
 SIGNATURES["egs_bobyqa_maximize"] = (ctypes.c_int, [ctypes.c_int, _D, _D, _D, ctypes.c_double, ctypes.c_double,
@@ -135,10 +166,15 @@ def _f64(a) -> np.ndarray:
 class Problem:
     """Device-resident problem of n locations (``egs_problem``)."""
 
-    def __init__(self, n: int, dts: int):
+    def __init__(self, n: int, dts: int, precision: int = 0, band_tiles: int = 0):
+        """precision 0: FP64, switchable later with set_precision; EGS_PRECISION_*: created in that precision."""
         self._lib = load_library()
         self._h = _P()
-        _check(self._lib.egs_problem_create(ctypes.byref(self._h), int(n), int(dts)), "egs_problem_create")
+        if precision:
+            _check(self._lib.egs_problem_create_ex(ctypes.byref(self._h), int(n), int(dts), int(precision),
+                                                   int(band_tiles)), "egs_problem_create_ex")
+        else:
+            _check(self._lib.egs_problem_create(ctypes.byref(self._h), int(n), int(dts)), "egs_problem_create")
         self.n = int(n)
         self.dts = int(dts)
         nn, ts, nt, nb = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()
@@ -237,6 +273,15 @@ class Problem:
         nn, ts, nt, nb = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()
         self._lib.egs_problem_info(self._h, ctypes.byref(nn), ctypes.byref(ts), ctypes.byref(nt), ctypes.byref(nb))
         self.ts, self.nt, self.bytes = ts.value, nt.value, nb.value
+
+    def predict(self, theta, x_miss, y_miss) -> np.ndarray:
+        """Kriging at the targets with the resident observations (either precision)."""
+        th = _f64(theta)
+        xm, ym = _f64(x_miss), _f64(y_miss)
+        out = np.zeros(len(xm))
+        _check(self._lib.egs_problem_predict(self._h, _dptr(th), len(xm), _dptr(xm), _dptr(ym), _dptr(out)),
+               "predict")
+        return out
 
     def set_stream(self, cuda_stream_handle) -> None:
         _check(self._lib.egs_problem_set_stream(self._h, _P(cuda_stream_handle)), "set_stream")
@@ -383,3 +428,69 @@ def split_update(ts: int, nt: int, band: int, k: int, panel_ptr: int, offband_pt
     _check(lib.egs_split_update(int(ts), int(nt), int(band), int(k), _P(panel_ptr), _P(offband_ptr),
                                 ctypes.byref(ms)), "egs_split_update")
     return ms.value
+
+
+def footprint(n: int, dts: int, precision: int = EGS_PRECISION_DOUBLE, band_tiles: int = 0) -> int:
+    """Device bytes of a problem of this shape (no device needed)."""
+    b = ctypes.c_longlong()
+    _check(load_library().egs_problem_footprint(int(n), int(dts), int(precision), int(band_tiles), ctypes.byref(b)),
+           "footprint")
+    return b.value
+
+
+class Server:
+    """The serving loop: queued requests admitted by HBM footprint, run concurrently."""
+
+    def __init__(self, hbm_budget: int, max_active: int, device: int = 0):
+        self._lib = load_library()
+        h = _P()
+        _check(self._lib.egs_server_create(ctypes.byref(h), int(device), int(hbm_budget), int(max_active)),
+               "egs_server_create")
+        self._h = h
+        self._keep = {}
+
+    def submit(self, kind, x, y, z, dts, theta=(1.0, 0.1, 0.5), precision=EGS_PRECISION_DOUBLE, band_tiles=0,
+               lb=(0.01, 0.01, 0.01), ub=(5.0, 5.0, 5.0), ftol_abs=1e-9, max_evals=100, x_miss=None, y_miss=None):
+        x, y, z = _f64(x), _f64(y), _f64(z)
+        r = Request(kind=int(kind), n=len(z), dts=int(dts), precision=int(precision), band_tiles=int(band_tiles),
+                    x=_dptr(x), y=_dptr(y), z=_dptr(z), ftol_abs=float(ftol_abs), max_evals=int(max_evals))
+        r.theta[:] = list(theta)
+        r.lb[:] = list(lb)
+        r.ub[:] = list(ub)
+        n_miss = 0
+        if x_miss is not None:
+            xm, ym = _f64(x_miss), _f64(y_miss)
+            r.n_miss, r.x_miss, r.y_miss = len(xm), _dptr(xm), _dptr(ym)
+            n_miss = len(xm)
+        t = ctypes.c_longlong()
+        _check(self._lib.egs_server_submit(self._h, ctypes.byref(r), ctypes.byref(t)), "egs_server_submit")
+        self._keep[t.value] = n_miss
+        return t.value
+
+    def wait(self, ticket: int):
+        """(Result, predictions or None); raises nothing: the status is in the result."""
+        n_miss = self._keep.pop(ticket)
+        res = Result()
+        out = np.zeros(max(n_miss, 1))
+        _check(self._lib.egs_server_wait(self._h, int(ticket), ctypes.byref(res), _dptr(out)), "egs_server_wait")
+        return res, (out[:n_miss] if n_miss else None)
+
+    def stats(self) -> dict:
+        q, a, pa = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        r, pr, c, e = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+        _check(self._lib.egs_server_stats(self._h, ctypes.byref(q), ctypes.byref(a), ctypes.byref(r),
+                                          ctypes.byref(pa), ctypes.byref(pr), ctypes.byref(c), ctypes.byref(e)),
+               "egs_server_stats")
+        return {"queued": q.value, "active": a.value, "reserved": r.value, "peak_active": pa.value,
+                "peak_reserved": pr.value, "completed": c.value, "evals": e.value}
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.egs_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -167,13 +167,17 @@ void collect_spans(egs_problem* p) {
   p->events_used = 0;
 }
 
+// Device buffers come from the stream-ordered allocator on the owning
+// problem's stream: neither the allocation nor the release synchronises the
+// device, so problems can be created and destroyed while other problems'
+// work is running (the serving loop relies on this).
 template <typename T>
-int dev_alloc(T** p, size_t count, long long* bytes) {
+int dev_alloc(T** p, size_t count, long long* bytes, cudaStream_t st) {
   const size_t b = count * sizeof(T);
-  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), b);
+  cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(p), b, st);
   if (e != cudaSuccess) {
     cudaGetLastError();
-    set_last_error(cudaGetErrorString(e), "cudaMalloc");
+    set_last_error(cudaGetErrorString(e), "cudaMallocAsync");
     *p = nullptr;
     return e == cudaErrorMemoryAllocation ? EGS_ERR_OOM : EGS_ERR_CUDA;
   }
@@ -181,10 +185,43 @@ int dev_alloc(T** p, size_t count, long long* bytes) {
   return EGS_OK;
 }
 
+void dev_free(void* ptr, cudaStream_t st) {
+  if (ptr) cudaFreeAsync(ptr, st);
+}
+
+// Small pinned host records (parameter block, result record, status words) are
+// 256-byte chunks of slabs that live until the process exits: cudaFreeHost
+// would synchronise the device.
+constexpr size_t kPinnedChunk = 256;
+constexpr size_t kPinnedSlabChunks = 256;
+std::mutex g_pinned_mutex;
+std::vector<void*> g_pinned_free;
+
+void* pinned_record() {
+  std::lock_guard<std::mutex> lock(g_pinned_mutex);
+  if (g_pinned_free.empty()) {
+    void* slab = nullptr;
+    if (cudaMallocHost(&slab, kPinnedChunk * kPinnedSlabChunks) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    for (size_t i = 0; i < kPinnedSlabChunks; ++i) g_pinned_free.push_back(static_cast<char*>(slab) + i * kPinnedChunk);
+  }
+  void* r = g_pinned_free.back();
+  g_pinned_free.pop_back();
+  return r;
+}
+
+void pinned_release(void* r) {
+  if (!r) return;
+  std::lock_guard<std::mutex> lock(g_pinned_mutex);
+  g_pinned_free.push_back(r);
+}
+
 void free_mixed(egs_problem* p) {
   void* bufs[] = {p->band_pool, p->off_pool, p->W, p->ph, p->pl, p->inv_scale, p->w, p->res_scratch,
                   p->gen_tiles, p->band_jobs, p->band_begin, p->inv_pool, p->solve_tmp};
-  for (void* b : bufs) cudaFree(b);
+  for (void* b : bufs) dev_free(b, p->stream);
   p->band_pool = nullptr;
   p->off_pool = nullptr;
   p->W = nullptr;
@@ -202,22 +239,15 @@ void free_mixed(egs_problem* p) {
 void free_problem(egs_problem* p) {
   if (!p) return;
   if (p->stream) cudaStreamSynchronize(p->stream);
-  cudaFree(p->tiles);
-  cudaFree(p->x);
-  cudaFree(p->y);
-  cudaFree(p->z);
-  cudaFree(p->zcpy);
-  cudaFree(p->partial);
-  cudaFree(p->result);
-  cudaFree(p->flags);
-  cudaFree(p->dparams);
-  cudaFree(p->ktab);
+  void* bufs[] = {p->tiles, p->x, p->y, p->z, p->zcpy, p->partial, p->result, p->flags, p->dparams, p->ktab};
+  for (void* b : bufs) dev_free(b, p->stream);
   free_mixed(p);
-  cudaFreeHost(p->hparams);
-  cudaFreeHost(p->hresult);
-  cudaFreeHost(p->hflags);
+  pinned_release(p->hparams);
+  pinned_release(p->hresult);
+  pinned_release(p->hflags);
   if (p->graph_exec) cudaGraphExecDestroy(p->graph_exec);
   if (p->graph) cudaGraphDestroy(p->graph);
+  if (p->stream) cudaStreamSynchronize(p->stream);
   if (p->own_stream && p->stream) cudaStreamDestroy(p->stream);
   for (cudaEvent_t e : p->events) cudaEventDestroy(e);
   delete p;
@@ -565,12 +595,8 @@ int enqueue_eval_mixed(egs_problem* p) {
 // job tables.
 int setup_mixed(egs_problem* p, int b) {
   free_mixed(p);
-  cudaFree(p->tiles);
-  cudaFree(p->x);
-  cudaFree(p->y);
-  cudaFree(p->z);
-  cudaFree(p->zcpy);
-  cudaFree(p->partial);
+  for (void* buf : {(void*)p->tiles, (void*)p->x, (void*)p->y, (void*)p->z, (void*)p->zcpy, (void*)p->partial})
+    dev_free(buf, p->stream);
   p->tiles = p->x = p->y = p->z = p->zcpy = p->partial = nullptr;
   p->bytes = (long long)(sizeof(MaternParams) + kKtabDoubles * sizeof(double) + 2 * sizeof(int) + 4 * sizeof(double));
   const int ts = ((std::max(p->dts, 256) + 255) / 256) * 256;
@@ -583,16 +609,18 @@ int setup_mixed(egs_problem* p, int b) {
   const int m = std::max(0, nt - b - 1);
   const size_t ts2 = (size_t)ts * ts;
   int rc = EGS_OK;
-  if ((rc = dev_alloc(&p->x, p->np, &p->bytes)) || (rc = dev_alloc(&p->y, p->np, &p->bytes)) ||
-      (rc = dev_alloc(&p->z, p->np, &p->bytes)) || (rc = dev_alloc(&p->zcpy, p->np, &p->bytes)) ||
-      (rc = dev_alloc(&p->partial, p->nt, &p->bytes)) ||
-      (rc = dev_alloc(&p->band_pool, (size_t)nt * (b + 1) * ts2, &p->bytes)) ||
-      (rc = dev_alloc(&p->off_pool, std::max<size_t>(1, (size_t)lower_tiles(m) * ts2), &p->bytes)) ||
-      (rc = dev_alloc(&p->W, (size_t)(nt + 1) * ts2, &p->bytes)) ||
-      (rc = dev_alloc(&p->inv_pool, (size_t)nt * ts2, &p->bytes)) || (rc = dev_alloc(&p->solve_tmp, ts, &p->bytes)) || (rc = dev_alloc(&p->ph, (size_t)p->np * ts, &p->bytes)) ||
-      (rc = dev_alloc(&p->pl, (size_t)p->np * ts, &p->bytes)) ||
-      (rc = dev_alloc(&p->inv_scale, (size_t)p->np, &p->bytes)) || (rc = dev_alloc(&p->w, p->np, &p->bytes)) ||
-      (rc = dev_alloc(&p->res_scratch, (size_t)residual_scratch_doubles(p->n), &p->bytes)))
+  if ((rc = dev_alloc(&p->x, p->np, &p->bytes, p->stream)) || (rc = dev_alloc(&p->y, p->np, &p->bytes, p->stream)) ||
+      (rc = dev_alloc(&p->z, p->np, &p->bytes, p->stream)) || (rc = dev_alloc(&p->zcpy, p->np, &p->bytes, p->stream)) ||
+      (rc = dev_alloc(&p->partial, p->nt, &p->bytes, p->stream)) ||
+      (rc = dev_alloc(&p->band_pool, (size_t)nt * (b + 1) * ts2, &p->bytes, p->stream)) ||
+      (rc = dev_alloc(&p->off_pool, std::max<size_t>(1, (size_t)lower_tiles(m) * ts2), &p->bytes, p->stream)) ||
+      (rc = dev_alloc(&p->W, (size_t)(nt + 1) * ts2, &p->bytes, p->stream)) ||
+      (rc = dev_alloc(&p->inv_pool, (size_t)nt * ts2, &p->bytes, p->stream)) ||
+      (rc = dev_alloc(&p->solve_tmp, ts, &p->bytes, p->stream)) ||
+      (rc = dev_alloc(&p->ph, (size_t)p->np * ts, &p->bytes, p->stream)) ||
+      (rc = dev_alloc(&p->pl, (size_t)p->np * ts, &p->bytes, p->stream)) ||
+      (rc = dev_alloc(&p->inv_scale, (size_t)p->np, &p->bytes, p->stream)) || (rc = dev_alloc(&p->w, p->np, &p->bytes, p->stream)) ||
+      (rc = dev_alloc(&p->res_scratch, (size_t)residual_scratch_doubles(p->n), &p->bytes, p->stream)))
     return rc;
   std::vector<int4> gen;
   for (int j = 0; j < nt; ++j)
@@ -600,7 +628,7 @@ int setup_mixed(egs_problem* p, int b) {
       gen.push_back(i - j <= b ? make_int4(i, j, 0, (int)((long long)j * (b + 1) + (i - j)))
                                : make_int4(i, j, 1, (int)tile_slot(i - b - 1, j, m)));
   p->ngen = (long long)gen.size();
-  if ((rc = dev_alloc(&p->gen_tiles, gen.size(), &p->bytes))) return rc;
+  if ((rc = dev_alloc(&p->gen_tiles, gen.size(), &p->bytes, p->stream))) return rc;
   EGS_CUDA_TRY(cudaMemcpy(p->gen_tiles, gen.data(), gen.size() * sizeof(int4), cudaMemcpyHostToDevice));
   // FP64 band update of step k: one job per target tile column j > k, rows of
   // tiles j .. min(nt-1, j+b), all operands W-relative (W[t] = tile (k+t, k)).
@@ -634,8 +662,8 @@ int setup_mixed(egs_problem* p, int b) {
     L.total = acc;
     p->band_launch.push_back(L);
   }
-  if ((rc = dev_alloc(&p->band_jobs, std::max<size_t>(1, jobs.size()), &p->bytes)) ||
-      (rc = dev_alloc(&p->band_begin, std::max<size_t>(1, begin.size()), &p->bytes)))
+  if ((rc = dev_alloc(&p->band_jobs, std::max<size_t>(1, jobs.size()), &p->bytes, p->stream)) ||
+      (rc = dev_alloc(&p->band_begin, std::max<size_t>(1, begin.size()), &p->bytes, p->stream)))
     return rc;
   if (!jobs.empty())
     EGS_CUDA_TRY(cudaMemcpy(p->band_jobs, jobs.data(), jobs.size() * sizeof(GemmDesc), cudaMemcpyHostToDevice));
@@ -736,7 +764,7 @@ int egs_hardware_init(int device) {
   return EGS_OK;
 }
 
-int egs_problem_create(egs_problem** out, int n, int dts) {
+static int create_problem(egs_problem** out, int n, int dts, bool with_tiles) {
   if (!out || n <= 0 || dts <= 0) return EGS_ERR_INVALID;
   *out = nullptr;
   int count = 0;
@@ -752,27 +780,33 @@ int egs_problem_create(egs_problem** out, int n, int dts) {
   p->nt = (n + p->ts - 1) / p->ts;
   p->np = p->nt * p->ts;
   p->ntiles = lower_tiles(p->nt);
-  int rc = EGS_OK;
-  if ((rc = dev_alloc(&p->tiles, (size_t)p->ntiles * p->ts * p->ts, &p->bytes)) ||
-      (rc = dev_alloc(&p->x, p->np, &p->bytes)) || (rc = dev_alloc(&p->y, p->np, &p->bytes)) ||
-      (rc = dev_alloc(&p->z, p->np, &p->bytes)) || (rc = dev_alloc(&p->zcpy, p->np, &p->bytes)) ||
-      (rc = dev_alloc(&p->partial, p->nt, &p->bytes)) || (rc = dev_alloc(&p->result, 4, &p->bytes)) ||
-      (rc = dev_alloc(&p->flags, 2, &p->bytes)) || (rc = dev_alloc(&p->dparams, 1, &p->bytes)) ||
-      (rc = dev_alloc(&p->ktab, kKtabDoubles, &p->bytes))) {
-    free_problem(p);
-    return rc;
-  }
-  if (cudaMallocHost(&p->hparams, sizeof(MaternParams)) != cudaSuccess ||
-      cudaMallocHost(&p->hresult, 4 * sizeof(double)) != cudaSuccess ||
-      cudaMallocHost(&p->hflags, 2 * sizeof(int)) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess) {
     cudaGetLastError();
-    set_last_error("pinned host allocation or stream creation failed", "egs_problem_create");
-    free_problem(p);
+    set_last_error("stream creation failed", "egs_problem_create");
+    delete p;
     return EGS_ERR_CUDA;
   }
   p->own_stream = true;
-  if ((rc = gemm_init_tensor_map(p->tmap, p->tiles, p->ts, p->ntiles)) != EGS_OK) {
+  int rc = EGS_OK;
+  if ((with_tiles && (rc = dev_alloc(&p->tiles, (size_t)p->ntiles * p->ts * p->ts, &p->bytes, p->stream))) ||
+      (rc = dev_alloc(&p->x, p->np, &p->bytes, p->stream)) || (rc = dev_alloc(&p->y, p->np, &p->bytes, p->stream)) ||
+      (rc = dev_alloc(&p->z, p->np, &p->bytes, p->stream)) || (rc = dev_alloc(&p->zcpy, p->np, &p->bytes, p->stream)) ||
+      (rc = dev_alloc(&p->partial, p->nt, &p->bytes, p->stream)) ||
+      (rc = dev_alloc(&p->result, 4, &p->bytes, p->stream)) || (rc = dev_alloc(&p->flags, 2, &p->bytes, p->stream)) ||
+      (rc = dev_alloc(&p->dparams, 1, &p->bytes, p->stream)) ||
+      (rc = dev_alloc(&p->ktab, kKtabDoubles, &p->bytes, p->stream))) {
+    free_problem(p);
+    return rc;
+  }
+  p->hparams = static_cast<MaternParams*>(pinned_record());
+  p->hresult = static_cast<double*>(pinned_record());
+  p->hflags = static_cast<int*>(pinned_record());
+  if (!p->hparams || !p->hresult || !p->hflags) {
+    set_last_error("pinned host allocation failed", "egs_problem_create");
+    free_problem(p);
+    return EGS_ERR_CUDA;
+  }
+  if (with_tiles && (rc = gemm_init_tensor_map(p->tmap, p->tiles, p->ts, p->ntiles)) != EGS_OK) {
     free_problem(p);
     return rc;
   }
@@ -785,6 +819,24 @@ int egs_problem_create(egs_problem** out, int n, int dts) {
     cudaGetLastError();
     free_problem(p);
     return EGS_ERR_CUDA;
+  }
+  *out = p;
+  return EGS_OK;
+}
+
+int egs_problem_create(egs_problem** out, int n, int dts) { return create_problem(out, n, dts, true); }
+
+int egs_problem_create_ex(egs_problem** out, int n, int dts, int precision, int band_tiles) {
+  if (!out) return EGS_ERR_INVALID;
+  *out = nullptr;
+  if (precision == EGS_PRECISION_DOUBLE) return create_problem(out, n, dts, true);
+  if (precision != EGS_PRECISION_MIXED || band_tiles < 0) return EGS_ERR_INVALID;
+  egs_problem* p = nullptr;
+  int rc = create_problem(&p, n, dts, false);  // the mixed layout replaces the FP64 tile storage
+  if (rc != EGS_OK) return rc;
+  if ((rc = egs_problem_set_precision(p, precision, band_tiles)) != EGS_OK) {
+    free_problem(p);
+    return rc;
   }
   *out = p;
   return EGS_OK;
@@ -1026,13 +1078,13 @@ int egs_generate_observations(egs_problem* p, const double* theta, int seed, dou
   if ((rc = egs_potrf(p)) != EGS_OK) return rc;
   double* part = nullptr;
   long long dummy = 0;
-  if ((rc = dev_alloc(&part, (size_t)p->ntiles * p->ts, &dummy)) != EGS_OK) return rc;
+  if ((rc = dev_alloc(&part, (size_t)p->ntiles * p->ts, &dummy, p->stream)) != EGS_OK) return rc;
   launch_trmv(p->tiles, p->ts, p->nt, p->z, part, p->zcpy, p->stream);
   cudaMemcpyAsync(p->z, p->zcpy, p->np * sizeof(double), cudaMemcpyDeviceToDevice, p->stream);
   if (z_out) cudaMemcpyAsync(z_out, p->zcpy, p->n * sizeof(double), cudaMemcpyDeviceToHost, p->stream);
   rc = check_cuda("egs_generate_observations");
+  dev_free(part, p->stream);
   cudaStreamSynchronize(p->stream);
-  cudaFree(part);
   if (rc != EGS_OK) return rc;
   p->have_observations = true;
   return EGS_OK;
@@ -1290,17 +1342,13 @@ int egs_predict_host(int n_obs, int n_miss, int dts, const double* x_obs, const 
   double *c12t = nullptr, *dxm = nullptr, *dym = nullptr, *dzm = nullptr, *dza = nullptr, *dsum = nullptr;
   long long dummy = 0;
   auto cleanup = [&]() {
+    for (void* b : {(void*)c12t, (void*)dxm, (void*)dym, (void*)dzm, (void*)dza, (void*)dsum}) dev_free(b, p->stream);
     cudaStreamSynchronize(p->stream);
-    cudaFree(c12t);
-    cudaFree(dxm);
-    cudaFree(dym);
-    cudaFree(dzm);
-    cudaFree(dza);
-    cudaFree(dsum);
   };
-  if ((rc = dev_alloc(&c12t, (size_t)n_obs * n_miss, &dummy)) || (rc = dev_alloc(&dxm, n_miss, &dummy)) ||
-      (rc = dev_alloc(&dym, n_miss, &dummy)) || (rc = dev_alloc(&dzm, n_miss, &dummy)) ||
-      (rc = dev_alloc(&dza, n_miss, &dummy)) || (rc = dev_alloc(&dsum, 1, &dummy))) {
+  cudaStream_t ps = p->stream;
+  if ((rc = dev_alloc(&c12t, (size_t)n_obs * n_miss, &dummy, ps)) || (rc = dev_alloc(&dxm, n_miss, &dummy, ps)) ||
+      (rc = dev_alloc(&dym, n_miss, &dummy, ps)) || (rc = dev_alloc(&dzm, n_miss, &dummy, ps)) ||
+      (rc = dev_alloc(&dza, n_miss, &dummy, ps)) || (rc = dev_alloc(&dsum, 1, &dummy, ps))) {
     cleanup();
     return rc;
   }
@@ -1335,3 +1383,76 @@ int egs_predict_host(int n_obs, int n_miss, int dts, const double* x_obs, const 
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Footprint and prediction on a resident problem (used by the serving loop)
+// ---------------------------------------------------------------------------
+
+int egs_problem_footprint(int n, int dts, int precision, int band_tiles, long long* bytes) {
+  if (n <= 0 || dts <= 0 || !bytes || band_tiles < 0) return EGS_ERR_INVALID;
+  const long long small = (long long)(sizeof(MaternParams) + kKtabDoubles * sizeof(double) + 4 * sizeof(double) +
+                                      2 * sizeof(int));
+  long long b = 0;
+  if (precision == EGS_PRECISION_DOUBLE) {
+    const long long ts = round_tile(dts), nt = (n + ts - 1) / ts, np = nt * ts;
+    b = lower_tiles((int)nt) * ts * ts * 8 + 4 * np * 8 + nt * 8 + small;
+  } else if (precision == EGS_PRECISION_MIXED) {
+    const long long ts = ((std::max(dts, 256) + 255) / 256) * 256, nt = (n + ts - 1) / ts, np = nt * ts;
+    const long long m = std::max<long long>(0, nt - band_tiles - 1);
+    b = 4 * np * 8 + nt * 8 + small;                                // x, y, z, zcpy, partial
+    b += nt * (band_tiles + 1) * ts * ts * 8;                       // FP64 band
+    b += std::max<long long>(1, lower_tiles((int)m)) * ts * ts * 4; // FP32 off-band
+    b += (nt + 1) * ts * ts * 8 + nt * ts * ts * 8 + ts * 8;        // W, inverses, solve temp
+    b += 2 * np * ts * 2 + np * 4 + np * 8;                         // FP16 split, row scales, w
+    b += residual_scratch_doubles(n) * 8 + lower_tiles((int)nt) * (long long)sizeof(int4);
+    b += (nt * nt / 2 + nt + 1) * ((long long)sizeof(GemmDesc) + 8);
+  } else {
+    return EGS_ERR_INVALID;
+  }
+  // allocator granularity: every buffer rounds up to 2 MiB in the worst case
+  *bytes = b + 32ll * (2ll << 20);
+  return EGS_OK;
+}
+
+int egs_problem_predict(egs_problem* p, const double* theta, int n_miss, const double* x_miss, const double* y_miss,
+                        double* z_miss) {
+  if (!p || !theta || n_miss <= 0 || !x_miss || !y_miss || !z_miss) return EGS_ERR_INVALID;
+  if (p->precision == kPrecisionBroken) return EGS_ERR_STATE;
+  if (!p->have_locations || !p->have_observations) {
+    set_last_error("locations and observations must be set", "egs_problem_predict");
+    return EGS_ERR_STATE;
+  }
+  int rc = EGS_OK;
+  if (p->precision == EGS_PRECISION_MIXED) {
+    // the mixed evaluation leaves (L L^T)^-1 z in z and the refinement
+    // correction in w: the kriging weights are their sum
+    double ll = 0.0;
+    if ((rc = egs_mle_eval(p, theta, &ll, nullptr, nullptr)) != EGS_OK) return rc;
+    launch_add_inplace(p->z, p->w, p->n, p->stream);
+  } else {
+    if ((rc = egs_covariance_generate(p, theta)) != EGS_OK) return rc;
+    if ((rc = egs_potrf(p)) != EGS_OK) return rc;
+    if ((rc = egs_restore_observations(p)) != EGS_OK) return rc;
+    enqueue_trsv(p);
+    enqueue_trsv_t(p);
+  }
+  cudaStream_t st = p->stream;
+  double *c12t = nullptr, *dxm = nullptr, *dym = nullptr, *dzm = nullptr;
+  long long dummy = 0;
+  if ((rc = dev_alloc(&c12t, (size_t)p->n * n_miss, &dummy, st)) || (rc = dev_alloc(&dxm, n_miss, &dummy, st)) ||
+      (rc = dev_alloc(&dym, n_miss, &dummy, st)) || (rc = dev_alloc(&dzm, n_miss, &dummy, st))) {
+    for (void* b : {(void*)c12t, (void*)dxm, (void*)dym, (void*)dzm}) dev_free(b, st);
+    return rc;
+  }
+  cudaMemcpyAsync(dxm, x_miss, n_miss * sizeof(double), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(dym, y_miss, n_miss * sizeof(double), cudaMemcpyHostToDevice, st);
+  MaternParams mp;
+  make_matern_params(theta, &mp);
+  launch_matern_block(c12t, p->n, p->n, n_miss, p->x, p->y, dxm, dym, mp, st);
+  launch_gemv_t_block(c12t, p->n, p->n, n_miss, p->z, dzm, st);
+  cudaMemcpyAsync(z_miss, dzm, n_miss * sizeof(double), cudaMemcpyDeviceToHost, st);
+  rc = check_cuda("egs_problem_predict");
+  for (void* b : {(void*)c12t, (void*)dxm, (void*)dym, (void*)dzm}) dev_free(b, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess && rc == EGS_OK) rc = check_cuda("egs_problem_predict/sync");
+  return rc;
+}

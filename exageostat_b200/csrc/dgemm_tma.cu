@@ -349,21 +349,24 @@ dgemm_update_kernel(const __grid_constant__ CUtensorMap tmap, double* __restrict
   }
 }
 
-static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
-
+// One-time lookups below use function-local statics, whose initialisation is
+// thread-safe: problems may be created from several host threads at once.
 int tensor_map_encoder(void** fn_out) {
-  if (!g_encode) {
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = []() -> PFN_cuTensorMapEncodeTiled_v12000 {
     cudaDriverEntryPointQueryResult q;
-    void* fn = nullptr;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
-        q != cudaDriverEntryPointSuccess || !fn) {
+    void* f = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !f) {
       cudaGetLastError();
-      set_last_error("cuTensorMapEncodeTiled unavailable", "tensor_map_encoder");
-      return EGS_ERR_CUDA;
+      return nullptr;
     }
-    g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  }();
+  if (!fn) {
+    set_last_error("cuTensorMapEncodeTiled unavailable", "tensor_map_encoder");
+    return EGS_ERR_CUDA;
   }
-  *fn_out = reinterpret_cast<void*>(g_encode);
+  *fn_out = reinterpret_cast<void*>(fn);
   return EGS_OK;
 }
 
@@ -375,7 +378,8 @@ int gemm_init_tensor_map(void* tmap_storage, double* tiles, int ts, long long nt
   cuuint64_t strides[2] = {(cuuint64_t)ts * 8, (cuuint64_t)ts * ts * 8};
   cuuint32_t box[3] = {gemm::BOX_ROWS, gemm::BK, 1};
   cuuint32_t estr[3] = {1, 1, 1};
-  CUresult r = g_encode(reinterpret_cast<CUtensorMap*>(tmap_storage), CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, tiles,
+  auto encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  CUresult r = encode(reinterpret_cast<CUtensorMap*>(tmap_storage), CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, tiles,
                         dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
@@ -385,24 +389,23 @@ int gemm_init_tensor_map(void* tmap_storage, double* tiles, int ts, long long nt
   return EGS_OK;
 }
 
-static int g_num_sms = 0;
 int gemm_num_sms() {
-  if (g_num_sms == 0) {
-    int dev = 0;
+  static const int sms = []() {
+    int dev = 0, n = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
-    if (g_num_sms <= 0) g_num_sms = 148;
-  }
-  return g_num_sms;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n > 0 ? n : 148;
+  }();
+  return sms;
 }
 
 static void set_gemm_smem_attributes() {
-  static bool attr_set = false;
-  if (!attr_set) {
+  static const bool attr_set = []() {
     cudaFuncSetAttribute(dgemm_update_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, gemm::SMEM_BYTES);
     cudaFuncSetAttribute(dgemm_update_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, gemm::SMEM_BYTES);
-    attr_set = true;
-  }
+    return true;
+  }();
+  (void)attr_set;
 }
 
 void finish_desc(GemmDesc& d) {

@@ -1,0 +1,271 @@
+// Serving loop of the B200 path: a request queue with admission by HBM
+// footprint and concurrent execution of admitted requests on one GPU.
+//
+// The reference answers one request per process: ExaGeoStat<T>::
+// ExaGeoStatDataModeling (src/api/ExaGeoStat.cpp:46-95) fits theta with NLopt
+// over a StarPU/Chameleon factorisation, ExaGeoStatPrediction (:97-120) krigs.
+// Here a long-lived server takes many such requests of different N:
+//   * submission copies the request's arrays and computes its footprint
+//     (egs_problem_footprint), refusing requests larger than the budget;
+//   * max_active worker threads, each with its own problem and CUDA stream,
+//     take the oldest queued request whose footprint fits the remaining
+//     budget (a request that has waited more than kStarveMs blocks younger
+//     ones until it fits);
+//   * a worker creates the request's problem (stream-ordered device memory,
+//     no device-wide synchronisation), uploads locations and observations
+//     once, and runs the request with everything resident: a fit drives the
+//     BOBYQA maximiser with one device evaluation per objective call, reusing
+//     the problem (and its captured evaluation graph) across iterations;
+//   * work of different requests overlaps on the device; every kernel's
+//     reduction order is fixed, so a request's result does not depend on what
+//     else runs.
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+#include <cuda_runtime.h>
+#include "exageostat_b200.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+constexpr double kStarveMs = 3000.0;
+
+double ms_between(Clock::time_point a, Clock::time_point b) {
+  return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+struct Request {
+  long long ticket = 0;
+  egs_request r{};
+  std::vector<double> x, y, z, xm, ym, zm;
+  long long footprint = 0;
+  Clock::time_point submitted, admitted;
+  egs_result res{};
+  bool done = false;
+};
+
+struct FitCtx {
+  egs_problem* p;
+  int status;
+  int evals;
+};
+
+double fit_objective(int, const double* theta, void* ctx) {
+  auto* c = static_cast<FitCtx*>(ctx);
+  double ll = 0.0;
+  const int rc = egs_mle_eval(c->p, theta, &ll, nullptr, nullptr);
+  ++c->evals;
+  if (rc != EGS_OK) {
+    // the reference's objective throws on a non-SPD matrix and the fit stops;
+    // here the point is rejected and the search goes on
+    if (c->status == EGS_OK) c->status = rc;
+    return -1e300;
+  }
+  return ll;
+}
+
+}  // namespace
+
+struct egs_server {
+  int device = 0;
+  long long budget = 0;
+  int max_active = 1;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<Request*> queue;
+  std::unordered_map<long long, std::unique_ptr<Request>> all;
+  long long next_ticket = 1;
+  long long reserved = 0, peak_reserved = 0, completed = 0, evals = 0;
+  int active = 0, peak_active = 0;
+  bool stopping = false;
+  std::vector<std::thread> workers;
+
+  // Oldest queued request that fits; the head, once starved, blocks the others.
+  Request* pick_locked() {
+    const auto now = Clock::now();
+    for (size_t i = 0; i < queue.size(); ++i) {
+      Request* q = queue[i];
+      if (reserved + q->footprint <= budget) {
+        queue.erase(queue.begin() + (long)i);
+        return q;
+      }
+      if (i == 0 && ms_between(q->submitted, now) > kStarveMs) return nullptr;
+    }
+    return nullptr;
+  }
+
+  void run(Request* q) {
+    egs_result& out = q->res;
+    out.kind = q->r.kind;
+    std::memcpy(out.theta, q->r.theta, sizeof(out.theta));
+    egs_problem* p = nullptr;
+    int rc = egs_problem_create_ex(&p, q->r.n, q->r.dts, q->r.precision, q->r.band_tiles);
+    if (rc == EGS_OK) rc = egs_problem_set_locations(p, q->x.data(), q->y.data());
+    if (rc == EGS_OK) rc = egs_problem_set_observations(p, q->z.data());
+    if (rc == EGS_OK) {
+      if (q->r.kind == EGS_REQ_LOGLIK) {
+        rc = egs_mle_eval(p, q->r.theta, &out.loglik, nullptr, nullptr);
+        out.evals = 1;
+      } else if (q->r.kind == EGS_REQ_FIT) {
+        FitCtx ctx{p, EGS_OK, 0};
+        double th[3];
+        std::memcpy(th, q->r.lb, sizeof(th));
+        double best = 0.0;
+        int nev = 0;
+        rc = egs_bobyqa_maximize(3, th, q->r.lb, q->r.ub, 0.0, q->r.ftol_abs, q->r.max_evals, fit_objective, &ctx,
+                                 &best, &nev);
+        if (rc == EGS_OK && ctx.status != EGS_OK && !(best > -1e299)) rc = ctx.status;
+        out.loglik = best;
+        std::memcpy(out.theta, th, sizeof(th));
+        out.evals = ctx.evals;
+      } else {
+        q->zm.assign(q->r.n_miss, 0.0);
+        rc = egs_problem_predict(p, q->r.theta, q->r.n_miss, q->xm.data(), q->ym.data(), q->zm.data());
+        out.evals = 1;
+      }
+    }
+    if (p) egs_problem_destroy(p);
+    out.status = rc;
+  }
+
+  void worker_main() {
+    cudaSetDevice(device);
+    for (;;) {
+      Request* q = nullptr;
+      {
+        std::unique_lock<std::mutex> lock(mu);
+        cv_work.wait(lock, [&] {
+          if (stopping && queue.empty()) return true;
+          q = pick_locked();
+          return q != nullptr;
+        });
+        if (!q) return;  // stopping with nothing left
+        reserved += q->footprint;
+        ++active;
+        if (reserved > peak_reserved) peak_reserved = reserved;
+        if (active > peak_active) peak_active = active;
+        q->admitted = Clock::now();
+      }
+      run(q);
+      const auto t = Clock::now();
+      {
+        std::lock_guard<std::mutex> lock(mu);
+        reserved -= q->footprint;
+        --active;
+        ++completed;
+        evals += q->res.evals;
+        q->res.queue_ms = ms_between(q->submitted, q->admitted);
+        q->res.latency_ms = ms_between(q->submitted, t);
+        q->res.footprint = q->footprint;
+        q->done = true;
+      }
+      cv_done.notify_all();
+      cv_work.notify_all();  // memory and a slot are free again
+    }
+  }
+};
+
+extern "C" {
+
+int egs_server_create(egs_server** out, int device, long long hbm_budget, int max_active) {
+  if (!out || hbm_budget <= 0 || max_active <= 0 || max_active > 64) return EGS_ERR_INVALID;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count <= device || device < 0) {
+    cudaGetLastError();
+    return EGS_ERR_NO_DEVICE;
+  }
+  auto* s = new egs_server();
+  s->device = device;
+  s->budget = hbm_budget;
+  s->max_active = max_active;
+  for (int i = 0; i < max_active; ++i) s->workers.emplace_back([s] { s->worker_main(); });
+  *out = s;
+  return EGS_OK;
+}
+
+int egs_server_submit(egs_server* s, const egs_request* r, long long* ticket) {
+  if (!s || !r || !ticket || r->n <= 0 || r->dts <= 0 || !r->x || !r->y || !r->z) return EGS_ERR_INVALID;
+  if (r->kind != EGS_REQ_LOGLIK && r->kind != EGS_REQ_FIT && r->kind != EGS_REQ_PREDICT) return EGS_ERR_INVALID;
+  if (r->kind == EGS_REQ_FIT && r->max_evals <= 0) return EGS_ERR_INVALID;
+  if (r->kind == EGS_REQ_PREDICT && (r->n_miss <= 0 || !r->x_miss || !r->y_miss)) return EGS_ERR_INVALID;
+  long long fp = 0;
+  int rc = egs_problem_footprint(r->n, r->dts, r->precision, r->band_tiles, &fp);
+  if (rc != EGS_OK) return rc;
+  if (r->kind == EGS_REQ_PREDICT) fp += ((long long)r->n * r->n_miss + 4ll * r->n_miss) * 8;
+  if (fp > s->budget) return EGS_ERR_OOM;
+  auto q = std::make_unique<Request>();
+  q->r = *r;
+  q->x.assign(r->x, r->x + r->n);
+  q->y.assign(r->y, r->y + r->n);
+  q->z.assign(r->z, r->z + r->n);
+  if (r->kind == EGS_REQ_PREDICT) {
+    q->xm.assign(r->x_miss, r->x_miss + r->n_miss);
+    q->ym.assign(r->y_miss, r->y_miss + r->n_miss);
+  }
+  q->r.x = q->r.y = q->r.z = q->r.x_miss = q->r.y_miss = nullptr;
+  q->footprint = fp;
+  q->submitted = Clock::now();
+  {
+    std::lock_guard<std::mutex> lock(s->mu);
+    if (s->stopping) return EGS_ERR_STATE;
+    q->ticket = s->next_ticket++;
+    *ticket = q->ticket;
+    s->queue.push_back(q.get());
+    s->all.emplace(q->ticket, std::move(q));
+  }
+  s->cv_work.notify_all();
+  return EGS_OK;
+}
+
+int egs_server_wait(egs_server* s, long long ticket, egs_result* out, double* z_miss) {
+  if (!s || !out) return EGS_ERR_INVALID;
+  std::unique_ptr<Request> q;
+  {
+    std::unique_lock<std::mutex> lock(s->mu);
+    auto it = s->all.find(ticket);
+    if (it == s->all.end()) return EGS_ERR_INVALID;
+    Request* raw = it->second.get();
+    s->cv_done.wait(lock, [&] { return raw->done; });
+    q = std::move(it->second);
+    s->all.erase(it);
+  }
+  *out = q->res;
+  if (z_miss && q->r.kind == EGS_REQ_PREDICT && !q->zm.empty())
+    std::memcpy(z_miss, q->zm.data(), q->zm.size() * sizeof(double));
+  return EGS_OK;
+}
+
+int egs_server_stats(egs_server* s, int* queued, int* active, long long* reserved, int* peak_active,
+                     long long* peak_reserved, long long* completed, long long* evals) {
+  if (!s) return EGS_ERR_INVALID;
+  std::lock_guard<std::mutex> lock(s->mu);
+  if (queued) *queued = (int)s->queue.size();
+  if (active) *active = s->active;
+  if (reserved) *reserved = s->reserved;
+  if (peak_active) *peak_active = s->peak_active;
+  if (peak_reserved) *peak_reserved = s->peak_reserved;
+  if (completed) *completed = s->completed;
+  if (evals) *evals = s->evals;
+  return EGS_OK;
+}
+
+int egs_server_destroy(egs_server* s) {
+  if (!s) return EGS_ERR_INVALID;
+  {
+    std::lock_guard<std::mutex> lock(s->mu);
+    s->stopping = true;
+  }
+  s->cv_work.notify_all();
+  for (auto& t : s->workers) t.join();
+  delete s;
+  return EGS_OK;
+}
+
+}  // extern "C"

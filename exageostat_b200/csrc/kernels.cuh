@@ -87,6 +87,7 @@ void launch_logdet_band(const double* band, int ts, int nt, int b, int n, double
 void launch_mixed_solve(const double* band, const float* off, const double* inv, int ts, int nt, int b, double* v,
                         double* tmp, cudaStream_t st, long long* launches);
 long long residual_scratch_doubles(int n);
+void launch_add_inplace(double* a, const double* b, int n, cudaStream_t st);
 void launch_matern_residual(const double* x, const double* y, const double* z, const double* v, int n, int np,
                             const MaternParams* params, const double* ktab, double* scratch, double* r,
                             cudaStream_t st);

@@ -213,6 +213,15 @@ inv_apply_kernel(const double* __restrict__ X, int ts, const double* __restrict_
   if (g == 0 && i < ts) out[i] = ((red[0][rl] + red[1][rl]) + red[2][rl]) + red[3][rl];
 }
 
+__global__ void add_inplace_kernel(double* __restrict__ a, const double* __restrict__ b, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] += b[i];
+}
+
+void launch_add_inplace(double* a, const double* b, int n, cudaStream_t st) {
+  add_inplace_kernel<<<(n + 255) / 256, 256, 0, st>>>(a, b, n);
+}
+
 __global__ void copy_segment_kernel(const double* __restrict__ src, double* __restrict__ dst, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) dst[i] = src[i];

@@ -514,11 +514,11 @@ int launch_split_update(const void* tm_hi, const void* tm_lo, const void* tm_c, 
   if (ts % BN != 0) return EGS_ERR_INVALID;
   const long long targets = split_targets(nt, band, k);
   if (targets == 0) return EGS_OK;
-  static bool attr = false;
-  if (!attr) {
+  static const bool attr = []() {
     cudaFuncSetAttribute(split_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-    attr = true;
-  }
+    return true;
+  }();
+  (void)attr;
   SplitStep P;
   P.ts = ts;
   P.nt = nt;

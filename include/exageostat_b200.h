@@ -91,6 +91,19 @@ EGS_API int egs_problem_set_band(egs_problem* p, int band);
  * dense path has no mixed implementation. */
 EGS_API int egs_problem_set_precision(egs_problem* p, int precision, int band_tiles);
 
+/* Create a problem directly in the given precision (EGS_PRECISION_DOUBLE or
+ * EGS_PRECISION_MIXED with band_tiles FP64 tile rows): the same as
+ * egs_problem_create followed by egs_problem_set_precision, without ever
+ * holding the FP64 tile storage of a mixed problem.  Replaces the descriptor
+ * set-up of LinearAlgebraMethods<T>::InitiateDescriptors for the precision the
+ * Configurations select (LinearAlgebraMethods.cpp:36-118, Definitions.hpp:258-262). */
+EGS_API int egs_problem_create_ex(egs_problem** out, int n, int dts, int precision, int band_tiles);
+
+/* Device bytes a problem of this shape holds (an upper bound of what
+ * egs_problem_info reports after creation), for admission by HBM footprint.
+ * Pure arithmetic: needs no device. */
+EGS_API int egs_problem_footprint(int n, int dts, int precision, int band_tiles, long long* bytes);
+
 /* Copy n locations from host memory (Locations<T> SoA x[], y[],
  * src/data-units/Locations.cpp:94-118). */
 EGS_API int egs_problem_set_locations(egs_problem* p, const double* x, const double* y);
@@ -174,7 +187,8 @@ EGS_API int egs_bobyqa_maximize(int n, double* x, const double* lb, const double
 #define EGS_STAGE_UPDATE 2     /* trailing syrk/gemm on the FP64 tensor path */
 #define EGS_STAGE_SOLVE 3      /* Z := L^-1 Z (and L^-T for kriging) */
 #define EGS_STAGE_REDUCE 4     /* log-det, dot, log-likelihood assembly */
-#define EGS_NUM_STAGES 5
+#define EGS_STAGE_UPDATE_LOW 5 /* mixed precision: off-band update on FP16 tensor cores (FP32-accurate) */
+#define EGS_NUM_STAGES 6
 
 /* Enable (1) or disable (0) CUDA-event timing of every stage on the problem's
  * stream; either call resets the counters.  Kernel launches are always counted. */
@@ -285,6 +299,15 @@ EGS_API int egs_matern_block(double* a, int lda, int rows, int cols, const doubl
 EGS_API int egs_mle_loglik_host(int n, int dts, const double* x, const double* y, const double* z,
                         const double* theta, double* loglik);
 
+/* Kriging on a resident problem of either precision: z_miss = C(miss, obs)
+ * C(obs, obs)^-1 z_obs at theta, for n_miss host target locations; the result
+ * goes to host memory.  The mixed form uses its refined solve.  The same
+ * computation as LinearAlgebraMethods<T>::ExaGeoStatMLEPredictTile
+ * (LinearAlgebraMethods.cpp:527-552) with the observed locations, observations
+ * and factor storage kept on the device between calls. */
+EGS_API int egs_problem_predict(egs_problem* p, const double* theta, int n_miss, const double* x_miss,
+                                const double* y_miss, double* z_miss);
+
 /* Kriging.  Replaces LinearAlgebraMethods<T>::ExaGeoStatMLEPredictTile
  * (src/linear-algebra-solvers/LinearAlgebraMethods.cpp:451-605):
  * C22 = C(obs, obs), w = C22^-1 z_obs (dposv), z_miss = C12 w, and
@@ -293,6 +316,75 @@ EGS_API int egs_mle_loglik_host(int n, int dts, const double* x, const double* y
 EGS_API int egs_predict_host(int n_obs, int n_miss, int dts, const double* x_obs, const double* y_obs,
                      const double* z_obs, const double* x_miss, const double* y_miss,
                      const double* z_actual, const double* theta, double* z_miss, double* mspe);
+
+/* ---- serving ------------------------------------------------------------ */
+
+/* A request loop on one GPU: likelihood, fit and predict requests of any N are
+ * queued, admitted while the sum of the admitted requests' HBM footprints
+ * (egs_problem_footprint) stays within a budget and fewer than max_active run,
+ * and executed concurrently, each on its own stream with its problem
+ * (locations, observations, factor storage) resident for the whole request --
+ * across every optimizer iteration of a fit.  Requests that arrive while others
+ * run are admitted as slots and memory free up; the oldest waiting request
+ * that fits goes first, and one that has waited longer than a few seconds
+ * blocks younger ones until it fits.  Results of a request do not depend on
+ * what else runs (all reductions have a fixed order).
+ * The reference runs one request per process (ExaGeoStat<T>::ExaGeoStatDataModeling
+ * / ExaGeoStatPrediction, src/api/ExaGeoStat.cpp:46-120); the request kinds map
+ * to those calls. */
+typedef struct egs_server egs_server;
+
+#define EGS_REQ_LOGLIK 1   /* log-likelihood at theta (one ExaGeoStatMLETile evaluation) */
+#define EGS_REQ_FIT 2      /* maximum-likelihood fit (ExaGeoStatDataModeling): BOBYQA from lb */
+#define EGS_REQ_PREDICT 3  /* kriging at n_miss targets with theta (ExaGeoStatPrediction) */
+
+typedef struct egs_request {
+  int kind;            /* EGS_REQ_* */
+  int n;               /* observed locations */
+  int dts;             /* tile size (the reference's --dts) */
+  int precision;       /* EGS_PRECISION_DOUBLE or EGS_PRECISION_MIXED */
+  int band_tiles;      /* FP64 band of a mixed request */
+  const double* x;     /* n locations and observations, copied at submission */
+  const double* y;
+  const double* z;
+  double theta[3];     /* LOGLIK, PREDICT: (sigma^2, beta, nu) */
+  double lb[3];        /* FIT: box bounds; the search starts at lb (Configurations.cpp:200) */
+  double ub[3];
+  double ftol_abs;     /* FIT: stop when an improvement is below this (10^-tol) */
+  int max_evals;       /* FIT: evaluation limit (--max_mle_iterations) */
+  int n_miss;          /* PREDICT: targets, copied at submission */
+  const double* x_miss;
+  const double* y_miss;
+} egs_request;
+
+typedef struct egs_result {
+  int status;          /* EGS_OK, a potrf info (> 0) or an EGS_ERR_* code of this request */
+  int kind;
+  double loglik;       /* LOGLIK: value at theta; FIT: best value; PREDICT: unused */
+  double theta[3];     /* FIT: fitted parameters; otherwise the request's theta */
+  int evals;           /* device log-likelihood evaluations made for the request */
+  double queue_ms;     /* submission -> admission */
+  double latency_ms;   /* submission -> completion */
+  long long footprint; /* HBM bytes reserved at admission */
+} egs_result;
+
+/* Start a server on `device` with hbm_budget bytes of admission budget and at
+ * most max_active concurrently running requests (one host worker thread and
+ * one stream each). */
+EGS_API int egs_server_create(egs_server** out, int device, long long hbm_budget, int max_active);
+/* Queue a request (its arrays are copied); *ticket identifies it.  A request
+ * whose footprint alone exceeds the budget is refused with EGS_ERR_OOM. */
+EGS_API int egs_server_submit(egs_server* s, const egs_request* r, long long* ticket);
+/* Block until the request is done; copy its result (and, for PREDICT, n_miss
+ * predictions into z_miss when it is not NULL) and release the ticket. */
+EGS_API int egs_server_wait(egs_server* s, long long ticket, egs_result* out, double* z_miss);
+/* Snapshot: queued and running requests, reserved bytes, the peak of running
+ * requests and of reserved bytes so far, completed requests, and device
+ * evaluations made. */
+EGS_API int egs_server_stats(egs_server* s, int* queued, int* active, long long* reserved, int* peak_active,
+                             long long* peak_reserved, long long* completed, long long* evals);
+/* Finish every queued and running request, then stop the workers and free the server. */
+EGS_API int egs_server_destroy(egs_server* s);
 
 #ifdef __cplusplus
 }
