@@ -24,6 +24,8 @@ EGS_ERR_TIMEOUT = -5
 EGS_ERR_STATE = -6
 EGS_PRECISION_DOUBLE = 1
 EGS_PRECISION_MIXED = 2
+EGS_BAND_OZAKI_INT8 = 0
+EGS_BAND_FP64_DMMA = 1
 EGS_REQ_LOGLIK = 1
 EGS_REQ_FIT = 2
 EGS_REQ_PREDICT = 3
@@ -84,6 +86,8 @@ SIGNATURES = {
                                              ctypes.c_int]),
     "egs_problem_footprint": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _LL]),
     "egs_problem_predict": (ctypes.c_int, [_P, _D, ctypes.c_int, _D, _D, _D]),
+    "egs_ozaki_band_update": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P, _D]),
+    "egs_problem_set_band_method": (ctypes.c_int, [_P, ctypes.c_int]),
 }
 
 
@@ -274,6 +278,10 @@ class Problem:
         self._lib.egs_problem_info(self._h, ctypes.byref(nn), ctypes.byref(ts), ctypes.byref(nt), ctypes.byref(nb))
         self.ts, self.nt, self.bytes = ts.value, nt.value, nb.value
 
+    def set_band_method(self, method: int) -> None:
+        """EGS_BAND_OZAKI_INT8 (default) or EGS_BAND_FP64_DMMA for the FP64 band of a mixed problem."""
+        _check(self._lib.egs_problem_set_band_method(self._h, int(method)), "set_band_method")
+
     def predict(self, theta, x_miss, y_miss) -> np.ndarray:
         """Kriging at the targets with the resident observations (either precision)."""
         th = _f64(theta)
@@ -427,6 +435,14 @@ def split_update(ts: int, nt: int, band: int, k: int, panel_ptr: int, offband_pt
     ms = ctypes.c_double()
     _check(lib.egs_split_update(int(ts), int(nt), int(band), int(k), _P(panel_ptr), _P(offband_ptr),
                                 ctypes.byref(ms)), "egs_split_update")
+    return ms.value
+
+
+def ozaki_band_update(ts: int, nt: int, band: int, k: int, w_ptr: int, band_ptr: int) -> float:
+    """One Ozaki-scheme band update on device buffers (test entry); returns the kernel time in ms."""
+    ms = ctypes.c_double()
+    _check(load_library().egs_ozaki_band_update(int(ts), int(nt), int(band), int(k), _P(w_ptr), _P(band_ptr),
+                                                ctypes.byref(ms)), "egs_ozaki_band_update")
     return ms.value
 
 

@@ -100,6 +100,19 @@ struct egs_problem {
     long long total;
   };
   std::vector<JobLaunch> band_launch;  // per step k
+  // Ozaki-scheme band update: int8 slices of the panel rows, row scales, and
+  // per-step target tables (offset into oz_targets, count, work items)
+  int band_method = EGS_BAND_OZAKI_INT8;
+  int8_t* oz_slices = nullptr;
+  double* oz_scale = nullptr;
+  int4* oz_targets = nullptr;
+  struct OzLaunch {
+    long long off;
+    int count;
+    long long items;
+  };
+  std::vector<OzLaunch> oz_launch;
+  alignas(64) unsigned char tm_oz[128];
   alignas(64) unsigned char tmapW[128];
   alignas(64) unsigned char tm_hi[128];
   alignas(64) unsigned char tm_lo[128];
@@ -219,13 +232,18 @@ void pinned_release(void* r) {
 }
 
 void free_mixed(egs_problem* p) {
-  void* bufs[] = {p->band_pool, p->off_pool, p->W, p->ph, p->pl, p->inv_scale, p->w, p->res_scratch,
-                  p->gen_tiles, p->band_jobs, p->band_begin, p->inv_pool, p->solve_tmp};
+  void* bufs[] = {p->band_pool, p->off_pool, p->W,         p->ph,      p->pl,          p->inv_scale,
+                  p->w,         p->res_scratch, p->gen_tiles, p->band_jobs, p->band_begin, p->inv_pool,
+                  p->solve_tmp, p->oz_slices, p->oz_scale, p->oz_targets};
   for (void* b : bufs) dev_free(b, p->stream);
   p->band_pool = nullptr;
   p->off_pool = nullptr;
   p->W = nullptr;
   p->inv_pool = p->solve_tmp = nullptr;
+  p->oz_slices = nullptr;
+  p->oz_scale = nullptr;
+  p->oz_targets = nullptr;
+  p->oz_launch.clear();
   p->ph = p->pl = nullptr;
   p->inv_scale = nullptr;
   p->w = p->res_scratch = nullptr;
@@ -548,12 +566,23 @@ int enqueue_eval_mixed(egs_problem* p) {
     if (ntp > 1) {
       // FP64 band targets: tile rows j .. min(nt-1, j+b) of every column j > k
       sp = span_begin(p, EGS_STAGE_UPDATE);
-      const egs_problem::JobLaunch& L = p->band_launch[k];
-      if (L.njobs > 0 && L.total > 0) {
-        int rc = launch_gemm_batched(p->tmapW, p->band_pool, p->band_jobs + L.job_off, p->band_begin + L.begin_off,
-                                     L.njobs, L.total, err, st);
-        if (rc != EGS_OK) return rc;
-        count_launches(p, EGS_STAGE_UPDATE, 1);
+      if (p->band_method == EGS_BAND_OZAKI_INT8) {
+        const egs_problem::OzLaunch& O = p->oz_launch[k];
+        if (O.count > 0) {
+          launch_ozaki_slice(p->W, ts, 1, ntp - 1, k, p->oz_scale, p->oz_slices, p->np, st);
+          int rc = launch_ozaki_band(p->tm_oz, p->oz_targets + O.off, O.count, O.items, ts, b, p->band_pool,
+                                     p->oz_scale, err, st);
+          if (rc != EGS_OK) return rc;
+          count_launches(p, EGS_STAGE_UPDATE, 3);
+        }
+      } else {
+        const egs_problem::JobLaunch& L = p->band_launch[k];
+        if (L.njobs > 0 && L.total > 0) {
+          int rc = launch_gemm_batched(p->tmapW, p->band_pool, p->band_jobs + L.job_off,
+                                       p->band_begin + L.begin_off, L.njobs, L.total, err, st);
+          if (rc != EGS_OK) return rc;
+          count_launches(p, EGS_STAGE_UPDATE, 1);
+        }
       }
       double band_tiles = 0.0;
       for (int j = k + 1; j < nt; ++j) band_tiles += (double)(std::min(nt - 1, j + b) - j + 1);
@@ -668,6 +697,26 @@ int setup_mixed(egs_problem* p, int b) {
   if (!jobs.empty())
     EGS_CUDA_TRY(cudaMemcpy(p->band_jobs, jobs.data(), jobs.size() * sizeof(GemmDesc), cudaMemcpyHostToDevice));
   EGS_CUDA_TRY(cudaMemcpy(p->band_begin, begin.data(), begin.size() * sizeof(long long), cudaMemcpyHostToDevice));
+  // Ozaki band update: slices of every panel row, per-step target tables
+  {
+    std::vector<int4> targets;
+    p->oz_launch.clear();
+    for (int k = 0; k < nt; ++k) {
+      const long long off = (long long)targets.size();
+      const long long items = ozaki_targets(ts, nt, b, k, targets);
+      p->oz_launch.push_back({off, (int)((long long)targets.size() - off), items});
+    }
+    if ((rc = dev_alloc(&p->oz_slices, (size_t)p->np * ts * ozaki_slices(), &p->bytes, p->stream)) ||
+        (rc = dev_alloc(&p->oz_scale, (size_t)p->np, &p->bytes, p->stream)) ||
+        (rc = dev_alloc(&p->oz_targets, std::max<size_t>(1, targets.size()), &p->bytes, p->stream)))
+      return rc;
+    if (!targets.empty())
+      EGS_CUDA_TRY(cudaMemcpyAsync(p->oz_targets, targets.data(), targets.size() * sizeof(int4),
+                                   cudaMemcpyHostToDevice, p->stream));
+    EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
+    if ((rc = ozaki_tensor_map(p->tm_oz, p->oz_slices, ts, p->np)) != EGS_OK) return rc;
+    EGS_CUDA_TRY(cudaMemsetAsync(p->oz_scale, 0, p->np * sizeof(double), p->stream));
+  }
   if ((rc = gemm_init_tensor_map(p->tmapW, p->W, ts, nt + 1)) != EGS_OK ||
       (rc = split_tensor_map(p->tm_hi, p->ph, ts, p->np)) != EGS_OK ||
       (rc = split_tensor_map(p->tm_lo, p->pl, ts, p->np)) != EGS_OK ||
@@ -898,6 +947,22 @@ int egs_problem_set_precision(egs_problem* p, int precision, int band_tiles) {
     p->precision = kPrecisionBroken;
   }
   return rc;
+}
+
+int egs_problem_set_band_method(egs_problem* p, int method) {
+  if (!p || (method != EGS_BAND_OZAKI_INT8 && method != EGS_BAND_FP64_DMMA)) return EGS_ERR_INVALID;
+  if (p->precision != EGS_PRECISION_MIXED) {
+    set_last_error("only a mixed-precision problem has a band method", "egs_problem_set_band_method");
+    return EGS_ERR_STATE;
+  }
+  if (method == p->band_method) return EGS_OK;
+  EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  if (p->graph_exec) cudaGraphExecDestroy(p->graph_exec);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  p->graph_exec = nullptr;
+  p->graph = nullptr;
+  p->band_method = method;
+  return EGS_OK;
 }
 
 int egs_problem_set_stream(egs_problem* p, void* cuda_stream) {

@@ -98,6 +98,16 @@ int split_c_maps(void* tm_c, void* tm_cr, const float* c_pool, int ts, long long
 void launch_panel_split(const double* W, int ts, int t0, int ntiles, int row_tile0, float* inv_scale, __half* Ph,
                         __half* Pl, cudaStream_t st);
 long long split_targets(int nt, int band, int k);
+int ozaki_slices();
+int ozaki_tensor_map(void* storage, const int8_t* slices, int ts, long long rows);
+void launch_ozaki_slice(const double* W, int ts, int t0, int ntiles, int row_tile0, double* scale, int8_t* slices,
+                        long long rows, cudaStream_t st);
+}  // namespace egs
+#include <vector>
+namespace egs {
+long long ozaki_targets(int ts, int nt, int band, int k, std::vector<int4>& out);
+int launch_ozaki_band(const void* tm_s, const int4* targets, int ntargets, long long total, int ts, int band,
+                      double* band_pool, const double* scale, int* err, cudaStream_t st);
 int launch_split_update(const void* tm_hi, const void* tm_lo, const void* tm_c, const void* tm_cr, int ts, int nt,
                         int band, int k, float* c_pool,
                         const float* inv_scale, int* err, cudaStream_t st);

@@ -1,0 +1,523 @@
+// FP64-class band update of the mixed-precision factorisation on the integer
+// tensor cores (tcgen05 kind::i8, sm_100a): the Ozaki splitting scheme.
+//
+// At step k every band target tile (i, j), k < j <= i <= j + band, receives
+// C_ij -= L_ik L_jk^T in FP64 storage.  The FP64 panel rows are split, after a
+// power-of-two row scaling 2^-e_r (|L_r.| < 2^e_r), into S signed 7-bit
+// slices:
+//     L_rc = 2^e_r * sum_{p=1..S} a_p(r, c) 2^(-7p),   a_p in [-127, 127],
+// exact up to 2^(-7S) of the row maximum (S = 7: 2^-49).  Then
+//     (L_i L_j^T)(r, c) = 2^(e_r + e_c) * sum_{d=2..S+1} 2^(-7d) G_d(r, c),
+//     G_d = sum_{p+q=d} A_p B_q^T,
+// where every G_d is an exact integer dot product: the int8 MMAs accumulate
+// in 32-bit integers without rounding (|G_d| <= S * K * 127^2 < 2^31 for
+// K <= 16384), so the only roundings are the final FP64 combination and the
+// dropped terms p + q > S + 1 (each below 2^(-7(S+1)) of the row maxima).
+// This follows Ozaki, Ogita, Oishi and Rump, "Error-free transformations of
+// matrix multiplication by using fast routines of matrix multiplication and
+// its applications", Numer. Algorithms 59 (2012), with the integer-slice
+// variant of Ootomo, Ozaki and Yokota (2024).
+//
+// Kernel (one CTA per SM, persistent over 128 x 64 output tiles; 320 threads):
+//   warp 0    TMA producer: per 64-wide K stage the S slices of the tile's 128
+//             A rows and 64 B rows (64-byte swizzle), 2-stage ring;
+//   warp 1    allocates 512 TMEM columns -- S groups of 64 int32 columns, one
+//             per d -- and issues S(S+1)/2 MMAs per 32-wide K step from one
+//             thread, the first of each group with accumulate = 0;
+//   warps 2-9 epilogue: warp w reads TMEM lane quarter w % 4 and 32 of the 64
+//             columns, combines the groups in FP64 (smallest first), scales by
+//             2^(e_r + e_c) and subtracts from the FP64 band tile.
+// The accumulator is single-buffered (S groups fill TMEM); the epilogue
+// releases it as soon as its TMEM loads are done, before the C update.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#include "common.cuh"
+#include "kernels.cuh"
+#include "mbarrier.cuh"
+
+namespace egs {
+
+namespace oz {
+constexpr int S = 7;                       // slices per operand
+constexpr int NGROUPS = S;                 // d = 2 .. S+1
+constexpr int BM = 128, BN = 64, BK = 64;  // BK int8 = one 64-byte swizzle row
+constexpr int STAGES = 2;
+constexpr int BOX_ROWS = 64;
+constexpr int A_SLICE = BM * BK;           // 8 KB
+constexpr int B_SLICE = BN * BK;           // 4 KB
+constexpr int STAGE_BYTES = S * (A_SLICE + B_SLICE);
+constexpr int EPI_WARPS = 8;
+constexpr int THREADS = 64 + 32 * EPI_WARPS;
+constexpr int SMEM_BYTES = 1024 + STAGES * STAGE_BYTES + 256;
+constexpr uint32_t TMEM_COLS = 512;
+static_assert(NGROUPS * BN <= (int)TMEM_COLS, "groups fit in tensor memory");
+static_assert(SMEM_BYTES <= 232448, "shared memory per CTA");
+// Instruction descriptor of kind::i8: D S32 (bits 4-5 = 2), A and B signed 8-bit
+// (bits 7-9 = 1, bits 10-12 = 1), both K-major, N >> 3 at bits 17-22, M >> 4 at 24-28.
+constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                           ((uint32_t)(BM >> 4) << 24);
+}  // namespace oz
+
+// ---------------------------------------------------------------------------
+// Slicing of the solved panel
+// ---------------------------------------------------------------------------
+
+// Row scale of panel tile t (rows of W tile t0 + blockIdx.y): scale = 2^e with
+// max_c |W(r, c)| < 2^e (e from the maximum's exponent + 1); 0 rows get scale 0.
+__global__ void __launch_bounds__(256)
+ozaki_rowscale_kernel(const double* __restrict__ W, int ts, int t0, int row_tile0, double* __restrict__ scale) {
+  __shared__ double red[4][64];
+  const int t = t0 + blockIdx.y;
+  const int rl = threadIdx.x & 63, g = threadIdx.x >> 6;
+  const int r = blockIdx.x * 64 + rl;
+  const double* col = W + (long long)t * ts * ts + r;
+  double m = 0.0;
+  for (int c = g; c < ts; c += 4) m = fmax(m, fabs(col[(long long)c * ts]));
+  red[g][rl] = m;
+  __syncthreads();
+  if (g == 0) {
+    m = fmax(fmax(red[0][rl], red[1][rl]), fmax(red[2][rl], red[3][rl]));
+    double sc;
+    if (!(m > 0.0)) {
+      sc = (m == 0.0) ? 0.0 : __longlong_as_double(0x7ff8000000000000ll);  // NaN rows stay NaN
+    } else {
+      const long long bits = __double_as_longlong(m);
+      const int e = (int)((bits >> 52) & 0x7FF) - 1023;  // 2^e <= m < 2^(e+1) for normal m
+      sc = (e >= 1023) ? __longlong_as_double(0x7ff8000000000000ll) : ldexp(1.0, e + 1);
+    }
+    scale[(long long)(row_tile0 + t) * ts + r] = sc;
+  }
+}
+
+// Slices of 64 x 64 blocks of panel tiles, transposed to row-major int8 rows
+// (K contiguous): slices[p][row][c], p = 0..S-1 for 2^-7 .. 2^-7S.
+__global__ void __launch_bounds__(256)
+ozaki_slice_kernel(const double* __restrict__ W, int ts, int t0, int row_tile0, const double* __restrict__ scale,
+                   int8_t* __restrict__ slices, long long slice_stride) {
+  __shared__ double Sm[64][65];
+  const int t = t0 + blockIdx.z;
+  const int r0 = blockIdx.x * 64, c0 = blockIdx.y * 64;
+  const double* src = W + (long long)t * ts * ts;
+  for (int e = threadIdx.x; e < 64 * 64; e += 256) {
+    const int r = e & 63, c = e >> 6;
+    Sm[r][c] = src[(long long)(c0 + c) * ts + r0 + r];
+  }
+  __syncthreads();
+  const long long grow0 = (long long)(row_tile0 + t) * ts + r0;
+  // thread: row r, 16 consecutive columns (16-byte stores per slice)
+  const int r = threadIdx.x >> 2, cq = (threadIdx.x & 3) * 16;
+  const double sc = scale[grow0 + r];
+  const double inv = (sc > 0.0) ? 1.0 / sc : 0.0;  // exact: a power of two
+  double v[16];
+#pragma unroll
+  for (int c = 0; c < 16; ++c) v[c] = Sm[r][cq + c] * inv;  // |v| < 1
+  int8_t* dst = slices + (grow0 + r) * ts + c0 + cq;
+#pragma unroll
+  for (int p = 0; p < oz::S; ++p) {
+    union {
+      int8_t b[16];
+      int4 q;
+    } out;
+#pragma unroll
+    for (int c = 0; c < 16; ++c) {
+      const double x = v[c] * 128.0;  // exact scaling
+      const double a = trunc(x);      // |a| <= 127
+      v[c] = x - a;                   // exact remainder, |v| < 1
+      out.b[c] = (int8_t)__double2int_rz(a);
+    }
+    *reinterpret_cast<int4*>(dst + p * slice_stride) = out.q;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// tcgen05 helpers (kind::i8, 64-byte swizzle)
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ uint64_t sdesc_sw64(uint32_t addr) {
+  uint64_t d = (uint64_t)((addr & 0x3FFFF) >> 4);
+  d |= (uint64_t)1 << 16;            // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(512 >> 4) << 32;   // stride byte offset: 8 rows x 64 B
+  d |= (uint64_t)1 << 46;            // descriptor version
+  d |= (uint64_t)4 << 61;            // SWIZZLE_64B
+  return d;
+}
+__device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(oz::IDESC), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void oz_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void oz_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void oz_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void oz_tma_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_u32(dst)),
+      "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tmem_ld16_i32(uint32_t taddr, int (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = (int)r[i];
+}
+
+// Targets of one step: target t = (i, j, first work item, diagonal flag);
+// items of an off-diagonal target: MB x NB tiles (row block fastest); of a
+// diagonal target: the tiles touching the lower triangle, nb <= 2 mb + 1,
+// enumerated row block by row block.
+struct OzStep {
+  const int4* targets;
+  int ntargets;
+  long long total;
+  int ts, band;
+  double* band_pool;
+  const double* scale;   // per global panel row
+  int* err;
+};
+
+__device__ __forceinline__ void oz_decode(const OzStep& P, long long L, int& i, int& j, int& mb, int& nb) {
+  int lo = 0, hi = P.ntargets - 1;
+  while (lo < hi) {  // last target whose first item <= L
+    const int mid = (lo + hi + 1) >> 1;
+    if ((long long)P.targets[mid].z <= L) lo = mid; else hi = mid - 1;
+  }
+  const int4 t = P.targets[lo];
+  i = t.x;
+  j = t.y;
+  const int l = (int)(L - t.z);
+  const int MB = P.ts / oz::BM;
+  if (t.w == 0) {
+    mb = l % MB;
+    nb = l / MB;
+  } else {
+    int m = 0;
+    while ((m + 1) * (m + 1) + (m + 1) <= l) ++m;  // items before row block m: m^2 + m
+    mb = m;
+    nb = l - (m * m + m);
+  }
+}
+
+__global__ void __launch_bounds__(oz::THREADS, 1)
+ozaki_band_kernel(const __grid_constant__ CUtensorMap tm_s, const __grid_constant__ OzStep P) {
+  using namespace oz;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
+  uint64_t* empty = full + STAGES;
+  uint64_t* acc_full = empty + STAGES;
+  uint64_t* acc_empty = acc_full + 1;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 1);
+  __shared__ int bail_flag;
+  volatile int& bail = bail_flag;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(acc_full, 1);
+    mbar_init(acc_empty, EPI_WARPS);
+    bail = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  oz_fence_before();
+  __syncthreads();
+  oz_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+  const int ksteps = P.ts / BK;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      uint32_t it = 0;
+      for (long long L = blockIdx.x; L < P.total && !bail; L += gridDim.x) {
+        int i, j, mb, nb;
+        oz_decode(P, L, i, j, mb, nb);
+        const int arow = i * P.ts + mb * BM, brow = j * P.ts + nb * BN;
+        for (int kt = 0; kt < ksteps; ++kt, ++it) {
+          const uint32_t s = it % STAGES;
+          if (it >= (uint32_t)STAGES && !mbar_wait(&empty[s], ((it / STAGES) & 1) ^ 1, P.err)) {
+            bail = 1;
+            break;
+          }
+          uint8_t* st = smem + s * STAGE_BYTES;
+          mbar_expect_tx(&full[s], STAGE_BYTES);
+          const int x = kt * BK;
+#pragma unroll 1
+          for (int p = 0; p < S; ++p) {
+            oz_tma_3d(st + p * A_SLICE, &tm_s, &full[s], x, arow, p);
+            oz_tma_3d(st + p * A_SLICE + BOX_ROWS * BK, &tm_s, &full[s], x, arow + BOX_ROWS, p);
+            oz_tma_3d(st + S * A_SLICE + p * B_SLICE, &tm_s, &full[s], x, brow, p);
+          }
+        }
+      }
+      const uint32_t first = it > (uint32_t)STAGES ? it - STAGES : 0;
+      for (uint32_t q = first; q < it; ++q) mbar_wait(&full[q % STAGES], (q / STAGES) & 1, P.err);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      uint32_t it = 0, tcount = 0;
+      bool ok = true;
+      for (long long L = blockIdx.x; L < P.total && ok && !bail; L += gridDim.x, ++tcount) {
+        if (tcount >= 1 && !mbar_wait(acc_empty, (tcount - 1) & 1, P.err)) {
+          ok = false;
+          break;
+        }
+        oz_fence_after();
+        for (int kt = 0; kt < ksteps; ++kt, ++it) {
+          const uint32_t s = it % STAGES;
+          if (!mbar_wait(&full[s], (it / STAGES) & 1, P.err)) {
+            ok = false;
+            break;
+          }
+          oz_fence_after();
+          const uint32_t sa = smem_u32(smem + s * STAGE_BYTES);
+          const uint32_t sb = sa + S * A_SLICE;
+#pragma unroll
+          for (int kk = 0; kk < BK / 32; ++kk) {
+#pragma unroll
+            for (int d = 2; d <= S + 1; ++d) {
+              const uint32_t dcol = tmem_base + (uint32_t)((d - 2) * BN);
+#pragma unroll
+              for (int p = 1; p <= S; ++p) {
+                const int q = d - p;
+                if (q < 1 || q > S) continue;
+                const uint32_t acc = (kt > 0 || kk > 0 || p > 1) ? 1u : 0u;  // p = 1 opens group d
+                umma_i8(dcol, sdesc_sw64(sa + (p - 1) * A_SLICE + kk * 32), sdesc_sw64(sb + (q - 1) * B_SLICE + kk * 32),
+                        acc);
+              }
+            }
+          }
+          oz_commit(&empty[s]);
+        }
+        if (!ok) break;
+        oz_commit(acc_full);
+      }
+      if (!ok) bail = 1;
+    }
+  } else {
+    // epilogue warps 2..9: lane quarter warp % 4, columns [half * 32, half * 32 + 32)
+    const int quarter = warp & 3, half = (warp - 2) >> 2;
+    const uint32_t tl = tmem_base + ((uint32_t)(quarter * 32) << 16) + half * 32;
+    uint32_t tcount = 0;
+    bool ok = true;
+    for (long long L = blockIdx.x; L < P.total && ok; L += gridDim.x, ++tcount) {
+      int w = 1;
+      if (lane == 0) w = mbar_wait(acc_full, tcount & 1, P.err) ? 1 : 0;
+      w = __shfl_sync(0xffffffffu, w, 0);
+      if (!w) {
+        ok = false;
+        break;
+      }
+      oz_fence_after();
+      double acc[32];
+#pragma unroll
+      for (int c = 0; c < 32; ++c) acc[c] = 0.0;
+      // smallest groups first: sum_d 2^(-7d) G_d
+#pragma unroll 1
+      for (int g = NGROUPS - 1; g >= 0; --g) {
+        const double f = __longlong_as_double((long long)(1023 - 7 * (g + 2)) << 52);  // 2^(-7(g+2))
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          int v[16];
+          tmem_ld16_i32(tl + (uint32_t)(g * BN + h * 16), v);
+#pragma unroll
+          for (int c = 0; c < 16; ++c) acc[h * 16 + c] = fma((double)v[c], f, acc[h * 16 + c]);
+        }
+      }
+      oz_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(acc_empty);
+      int i, j, mb, nb;
+      oz_decode(P, L, i, j, mb, nb);
+      const int r = mb * BM + quarter * 32 + lane;
+      const int c0 = nb * BN + half * 32;
+      const double sr = P.scale[(long long)i * P.ts + r];
+      const double* sc = P.scale + (long long)j * P.ts + c0;
+      double* C = P.band_pool + ((long long)j * (P.band + 1) + (i - j)) * P.ts * P.ts;
+      double* cp = C + (long long)c0 * P.ts + r;
+      const bool diag = (i == j);
+#pragma unroll
+      for (int c = 0; c < 32; ++c) {
+        if (!diag || r >= c0 + c) {
+          double* e = cp + (long long)c * P.ts;
+          *e -= acc[c] * (sr * __ldg(sc + c));
+        }
+      }
+    }
+    if (!ok) bail = 1;
+  }
+  oz_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    __syncwarp();
+    oz_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS) : "memory");
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+
+int ozaki_slices() { return oz::S; }
+
+// Slice storage: S planes of rows x ts int8 (rows = every global panel row).
+int ozaki_tensor_map(void* storage, const int8_t* slices, int ts, long long rows) {
+  void* fn = nullptr;
+  if (tensor_map_encoder(&fn) != EGS_OK) return EGS_ERR_CUDA;
+  if (ts % oz::BK != 0 || ((uintptr_t)slices & 15) != 0) return EGS_ERR_INVALID;
+  auto encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  cuuint64_t dims[3] = {(cuuint64_t)ts, (cuuint64_t)rows, (cuuint64_t)oz::S};
+  cuuint64_t strides[2] = {(cuuint64_t)ts, (cuuint64_t)ts * (cuuint64_t)rows};
+  cuuint32_t box[3] = {oz::BK, oz::BOX_ROWS, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = encode(reinterpret_cast<CUtensorMap*>(storage), CU_TENSOR_MAP_DATA_TYPE_UINT8, 3,
+                      const_cast<int8_t*>(slices), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                      CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_last_error("cuTensorMapEncodeTiled failed", "ozaki_tensor_map");
+    return EGS_ERR_CUDA;
+  }
+  return EGS_OK;
+}
+
+void launch_ozaki_slice(const double* W, int ts, int t0, int ntiles, int row_tile0, double* scale, int8_t* slices,
+                        long long rows, cudaStream_t st) {
+  if (ntiles <= 0) return;
+  ozaki_rowscale_kernel<<<dim3(ts / 64, ntiles), 256, 0, st>>>(W, ts, t0, row_tile0, scale);
+  ozaki_slice_kernel<<<dim3(ts / 64, ts / 64, ntiles), 256, 0, st>>>(W, ts, t0, row_tile0, scale, slices,
+                                                                      rows * (long long)ts);
+}
+
+// Target table of step k: band targets (i, j), k < j <= i <= min(nt-1, j+band),
+// column by column; returns the total work items.
+long long ozaki_targets(int ts, int nt, int band, int k, std::vector<int4>& out) {
+  const int MB = ts / oz::BM, NB = ts / oz::BN;
+  long long items = 0;
+  for (int j = k + 1; j < nt; ++j) {
+    for (int i = j; i <= j + band && i < nt; ++i) {
+      out.push_back(make_int4(i, j, (int)items, i == j ? 1 : 0));
+      if (i == j) {
+        for (int m = 0; m < MB; ++m) items += std::min(NB, 2 * m + 2);
+      } else {
+        items += (long long)MB * NB;
+      }
+    }
+  }
+  return items;
+}
+
+int launch_ozaki_band(const void* tm_s, const int4* targets, int ntargets, long long total, int ts, int band,
+                      double* band_pool, const double* scale, int* err, cudaStream_t st) {
+  using namespace oz;
+  if (ts % BM != 0 || ts / BN > 2 * (ts / BM)) return EGS_ERR_INVALID;
+  if (total <= 0 || ntargets <= 0) return EGS_OK;
+  static const bool attr = []() {
+    cudaFuncSetAttribute(ozaki_band_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    return true;
+  }();
+  (void)attr;
+  OzStep P;
+  P.targets = targets;
+  P.ntargets = ntargets;
+  P.total = total;
+  P.ts = ts;
+  P.band = band;
+  P.band_pool = band_pool;
+  P.scale = scale;
+  P.err = err;
+  const long long grid = total < gemm_num_sms() ? total : gemm_num_sms();
+  ozaki_band_kernel<<<(unsigned)grid, THREADS, SMEM_BYTES, st>>>(*reinterpret_cast<const CUtensorMap*>(tm_s), P);
+  return cudaGetLastError() == cudaSuccess ? EGS_OK : EGS_ERR_CUDA;
+}
+
+}  // namespace egs
+
+using namespace egs;
+
+// Test entry: one band update of step k from panel tiles W[t] = L_{k+t,k}
+// (t = 0 .. nt-k-1, FP64 column-major ts x ts; W[0] is not read) into the FP64
+// band pool (nt * (band + 1) tiles, slot j * (band + 1) + (i - j)).
+extern "C" int egs_ozaki_band_update(int ts, int nt, int band, int k, const double* W, double* band_pool,
+                                     double* ms) {
+  if (ts <= 0 || ts % oz::BM != 0 || nt <= 0 || band < 0 || k < 0 || k >= nt || !W || !band_pool)
+    return EGS_ERR_INVALID;
+  const int ntp = nt - k;
+  const long long rows = (long long)nt * ts;
+  int8_t* sl = nullptr;
+  double* scale = nullptr;
+  int* err = nullptr;
+  int4* dt = nullptr;
+  alignas(64) unsigned char tm[128];
+  std::vector<int4> targets;
+  const long long total = ozaki_targets(ts, nt, band, k, targets);
+  int rc = EGS_OK;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaMalloc(&sl, (size_t)rows * ts * oz::S) || cudaMalloc(&scale, rows * sizeof(double)) ||
+      cudaMalloc(&err, sizeof(int)) || cudaMalloc(&dt, std::max<size_t>(1, targets.size()) * sizeof(int4))) {
+    cudaGetLastError();
+    rc = EGS_ERR_OOM;
+    goto done;
+  }
+  cudaMemset(err, 0, sizeof(int));
+  cudaMemset(scale, 0, rows * sizeof(double));
+  cudaMemset(sl, 0, (size_t)rows * ts * oz::S);
+  if (!targets.empty()) cudaMemcpy(dt, targets.data(), targets.size() * sizeof(int4), cudaMemcpyHostToDevice);
+  if ((rc = ozaki_tensor_map(tm, sl, ts, rows)) != EGS_OK) goto done;
+  launch_ozaki_slice(W, ts, 1, ntp - 1, k, scale, sl, rows, 0);
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, 0);
+  if ((rc = launch_ozaki_band(tm, dt, (int)targets.size(), total, ts, band, band_pool, scale, err, 0)) != EGS_OK)
+    goto done;
+  cudaEventRecord(e1, 0);
+  if (cudaDeviceSynchronize() != cudaSuccess) {
+    rc = EGS_ERR_CUDA;
+    set_last_error(cudaGetErrorString(cudaGetLastError()), "egs_ozaki_band_update");
+    goto done;
+  }
+  {
+    int h = 0;
+    cudaMemcpy(&h, err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (h) {
+      set_last_error("a device-side wait exceeded its limit", "egs_ozaki_band_update");
+      rc = EGS_ERR_TIMEOUT;
+    }
+    float t = 0.f;
+    cudaEventElapsedTime(&t, e0, e1);
+    if (ms) *ms = t;
+  }
+done:
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(sl);
+  cudaFree(scale);
+  cudaFree(err);
+  cudaFree(dt);
+  return rc;
+}

@@ -91,6 +91,15 @@ EGS_API int egs_problem_set_band(egs_problem* p, int band);
  * dense path has no mixed implementation. */
 EGS_API int egs_problem_set_precision(egs_problem* p, int precision, int band_tiles);
 
+/* Arithmetic of the FP64 band updates of a mixed problem:
+ * EGS_BAND_OZAKI_INT8 (default) splits the panel into seven signed 7-bit
+ * slices per row and forms the products exactly on the int8 tensor cores
+ * (FP64-class accuracy, 2^-49 of the row maxima per operand);
+ * EGS_BAND_FP64_DMMA uses the FP64 tensor path. */
+#define EGS_BAND_OZAKI_INT8 0
+#define EGS_BAND_FP64_DMMA 1
+EGS_API int egs_problem_set_band_method(egs_problem* p, int method);
+
 /* Create a problem directly in the given precision (EGS_PRECISION_DOUBLE or
  * EGS_PRECISION_MIXED with band_tiles FP64 tile rows): the same as
  * egs_problem_create followed by egs_problem_set_precision, without ever
@@ -278,6 +287,15 @@ EGS_API int egs_batch_autotune(int B, const int* n, const double* x, const doubl
  * k = -1 updates every off-band tile.  *ms (may be NULL) receives the device
  * time of the update kernel.  Allocates and frees its scratch per call. */
 EGS_API int egs_split_update(int ts, int nt, int band, int k, const double* panel, float* offband, double* ms);
+
+/* Test entry of the FP64-class band update of the mixed-precision form (Ozaki
+ * scheme on the int8 tensor cores): for step k, C_ij -= L_ik L_jk^T for every
+ * band target k < j <= i <= min(nt-1, j+band), with panel tiles
+ * W[t] = L_{k+t,k} (t = 0 .. nt-k-1, FP64 column-major ts x ts, device; W[0]
+ * is not read) and the FP64 band pool (nt*(band+1) tiles, slot
+ * j*(band+1) + i-j, device).  ts must be a multiple of 128.  *ms receives the
+ * update kernel's time.  Allocates its own scratch. */
+EGS_API int egs_ozaki_band_update(int ts, int nt, int band, int k, const double* W, double* band_pool, double* ms);
 
 /* ---- kernel plugin ------------------------------------------------------ */
 
