@@ -51,12 +51,12 @@ matern_batch_kernel(double* __restrict__ tiles, const double* __restrict__ x, co
                     (long long)blockIdx.x * kGenPairsPerBlock, prm, stab);
 }
 
-__global__ void __launch_bounds__(32)
+__global__ void __launch_bounds__(256)
 potrf_batch_kernel(double* __restrict__ tiles, int ts, int k, int kb, const long long* __restrict__ tile_base,
                    const int* __restrict__ ntv, int* __restrict__ info) {
   const int p = blockIdx.x;
   const long long slot = tile_base[p] + tile_slot(k, k, ntv[p]);
-  potrf64_body(tiles + slot * (long long)ts * ts + (long long)kb * ts + kb, ts, k * ts + kb, info + p);
+  potrf64_body<256>(tiles + slot * (long long)ts * ts + (long long)kb * ts + kb, ts, k * ts + kb, info + p);
 }
 
 // panel = 0: rows [row0, ts) of the diagonal tile; panel = 1: all rows of tiles k+1.. of each problem.
@@ -303,7 +303,7 @@ int enqueue_batch_eval(egs_batch* b) {
     const int A = b->active[k];
     const int A1 = (k + 1 < b->nt_max) ? b->active[k + 1] : 0;
     for (int kb = 0; kb < ts; kb += kBatchInner, ++li) {
-      potrf_batch_kernel<<<A, 32, 0, st>>>(b->tiles, ts, k, kb, b->d_tile_base, b->d_nt, b->info);
+      potrf_batch_kernel<<<A, 256, 0, st>>>(b->tiles, ts, k, kb, b->d_tile_base, b->d_nt, b->info);
       ++b->launches_per_eval;
       if (kb + kBatchInner < ts) {
         const int rows = ts - kb - kBatchInner;

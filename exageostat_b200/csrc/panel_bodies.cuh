@@ -21,46 +21,67 @@ __device__ __forceinline__ double block_sum_256(double v, double* red) {
   return out;
 }
 
-// Cholesky of the 64x64 block at T (ld ts) by one warp.  The block sits in
-// shared memory; lane l owns rows l and l + 32.  Step j: every lane reads the
-// pivot (a broadcast), scales its entries of column j, and applies the rank-1
-// update to its rows, reading L[c][j] as broadcasts; only __syncwarp separates
-// the steps.  info records the 1-based global column (gcol0 + j + 1) of the
-// first pivot that is not positive (or NaN).
+// Cholesky of the 64x64 block at T (ld ts).  Every thread of the block (NTHR,
+// whole warps) takes part in moving the block between global
+// and shared memory with all loads issued before any is used; warp 0 factors
+// it: lane l owns rows l and l + 32.  Step j: every lane reads the pivot (a
+// broadcast), scales its entries of column j, and applies the rank-1 update to
+// its rows, reading L[c][j] as broadcasts; only __syncwarp separates the
+// steps.  info records the 1-based global column (gcol0 + j + 1) of the first
+// pivot that is not positive (or NaN).
+template <int NTHR>
 __device__ __forceinline__ void potrf64_body(double* __restrict__ T, int ts, int gcol0, int* __restrict__ info) {
+  static_assert(NTHR % 32 == 0 && NTHR >= 32 && NTHR <= 1024, "whole warps");
   __shared__ double S[kNB][kNB + 1];
-  const int lane = threadIdx.x;
-  for (int c = 0; c < kNB; ++c) {
-    S[lane][c] = (lane >= c) ? T[(long long)c * ts + lane] : 0.0;
-    S[lane + 32][c] = T[(long long)c * ts + lane + 32];
-  }
-  __syncwarp();
-  const int r0 = lane, r1 = lane + 32;
-  for (int j = 0; j < kNB; ++j) {
-    const double d = S[j][j];
-    if (lane == 0 && !(d > 0.0)) atomicCAS(info, 0, gcol0 + j + 1);
-    const double ljj = sqrt(d);
-    const double inv = 1.0 / ljj;
-    const double l0 = (r0 > j) ? S[r0][j] * inv : 0.0;
-    const double l1 = (r1 > j) ? S[r1][j] * inv : 0.0;
-    __syncwarp();
-    if (r0 > j) S[r0][j] = l0;
-    if (r1 > j) S[r1][j] = l1;
-    if (r0 == j) S[r0][j] = ljj;
-    if (r1 == j) S[r1][j] = ljj;
-    __syncwarp();
-    // Independent columns: unrolled so their shared-memory latencies overlap.
-#pragma unroll 8
-    for (int c = j + 1; c < kNB; ++c) {
-      const double lcj = S[c][j];
-      if (r0 >= c) S[r0][c] = fma(-l0, lcj, S[r0][c]);
-      if (r1 >= c) S[r1][c] = fma(-l1, lcj, S[r1][c]);
+  constexpr int per = kNB * kNB / NTHR;
+  {
+    // column-major block: element e = c * 64 + r; all loads issued first
+    double v[per];
+#pragma unroll
+    for (int q = 0; q < per; ++q) {
+      const int e = q * NTHR + threadIdx.x;
+      const int r = e & (kNB - 1), c = e >> 6;
+      v[q] = (r >= c) ? T[(long long)c * ts + r] : 0.0;
     }
-    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < per; ++q) {
+      const int e = q * NTHR + threadIdx.x;
+      S[e & (kNB - 1)][e >> 6] = v[q];
+    }
   }
-  for (int c = 0; c < kNB; ++c) {
-    if (lane >= c) T[(long long)c * ts + lane] = S[lane][c];
-    T[(long long)c * ts + lane + 32] = S[lane + 32][c];
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    const int r0 = lane, r1 = lane + 32;
+    for (int j = 0; j < kNB; ++j) {
+      const double d = S[j][j];
+      if (lane == 0 && !(d > 0.0)) atomicCAS(info, 0, gcol0 + j + 1);
+      const double ljj = sqrt(d);
+      const double inv = 1.0 / ljj;
+      const double l0 = (r0 > j) ? S[r0][j] * inv : 0.0;
+      const double l1 = (r1 > j) ? S[r1][j] * inv : 0.0;
+      __syncwarp();
+      if (r0 > j) S[r0][j] = l0;
+      if (r1 > j) S[r1][j] = l1;
+      if (r0 == j) S[r0][j] = ljj;
+      if (r1 == j) S[r1][j] = ljj;
+      __syncwarp();
+      // Independent columns: unrolled so their shared-memory latencies overlap.
+#pragma unroll 8
+      for (int c = j + 1; c < kNB; ++c) {
+        const double lcj = S[c][j];
+        if (r0 >= c) S[r0][c] = fma(-l0, lcj, S[r0][c]);
+        if (r1 >= c) S[r1][c] = fma(-l1, lcj, S[r1][c]);
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < per; ++q) {
+    const int e = q * NTHR + threadIdx.x;
+    const int r = e & (kNB - 1), c = e >> 6;
+    if (r >= c) T[(long long)c * ts + r] = S[r][c];
   }
 }
 

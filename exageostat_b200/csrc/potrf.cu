@@ -21,15 +21,15 @@
 namespace egs {
 
 // Cholesky of the 64x64 diagonal block at (off, off) of one tile (potrf64_body).
-__global__ void __launch_bounds__(32)
+__global__ void __launch_bounds__(256)
 potrf_diag_block_kernel(double* __restrict__ tiles, int ts, long long slot, int off, int col_base,
                         int* __restrict__ info) {
-  potrf64_body(tiles + slot * (long long)ts * ts + (long long)off * ts + off, ts, col_base + off, info);
+  potrf64_body<256>(tiles + slot * (long long)ts * ts + (long long)off * ts + off, ts, col_base + off, info);
 }
 
 void launch_potrf_diag_block(double* tiles, int ts, long long slot, int off, int col_base, int* info,
                              cudaStream_t st) {
-  potrf_diag_block_kernel<<<1, 32, 0, st>>>(tiles, ts, slot, off, col_base, info);
+  potrf_diag_block_kernel<<<1, 256, 0, st>>>(tiles, ts, slot, off, col_base, info);
 }
 
 // X := A * L^-T for the 64-column block [col0, col0+64) of rows [row0, ts) of
