@@ -88,6 +88,7 @@ SIGNATURES = {
     "egs_problem_predict": (ctypes.c_int, [_P, _D, ctypes.c_int, _D, _D, _D]),
     "egs_ozaki_band_update": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P, _D]),
     "egs_problem_set_band_method": (ctypes.c_int, [_P, ctypes.c_int]),
+    "egs_problem_set_lookahead": (ctypes.c_int, [_P, ctypes.c_int]),
 }
 
 
@@ -281,6 +282,10 @@ class Problem:
     def set_band_method(self, method: int) -> None:
         """EGS_BAND_OZAKI_INT8 (default) or EGS_BAND_FP64_DMMA for the FP64 band of a mixed problem."""
         _check(self._lib.egs_problem_set_band_method(self._h, int(method)), "set_band_method")
+
+    def set_lookahead(self, sms: int) -> None:
+        """SMs given to the look-ahead panel of a mixed problem (0: none); results do not change."""
+        _check(self._lib.egs_problem_set_lookahead(self._h, int(sms)), "set_lookahead")
 
     def predict(self, theta, x_miss, y_miss) -> np.ndarray:
         """Kriging at the targets with the resident observations (either precision)."""

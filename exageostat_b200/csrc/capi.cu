@@ -112,7 +112,16 @@ struct egs_problem {
     long long items;
   };
   std::vector<OzLaunch> oz_launch;
+  int4* oz_trsm_targets = nullptr;
+  std::vector<OzLaunch> oz_trsm_launch;
+  double* W2 = nullptr;  // short panel: diagonal tile, band tiles, identity
+  // look-ahead: the short panel of step k+1 runs on `side` while the off-band
+  // update of step k runs on the other SMs of the problem stream
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_band = nullptr, ev_panel = nullptr;
+  int lookahead_sms = 0;  // SMs left to the look-ahead panel (0: no look-ahead)
   alignas(64) unsigned char tm_oz[128];
+  alignas(64) unsigned char tmapW2[128];
   alignas(64) unsigned char tmapW[128];
   alignas(64) unsigned char tm_hi[128];
   alignas(64) unsigned char tm_lo[128];
@@ -150,17 +159,17 @@ cudaEvent_t take_event(egs_problem* p) {
 }
 
 // Opens a timed span of `stage` on the problem stream (no-op unless profiling).
-int span_begin(egs_problem* p, int stage) {
+int span_begin(egs_problem* p, int stage, cudaStream_t on = nullptr) {
   if (!p->profiling) return -1;
   egs_problem::Span s{stage, take_event(p), take_event(p), 0.0};
-  cudaEventRecord(s.a, p->stream);
+  cudaEventRecord(s.a, on ? on : p->stream);
   p->spans.push_back(s);
   return (int)p->spans.size() - 1;
 }
 
-void span_end(egs_problem* p, int idx, double flops) {
+void span_end(egs_problem* p, int idx, double flops, cudaStream_t on = nullptr) {
   if (idx < 0) return;
-  cudaEventRecord(p->spans[idx].b, p->stream);
+  cudaEventRecord(p->spans[idx].b, on ? on : p->stream);
   p->spans[idx].flops = flops;
 }
 
@@ -234,7 +243,7 @@ void pinned_release(void* r) {
 void free_mixed(egs_problem* p) {
   void* bufs[] = {p->band_pool, p->off_pool, p->W,         p->ph,      p->pl,          p->inv_scale,
                   p->w,         p->res_scratch, p->gen_tiles, p->band_jobs, p->band_begin, p->inv_pool,
-                  p->solve_tmp, p->oz_slices, p->oz_scale, p->oz_targets};
+                  p->solve_tmp, p->oz_slices, p->oz_scale, p->oz_targets, p->oz_trsm_targets, p->W2};
   for (void* b : bufs) dev_free(b, p->stream);
   p->band_pool = nullptr;
   p->off_pool = nullptr;
@@ -244,6 +253,17 @@ void free_mixed(egs_problem* p) {
   p->oz_scale = nullptr;
   p->oz_targets = nullptr;
   p->oz_launch.clear();
+  p->oz_trsm_targets = nullptr;
+  p->oz_trsm_launch.clear();
+  p->W2 = nullptr;
+  if (p->side) {
+    cudaStreamSynchronize(p->side);
+    cudaStreamDestroy(p->side);
+  }
+  if (p->ev_band) cudaEventDestroy(p->ev_band);
+  if (p->ev_panel) cudaEventDestroy(p->ev_panel);
+  p->side = nullptr;
+  p->ev_band = p->ev_panel = nullptr;
   p->ph = p->pl = nullptr;
   p->inv_scale = nullptr;
   p->w = p->res_scratch = nullptr;
@@ -282,7 +302,7 @@ void free_problem(egs_problem* p) {
 // single-level 64-blocking.  col_base is the global column of the tile (for
 // the LAPACK-style info of a failed pivot).  Returns the launch count in *nl.
 int enqueue_panel(double* tiles, const void* tmap, int ts, int nt, int k, int col_base, int* info, int* err,
-                  cudaStream_t st, long long* nl) {
+                  cudaStream_t st, long long* nl, int max_ctas = 0) {
   const long long skk = tile_slot(k, k, nt);
   const int ntl = nt - 1 - k;
   const long long s0 = ntl > 0 ? tile_slot(k + 1, k, nt) : 0;
@@ -299,7 +319,7 @@ int enqueue_panel(double* tiles, const void* tmap, int ts, int nt, int k, int co
         if (kb + kInnerBlock < KE) {
           const int r0 = drow + kb + kInnerBlock;
           int rc = launch_gemm_rows(tmap, tiles, ts, nt, ts - kb - kInnerBlock, KE - kb - kInnerBlock, kInnerBlock,
-                                    r0, kb, k, r0, kb, k, r0, r0, 1, err, st);
+                                    r0, kb, k, r0, kb, k, r0, r0, 1, err, st, max_ctas);
           if (rc != EGS_OK) return rc;
           ++*nl;
         }
@@ -308,7 +328,7 @@ int enqueue_panel(double* tiles, const void* tmap, int ts, int nt, int k, int co
     if (KE < ts) {
       const int r0 = drow + KE;
       int rc = launch_gemm_rows(tmap, tiles, ts, nt, ts - KE, ts - KE, KE - KB, r0, KB, k, r0, KB, k, r0, r0, 1, err,
-                                st);
+                                st, max_ctas);
       if (rc != EGS_OK) return rc;
       ++*nl;
     }
@@ -323,7 +343,7 @@ int enqueue_panel(double* tiles, const void* tmap, int ts, int nt, int k, int co
         if (kb + kInnerBlock < KE) {
           const int brow = drow + kb + kInnerBlock;
           int rc = launch_gemm_rows(tmap, tiles, ts, nt, m, KE - kb - kInnerBlock, kInnerBlock, below, kb, k, brow, kb,
-                                    k, below, brow, 0, err, st);
+                                    k, below, brow, 0, err, st, max_ctas);
           if (rc != EGS_OK) return rc;
           ++*nl;
         }
@@ -331,7 +351,7 @@ int enqueue_panel(double* tiles, const void* tmap, int ts, int nt, int k, int co
       if (KE < ts) {
         const int brow = drow + KE;
         int rc = launch_gemm_rows(tmap, tiles, ts, nt, m, ts - KE, KE - KB, below, KB, k, brow, KB, k, below, brow, 0,
-                                  err, st);
+                                  err, st, max_ctas);
         if (rc != EGS_OK) return rc;
         ++*nl;
       }
@@ -524,81 +544,50 @@ int enqueue_eval(egs_problem* p) {
   return check_cuda("egs_mle_eval");
 }
 
-// Mixed-precision evaluation.  Step k: gather tile column k into the FP64
-// workspace W, factor and solve it there (the FP64 panel kernels with W as a
-// one-column problem), scatter it back (off-band tiles rounded to FP32), split
-// its rows for the FP16 tensor-core update, then update the band targets with
-// FP64 DMMA and the off-band targets with the split tcgen05 kernel.  After the
-// factorisation: log-det from the FP64 diagonal tiles, v = (L L^T)^-1 z, one
-// refinement step with the FP64 residual z - C v, and the assembly with
-// z^T (v + w).
-int enqueue_eval_mixed(egs_problem* p) {
+// Off-band update (split-FP16 tensor cores) of step k on stream st.
+static int enqueue_offband_update(egs_problem* p, int k, cudaStream_t st, int max_ctas) {
+  const int ts = p->ts, nt = p->nt, b = p->mband;
+  const long long off_targets = split_targets(nt, b, k);
+  if (off_targets <= 0) return EGS_OK;
+  int sp = span_begin(p, EGS_STAGE_UPDATE_LOW);
+  int rc = launch_split_update(p->tm_hi, p->tm_lo, p->tm_c, p->tm_cr, ts, nt, b, k, p->off_pool, p->inv_scale,
+                               p->flags + 1, st, max_ctas);
+  if (rc != EGS_OK) return rc;
+  count_launches(p, EGS_STAGE_UPDATE_LOW, 1);
+  span_end(p, sp, 2.0 * (double)off_targets * (double)ts * ts * ts);
+  return EGS_OK;
+}
+
+static double band_update_flops(int ts, int nt, int b, int k) {
+  double band_tiles = 0.0;
+  for (int j = k + 1; j < nt; ++j) band_tiles += (double)(std::min(nt - 1, j + b) - j + 1);
+  return 2.0 * band_tiles * (double)ts * ts * ts;
+}
+
+static double panel_flops(int ts, int n, int k) {
+  const double wd = (double)std::min(ts, n - k * ts);
+  const double below = (double)std::max(0, n - (k + 1) * ts);
+  return wd * wd * wd / 3.0 + wd * wd / 2.0 + wd / 6.0 + below * wd * wd;
+}
+
+static int enqueue_mixed_head(egs_problem* p) {
   cudaStream_t st = p->stream;
-  const int ts = p->ts, nt = p->nt, n = p->n, b = p->mband;
-  int* info = p->flags;
-  int* err = p->flags + 1;
   EGS_CUDA_TRY(cudaMemsetAsync(p->flags, 0, 2 * sizeof(int), st));
   EGS_CUDA_TRY(cudaMemcpyAsync(p->z, p->zcpy, p->np * sizeof(double), cudaMemcpyDeviceToDevice, st));
   int sp = span_begin(p, EGS_STAGE_GENERATE);
-  launch_matern_mixed(p->band_pool, p->off_pool, p->x, p->y, n, ts, p->gen_tiles, p->ngen, p->dparams, p->ktab, st);
+  launch_matern_mixed(p->band_pool, p->off_pool, p->x, p->y, p->n, p->ts, p->gen_tiles, p->ngen, p->dparams,
+                      p->ktab, st);
   count_launches(p, EGS_STAGE_GENERATE, 1 + (p->ngen + 65534) / 65535);
   span_end(p, sp, 0.0);
-  for (int k = 0; k < nt; ++k) {
-    const int ntp = nt - k;
-    sp = span_begin(p, EGS_STAGE_PANEL);
-    launch_gather_column(p->band_pool, p->off_pool, p->W, ts, nt, b, k, st);
-    long long nl = 1;
-    // W holds tile column k and an identity tile as a one-column problem of
-    // ntp + 1 tiles; the solve of the identity row gives L_kk^-T
-    if (int rc = enqueue_panel(p->W, p->tmapW, ts, ntp + 1, 0, k * ts, info, err, st, &nl)) return rc;
-    launch_scatter_column(p->W, p->band_pool, p->off_pool, p->inv_pool, ts, nt, b, k, st);
-    ++nl;
-    if (ntp > 1) {
-      launch_panel_split(p->W, ts, 1, ntp - 1, k, p->inv_scale, p->ph, p->pl, st);
-      nl += 2;
-    }
-    count_launches(p, EGS_STAGE_PANEL, nl);
-    {
-      const double wd = (double)std::min(ts, n - k * ts);
-      const double below = (double)std::max(0, n - (k + 1) * ts);
-      span_end(p, sp, wd * wd * wd / 3.0 + wd * wd / 2.0 + wd / 6.0 + below * wd * wd);
-    }
-    if (ntp > 1) {
-      // FP64 band targets: tile rows j .. min(nt-1, j+b) of every column j > k
-      sp = span_begin(p, EGS_STAGE_UPDATE);
-      if (p->band_method == EGS_BAND_OZAKI_INT8) {
-        const egs_problem::OzLaunch& O = p->oz_launch[k];
-        if (O.count > 0) {
-          launch_ozaki_slice(p->W, ts, 1, ntp - 1, k, p->oz_scale, p->oz_slices, p->np, st);
-          int rc = launch_ozaki_band(p->tm_oz, p->oz_targets + O.off, O.count, O.items, ts, b, p->band_pool,
-                                     p->oz_scale, err, st);
-          if (rc != EGS_OK) return rc;
-          count_launches(p, EGS_STAGE_UPDATE, 3);
-        }
-      } else {
-        const egs_problem::JobLaunch& L = p->band_launch[k];
-        if (L.njobs > 0 && L.total > 0) {
-          int rc = launch_gemm_batched(p->tmapW, p->band_pool, p->band_jobs + L.job_off,
-                                       p->band_begin + L.begin_off, L.njobs, L.total, err, st);
-          if (rc != EGS_OK) return rc;
-          count_launches(p, EGS_STAGE_UPDATE, 1);
-        }
-      }
-      double band_tiles = 0.0;
-      for (int j = k + 1; j < nt; ++j) band_tiles += (double)(std::min(nt - 1, j + b) - j + 1);
-      span_end(p, sp, 2.0 * band_tiles * (double)ts * ts * ts);
-      const long long off_targets = split_targets(nt, b, k);
-      if (off_targets > 0) {
-        sp = span_begin(p, EGS_STAGE_UPDATE_LOW);
-        int rc = launch_split_update(p->tm_hi, p->tm_lo, p->tm_c, p->tm_cr, ts, nt, b, k, p->off_pool, p->inv_scale,
-                                     err, st);
-        if (rc != EGS_OK) return rc;
-        count_launches(p, EGS_STAGE_UPDATE_LOW, 1);
-        span_end(p, sp, 2.0 * (double)off_targets * (double)ts * ts * ts);
-      }
-    }
-  }
-  sp = span_begin(p, EGS_STAGE_REDUCE);
+  return EGS_OK;
+}
+
+// Log-det, the two solves with the refinement residual, the assembly and the
+// copies of the result record: the tail of every mixed evaluation.
+static int enqueue_mixed_tail(egs_problem* p) {
+  cudaStream_t st = p->stream;
+  const int ts = p->ts, nt = p->nt, n = p->n, b = p->mband;
+  int sp = span_begin(p, EGS_STAGE_REDUCE);
   launch_logdet_band(p->band_pool, ts, nt, b, n, p->partial, st);
   count_launches(p, EGS_STAGE_REDUCE, 1);
   span_end(p, sp, 0.0);
@@ -616,6 +605,136 @@ int enqueue_eval_mixed(egs_problem* p) {
   EGS_CUDA_TRY(cudaMemcpyAsync(p->hflags, p->flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
   EGS_CUDA_TRY(cudaMemcpyAsync(p->hresult, p->result, 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
   return check_cuda("egs_mle_eval (mixed)");
+}
+
+// Short panel of step k on stream s: gather the diagonal tile, the band tiles
+// and an identity tile into W2, factor and solve them with the FP64 panel
+// kernels (the identity row becomes L_kk^-T), scatter back.  max_ctas bounds
+// the persistent update kernels of the panel (look-ahead on spare SMs).
+static int enqueue_short_panel(egs_problem* p, int k, cudaStream_t s, int max_ctas) {
+  const int ts = p->ts, nt = p->nt, b = p->mband;
+  const int nb = std::min(b, nt - k - 1);
+  int sp = span_begin(p, EGS_STAGE_PANEL, s);
+  long long nl = 0;
+  launch_gather_panel(p->band_pool, p->W2, ts, b, nb, k, s);
+  if (int rc = enqueue_panel(p->W2, p->tmapW2, ts, nb + 2, 0, k * ts, p->flags, p->flags + 1, s, &nl, max_ctas))
+    return rc;
+  launch_scatter_panel(p->W2, p->band_pool, p->inv_pool, p->W, ts, b, nb, k, s);
+  count_launches(p, EGS_STAGE_PANEL, nl + 2);
+  span_end(p, sp, panel_flops(ts, p->n, k), s);
+  return EGS_OK;
+}
+
+// Mixed-precision evaluation, Ozaki form.  Step k on the problem stream: solve
+// the off-band rows of tile column k as one product with L_kk^-1 on the int8
+// tensor cores (read from the FP32 pool, written to W in FP64, rounded back),
+// split the panel rows to FP16, update the FP64 band (Ozaki) and, on all but
+// lookahead_sms SMs, the off-band targets (split-FP16).  The short FP64 panel
+// of step k+1 (diagonal tile, band rows, L^-T) needs only the band update of
+// step k, so it runs on the side stream during the off-band update of step k.
+int enqueue_eval_mixed_ozaki(egs_problem* p) {
+  cudaStream_t st = p->stream, side = p->side;
+  const int ts = p->ts, nt = p->nt, b = p->mband;
+  int* err = p->flags + 1;
+  if (int rc = enqueue_mixed_head(p)) return rc;
+  if (int rc = enqueue_short_panel(p, 0, st, 0)) return rc;
+  for (int k = 0; k < nt; ++k) {
+    const int ntp = nt - k;
+    const int nb = std::min(b, ntp - 1);
+    if (k > 0) EGS_CUDA_TRY(cudaStreamWaitEvent(st, p->ev_panel, 0));
+    int sp = span_begin(p, EGS_STAGE_PANEL);
+    long long nl = 0;
+    const egs_problem::OzLaunch& T = p->oz_trsm_launch[k];
+    if (T.count > 0) {
+      const long long srows = (long long)p->np + ts;
+      launch_ozaki_slice_f32(offband_tile(p->off_pool, ts, nt, b, k + nb + 1, k), ts, T.count, k + nb + 1,
+                             p->oz_scale, p->oz_slices, srows, st);
+      launch_ozaki_slice_rows(p->W2 + (size_t)(nb + 1) * ts * ts, ts, p->np, p->oz_scale, p->oz_slices, srows, st);
+      if (int rc = launch_ozaki_trsm(p->tm_oz, p->oz_trsm_targets + T.off, T.count, T.items, ts, k, p->np, p->W,
+                                     p->oz_scale, err, st))
+        return rc;
+      launch_scatter_offband(p->W, p->off_pool, ts, nt, b, nb, k, st);
+      nl += 6;
+    }
+    if (ntp > 1) {
+      launch_panel_split(p->W, ts, 1, ntp - 1, k, p->inv_scale, p->ph, p->pl, st);
+      nl += 2;
+    }
+    count_launches(p, EGS_STAGE_PANEL, nl);
+    span_end(p, sp, 0.0);
+    if (ntp <= 1) continue;
+    sp = span_begin(p, EGS_STAGE_UPDATE);
+    const egs_problem::OzLaunch& O = p->oz_launch[k];
+    if (O.count > 0) {
+      launch_ozaki_slice(p->W, ts, 1, ntp - 1, k, p->oz_scale, p->oz_slices, (long long)p->np + ts, st);
+      if (int rc = launch_ozaki_band(p->tm_oz, p->oz_targets + O.off, O.count, O.items, ts, b, p->band_pool,
+                                     p->oz_scale, err, st))
+        return rc;
+      count_launches(p, EGS_STAGE_UPDATE, 3);
+    }
+    span_end(p, sp, band_update_flops(ts, nt, b, k));
+    const int la = p->lookahead_sms;
+    if (la > 0) {
+      // look-ahead: the next short panel beside the off-band update
+      EGS_CUDA_TRY(cudaEventRecord(p->ev_band, st));
+      EGS_CUDA_TRY(cudaStreamWaitEvent(side, p->ev_band, 0));
+      if (int rc = enqueue_short_panel(p, k + 1, side, la)) return rc;
+      EGS_CUDA_TRY(cudaEventRecord(p->ev_panel, side));
+      if (int rc = enqueue_offband_update(p, k, st, gemm_num_sms() - la)) return rc;
+    } else {
+      if (int rc = enqueue_offband_update(p, k, st, 0)) return rc;
+      if (int rc = enqueue_short_panel(p, k + 1, st, 0)) return rc;
+      EGS_CUDA_TRY(cudaEventRecord(p->ev_panel, st));
+    }
+  }
+  return enqueue_mixed_tail(p);
+}
+
+// Mixed-precision evaluation, FP64-DMMA form.  Step k: gather tile column k into
+// the FP64 workspace W, factor and solve it there (the FP64 panel kernels with W
+// as a one-column problem, plus an identity row that becomes L_kk^-T), scatter
+// it back (off-band tiles rounded to FP32), split its rows for the FP16
+// tensor-core update, then update the band targets with FP64 DMMA and the
+// off-band targets with the split tcgen05 kernel.  After the factorisation:
+// log-det from the FP64 diagonal tiles, v = (L L^T)^-1 z, one refinement step
+// with the FP64 residual z - C v, and the assembly with z^T (v + w).
+int enqueue_eval_mixed(egs_problem* p) {
+  if (p->band_method == EGS_BAND_OZAKI_INT8) return enqueue_eval_mixed_ozaki(p);
+  cudaStream_t st = p->stream;
+  const int ts = p->ts, nt = p->nt, n = p->n, b = p->mband;
+  int* info = p->flags;
+  int* err = p->flags + 1;
+  if (int rc = enqueue_mixed_head(p)) return rc;
+  for (int k = 0; k < nt; ++k) {
+    const int ntp = nt - k;
+    int sp = span_begin(p, EGS_STAGE_PANEL);
+    long long nl = 0;
+    launch_gather_column(p->band_pool, p->off_pool, p->W, ts, nt, b, k, st);
+    ++nl;
+    // W holds tile column k and an identity tile as a one-column problem of
+    // ntp + 1 tiles; the solve of the identity row gives L_kk^-T
+    if (int rc = enqueue_panel(p->W, p->tmapW, ts, ntp + 1, 0, k * ts, info, err, st, &nl)) return rc;
+    launch_scatter_column(p->W, p->band_pool, p->off_pool, p->inv_pool, ts, nt, b, k, st);
+    ++nl;
+    if (ntp > 1) {
+      launch_panel_split(p->W, ts, 1, ntp - 1, k, p->inv_scale, p->ph, p->pl, st);
+      nl += 2;
+    }
+    count_launches(p, EGS_STAGE_PANEL, nl);
+    span_end(p, sp, panel_flops(ts, n, k));
+    if (ntp <= 1) continue;
+    sp = span_begin(p, EGS_STAGE_UPDATE);
+    const egs_problem::JobLaunch& L = p->band_launch[k];
+    if (L.njobs > 0 && L.total > 0) {
+      int rc = launch_gemm_batched(p->tmapW, p->band_pool, p->band_jobs + L.job_off, p->band_begin + L.begin_off,
+                                   L.njobs, L.total, err, st);
+      if (rc != EGS_OK) return rc;
+      count_launches(p, EGS_STAGE_UPDATE, 1);
+    }
+    span_end(p, sp, band_update_flops(ts, nt, b, k));
+    if (int rc = enqueue_offband_update(p, k, st, 0)) return rc;
+  }
+  return enqueue_mixed_tail(p);
 }
 
 // Re-lays a problem out for mixed precision: device tile rounded up to a
@@ -706,16 +825,39 @@ int setup_mixed(egs_problem* p, int b) {
       const long long items = ozaki_targets(ts, nt, b, k, targets);
       p->oz_launch.push_back({off, (int)((long long)targets.size() - off), items});
     }
-    if ((rc = dev_alloc(&p->oz_slices, (size_t)p->np * ts * ozaki_slices(), &p->bytes, p->stream)) ||
-        (rc = dev_alloc(&p->oz_scale, (size_t)p->np, &p->bytes, p->stream)) ||
-        (rc = dev_alloc(&p->oz_targets, std::max<size_t>(1, targets.size()), &p->bytes, p->stream)))
+    // panel solve of the off-band rows through L_kk^-1: tiles k+b+1 .. nt-1
+    std::vector<int4> tt;
+    p->oz_trsm_launch.clear();
+    for (int k = 0; k < nt; ++k) {
+      const long long off = (long long)tt.size();
+      const long long items = ozaki_trsm_targets(ts, nt, k + b + 1, tt);
+      p->oz_trsm_launch.push_back({off, (int)((long long)tt.size() - off), items});
+    }
+    // slice rows: every panel row, then ts rows for L_kk^-1
+    const long long srows = (long long)p->np + ts;
+    if ((rc = dev_alloc(&p->oz_slices, (size_t)srows * ts * ozaki_slices(), &p->bytes, p->stream)) ||
+        (rc = dev_alloc(&p->oz_scale, (size_t)srows, &p->bytes, p->stream)) ||
+        (rc = dev_alloc(&p->oz_targets, std::max<size_t>(1, targets.size()), &p->bytes, p->stream)) ||
+        (rc = dev_alloc(&p->oz_trsm_targets, std::max<size_t>(1, tt.size()), &p->bytes, p->stream)) ||
+        (rc = dev_alloc(&p->W2, (size_t)(b + 2) * ts2, &p->bytes, p->stream)))
       return rc;
     if (!targets.empty())
       EGS_CUDA_TRY(cudaMemcpyAsync(p->oz_targets, targets.data(), targets.size() * sizeof(int4),
                                    cudaMemcpyHostToDevice, p->stream));
+    if (!tt.empty())
+      EGS_CUDA_TRY(cudaMemcpyAsync(p->oz_trsm_targets, tt.data(), tt.size() * sizeof(int4), cudaMemcpyHostToDevice,
+                                   p->stream));
     EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
-    if ((rc = ozaki_tensor_map(p->tm_oz, p->oz_slices, ts, p->np)) != EGS_OK) return rc;
-    EGS_CUDA_TRY(cudaMemsetAsync(p->oz_scale, 0, p->np * sizeof(double), p->stream));
+    if ((rc = ozaki_tensor_map(p->tm_oz, p->oz_slices, ts, srows)) != EGS_OK) return rc;
+    if ((rc = gemm_init_tensor_map(p->tmapW2, p->W2, ts, b + 2)) != EGS_OK) return rc;
+    EGS_CUDA_TRY(cudaMemsetAsync(p->oz_scale, 0, srows * sizeof(double), p->stream));
+    if (cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&p->ev_band, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&p->ev_panel, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      set_last_error("stream or event creation failed", "egs_problem_set_precision");
+      return EGS_ERR_CUDA;
+    }
   }
   if ((rc = gemm_init_tensor_map(p->tmapW, p->W, ts, nt + 1)) != EGS_OK ||
       (rc = split_tensor_map(p->tm_hi, p->ph, ts, p->np)) != EGS_OK ||
@@ -947,6 +1089,18 @@ int egs_problem_set_precision(egs_problem* p, int precision, int band_tiles) {
     p->precision = kPrecisionBroken;
   }
   return rc;
+}
+
+int egs_problem_set_lookahead(egs_problem* p, int sms) {
+  if (!p || sms < 0 || sms >= gemm_num_sms()) return EGS_ERR_INVALID;
+  if (sms == p->lookahead_sms) return EGS_OK;
+  EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  if (p->graph_exec) cudaGraphExecDestroy(p->graph_exec);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  p->graph_exec = nullptr;
+  p->graph = nullptr;
+  p->lookahead_sms = sms;
+  return EGS_OK;
 }
 
 int egs_problem_set_band_method(egs_problem* p, int method) {

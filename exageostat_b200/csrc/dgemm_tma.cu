@@ -420,14 +420,15 @@ void finish_desc(GemmDesc& d) {
   d.total = total;
 }
 
-static int launch_desc(const void* tmap, double* tiles, GemmDesc& d, int* err, cudaStream_t st) {
+static int launch_desc(const void* tmap, double* tiles, GemmDesc& d, int* err, cudaStream_t st, int max_ctas = 0) {
   using namespace gemm;
   if (d.M <= 0 || d.N <= 0 || d.K <= 0) return EGS_OK;
   if (d.K % BK != 0) return EGS_ERR_INVALID;
   finish_desc(d);
   const long long total = d.total;
   set_gemm_smem_attributes();
-  const long long grid = total < gemm_num_sms() ? total : gemm_num_sms();
+  const long long cap = (max_ctas > 0 && max_ctas < gemm_num_sms()) ? max_ctas : gemm_num_sms();
+  const long long grid = total < cap ? total : cap;
   GemmJobs none{nullptr, nullptr, 0, 0};
   dgemm_update_kernel<false><<<(unsigned)grid, THREADS, SMEM_BYTES, st>>>(
       *reinterpret_cast<const CUtensorMap*>(tmap), tiles, d, none, err);
@@ -453,7 +454,7 @@ int launch_gemm_trailing(const void* tmap, double* tiles, int ts, int nt, int k,
 // General form used by the panel factorisation (see kernels.cuh).
 int launch_gemm_rows(const void* tmap, double* tiles, int ts, int nt, int M, int N, int K, int a_row0,
                      int a_col0, int a_tcol, int b_row0, int b_col0, int b_tcol, int c_row0, int c_col0,
-                     int lower, int* err, cudaStream_t st) {
+                     int lower, int* err, cudaStream_t st, int max_ctas) {
   GemmDesc d{};
   d.ts = ts;
   d.nt = nt;
@@ -470,7 +471,7 @@ int launch_gemm_rows(const void* tmap, double* tiles, int ts, int nt, int M, int
   d.c_row0 = c_row0;
   d.c_col0 = c_col0;
   d.lower = lower;
-  return launch_desc(tmap, tiles, d, err, st);
+  return launch_desc(tmap, tiles, d, err, st, max_ctas);
 }
 
 }  // namespace egs

@@ -72,7 +72,7 @@ int tensor_map_encoder(void** fn);
 int launch_gemm_trailing(const void* tmap, double* tiles, int ts, int nt, int k, int* err, cudaStream_t st);
 int launch_gemm_rows(const void* tmap, double* tiles, int ts, int nt, int M, int N, int K, int a_row0,
                      int a_col0, int a_tcol, int b_row0, int b_col0, int b_tcol, int c_row0, int c_col0,
-                     int lower, int* err, cudaStream_t st);
+                     int lower, int* err, cudaStream_t st, int max_ctas = 0);
 int gemm_num_sms();
 
 // Mixed-precision evaluation (mixed.cu, split_gemm.cu).
@@ -86,6 +86,11 @@ void launch_scatter_column(const double* W, double* band, float* off, double* in
 void launch_logdet_band(const double* band, int ts, int nt, int b, int n, double* partial, cudaStream_t st);
 void launch_mixed_solve(const double* band, const float* off, const double* inv, int ts, int nt, int b, double* v,
                         double* tmp, cudaStream_t st, long long* launches);
+void launch_gather_panel(const double* band, double* W2, int ts, int b, int nb, int k, cudaStream_t st);
+void launch_scatter_panel(const double* W2, double* band, double* inv, double* W, int ts, int b, int nb, int k,
+                          cudaStream_t st);
+void launch_scatter_offband(const double* W, float* off, int ts, int nt, int b, int nb, int k, cudaStream_t st);
+const float* offband_tile(const float* off, int ts, int nt, int b, int i, int k);
 long long residual_scratch_doubles(int n);
 void launch_add_inplace(double* a, const double* b, int n, cudaStream_t st);
 void launch_matern_residual(const double* x, const double* y, const double* z, const double* v, int n, int np,
@@ -106,10 +111,17 @@ void launch_ozaki_slice(const double* W, int ts, int t0, int ntiles, int row_til
 #include <vector>
 namespace egs {
 long long ozaki_targets(int ts, int nt, int band, int k, std::vector<int4>& out);
+long long ozaki_trsm_targets(int ts, int nt, int first, std::vector<int4>& out);
+void launch_ozaki_slice_f32(const float* tiles0, int ts, int ntiles, int row_tile0, double* scale, int8_t* slices,
+                            long long rows, cudaStream_t st);
+void launch_ozaki_slice_rows(const double* src, int ts, long long row0, double* scale, int8_t* slices,
+                             long long rows, cudaStream_t st);
+int launch_ozaki_trsm(const void* tm_s, const int4* targets, int ntargets, long long total, int ts, int k,
+                      long long b_row_base, double* w_out, const double* scale, int* err, cudaStream_t st);
 int launch_ozaki_band(const void* tm_s, const int4* targets, int ntargets, long long total, int ts, int band,
                       double* band_pool, const double* scale, int* err, cudaStream_t st);
 int launch_split_update(const void* tm_hi, const void* tm_lo, const void* tm_c, const void* tm_cr, int ts, int nt,
                         int band, int k, float* c_pool,
-                        const float* inv_scale, int* err, cudaStream_t st);
+                        const float* inv_scale, int* err, cudaStream_t st, int max_ctas = 0);
 
 }  // namespace egs

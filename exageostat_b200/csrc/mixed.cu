@@ -117,6 +117,72 @@ void launch_scatter_column(const double* W, double* band, float* off, double* in
   scatter_column_kernel<<<dim3(gx, nt - k + 1), 256, 0, st>>>(W, band, off, inv, ts, nt, b, k);
 }
 
+// Short panel of the Ozaki form: W2[0 .. nb] = tiles (k .. k+nb, k) from the
+// FP64 band pool, W2[nb+1] = identity (nb = min(b, nt-k-1)).
+__global__ void __launch_bounds__(256)
+gather_panel_kernel(const double* __restrict__ band, double* __restrict__ W2, int ts, int b, int nb, int k) {
+  const int t = blockIdx.y;
+  const long long e = ((long long)blockIdx.x * 256 + threadIdx.x) * 2;
+  if (e >= (long long)ts * ts) return;
+  double2 v;
+  if (t == nb + 1) {
+    const long long c = e / ts, r = e - c * ts;
+    v = make_double2(r == c ? 1.0 : 0.0, r + 1 == c ? 1.0 : 0.0);
+  } else {
+    v = *reinterpret_cast<const double2*>(band + band_slot(k + t, k, b) * ts * ts + e);
+  }
+  *reinterpret_cast<double2*>(W2 + (long long)t * ts * ts + e) = v;
+}
+
+// W2[0 .. nb] back to the band pool (and W2[1 .. nb] into W[1 .. nb] for the
+// split and slicing of the whole panel); W2[nb+1] = L_kk^-T to inverse slot k.
+__global__ void __launch_bounds__(256)
+scatter_panel_kernel(const double* __restrict__ W2, double* __restrict__ band, double* __restrict__ inv,
+                     double* __restrict__ W, int ts, int b, int nb, int k) {
+  const int t = blockIdx.y;
+  const long long e = ((long long)blockIdx.x * 256 + threadIdx.x) * 2;
+  if (e >= (long long)ts * ts) return;
+  const double2 v = *reinterpret_cast<const double2*>(W2 + (long long)t * ts * ts + e);
+  if (t == nb + 1) {
+    *reinterpret_cast<double2*>(inv + (long long)k * ts * ts + e) = v;
+  } else {
+    *reinterpret_cast<double2*>(band + band_slot(k + t, k, b) * ts * ts + e) = v;
+    if (t > 0) *reinterpret_cast<double2*>(W + (long long)t * ts * ts + e) = v;
+  }
+}
+
+// Off-band tiles W[nb+1 .. nt-k-1] = (k+nb+1 .. nt-1, k) rounded into the FP32 pool.
+__global__ void __launch_bounds__(256)
+scatter_offband_kernel(const double* __restrict__ W, float* __restrict__ off, int ts, int nt, int b, int nb, int k) {
+  const int t = nb + 1 + blockIdx.y;
+  const long long e = ((long long)blockIdx.x * 256 + threadIdx.x) * 2;
+  if (e >= (long long)ts * ts) return;
+  const double2 v = *reinterpret_cast<const double2*>(W + (long long)t * ts * ts + e);
+  *reinterpret_cast<float2*>(off + off_slot(k + t, k, nt, b) * ts * ts + e) = make_float2((float)v.x, (float)v.y);
+}
+
+void launch_gather_panel(const double* band, double* W2, int ts, int b, int nb, int k, cudaStream_t st) {
+  const unsigned gx = (unsigned)(((long long)ts * ts / 2 + 255) / 256);
+  gather_panel_kernel<<<dim3(gx, nb + 2), 256, 0, st>>>(band, W2, ts, b, nb, k);
+}
+
+void launch_scatter_panel(const double* W2, double* band, double* inv, double* W, int ts, int b, int nb, int k,
+                          cudaStream_t st) {
+  const unsigned gx = (unsigned)(((long long)ts * ts / 2 + 255) / 256);
+  scatter_panel_kernel<<<dim3(gx, nb + 2), 256, 0, st>>>(W2, band, inv, W, ts, b, nb, k);
+}
+
+void launch_scatter_offband(const double* W, float* off, int ts, int nt, int b, int nb, int k, cudaStream_t st) {
+  const int count = nt - k - 1 - nb;
+  if (count <= 0) return;
+  const unsigned gx = (unsigned)(((long long)ts * ts / 2 + 255) / 256);
+  scatter_offband_kernel<<<dim3(gx, count), 256, 0, st>>>(W, off, ts, nt, b, nb, k);
+}
+
+const float* offband_tile(const float* off, int ts, int nt, int b, int i, int k) {
+  return off + off_slot(i, k, nt, b) * (long long)ts * ts;
+}
+
 // ---------------------------------------------------------------------------
 // Reductions and solves
 // ---------------------------------------------------------------------------

@@ -65,56 +65,50 @@ constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >
 // Slicing of the solved panel
 // ---------------------------------------------------------------------------
 
-// Row scale of panel tile t (rows of W tile t0 + blockIdx.y): scale = 2^e with
-// max_c |W(r, c)| < 2^e (e from the maximum's exponent + 1); 0 rows get scale 0.
+__device__ __forceinline__ double oz_row_scale(double m) {
+  if (!(m > 0.0)) return (m == 0.0) ? 0.0 : __longlong_as_double(0x7ff8000000000000ll);  // NaN rows stay NaN
+  const long long bits = __double_as_longlong(m);
+  const int e = (int)((bits >> 52) & 0x7FF) - 1023;  // 2^e <= m < 2^(e+1) for normal m
+  return (e >= 1023) ? __longlong_as_double(0x7ff8000000000000ll) : ldexp(1.0, e + 1);
+}
+
+// Row scale of column-major tile t (tiles0 + t ts^2, global tile row
+// row_tile0 + t): scale = 2^e with max_c |A(r, c)| < 2^e; 0 rows get scale 0.
+template <typename T>
 __global__ void __launch_bounds__(256)
-ozaki_rowscale_kernel(const double* __restrict__ W, int ts, int t0, int row_tile0, double* __restrict__ scale) {
+ozaki_rowscale_kernel(const T* __restrict__ tiles0, int ts, int row_tile0, double* __restrict__ scale) {
   __shared__ double red[4][64];
-  const int t = t0 + blockIdx.y;
+  const int t = blockIdx.y;
   const int rl = threadIdx.x & 63, g = threadIdx.x >> 6;
   const int r = blockIdx.x * 64 + rl;
-  const double* col = W + (long long)t * ts * ts + r;
+  const T* col = tiles0 + (long long)t * ts * ts + r;
   double m = 0.0;
-  for (int c = g; c < ts; c += 4) m = fmax(m, fabs(col[(long long)c * ts]));
+  for (int c = g; c < ts; c += 4) m = fmax(m, fabs((double)col[(long long)c * ts]));
   red[g][rl] = m;
   __syncthreads();
   if (g == 0) {
     m = fmax(fmax(red[0][rl], red[1][rl]), fmax(red[2][rl], red[3][rl]));
-    double sc;
-    if (!(m > 0.0)) {
-      sc = (m == 0.0) ? 0.0 : __longlong_as_double(0x7ff8000000000000ll);  // NaN rows stay NaN
-    } else {
-      const long long bits = __double_as_longlong(m);
-      const int e = (int)((bits >> 52) & 0x7FF) - 1023;  // 2^e <= m < 2^(e+1) for normal m
-      sc = (e >= 1023) ? __longlong_as_double(0x7ff8000000000000ll) : ldexp(1.0, e + 1);
-    }
-    scale[(long long)(row_tile0 + t) * ts + r] = sc;
+    scale[(long long)(row_tile0 + t) * ts + r] = oz_row_scale(m);
   }
 }
 
-// Slices of 64 x 64 blocks of panel tiles, transposed to row-major int8 rows
-// (K contiguous): slices[p][row][c], p = 0..S-1 for 2^-7 .. 2^-7S.
+// Row scale of ts rows stored row by row (row r at src + r ts), written to
+// scale[row0 + r]: one warp per row.
 __global__ void __launch_bounds__(256)
-ozaki_slice_kernel(const double* __restrict__ W, int ts, int t0, int row_tile0, const double* __restrict__ scale,
-                   int8_t* __restrict__ slices, long long slice_stride) {
-  __shared__ double Sm[64][65];
-  const int t = t0 + blockIdx.z;
-  const int r0 = blockIdx.x * 64, c0 = blockIdx.y * 64;
-  const double* src = W + (long long)t * ts * ts;
-  for (int e = threadIdx.x; e < 64 * 64; e += 256) {
-    const int r = e & 63, c = e >> 6;
-    Sm[r][c] = src[(long long)(c0 + c) * ts + r0 + r];
-  }
-  __syncthreads();
-  const long long grow0 = (long long)(row_tile0 + t) * ts + r0;
-  // thread: row r, 16 consecutive columns (16-byte stores per slice)
-  const int r = threadIdx.x >> 2, cq = (threadIdx.x & 3) * 16;
-  const double sc = scale[grow0 + r];
-  const double inv = (sc > 0.0) ? 1.0 / sc : 0.0;  // exact: a power of two
-  double v[16];
+ozaki_rowscale_rm_kernel(const double* __restrict__ src, int ts, long long row0, double* __restrict__ scale) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int r = blockIdx.x * 8 + warp;
+  if (r >= ts) return;
+  const double* row = src + (long long)r * ts;
+  double m = 0.0;
+  for (int c = lane; c < ts; c += 32) m = fmax(m, fabs(row[c]));
 #pragma unroll
-  for (int c = 0; c < 16; ++c) v[c] = Sm[r][cq + c] * inv;  // |v| < 1
-  int8_t* dst = slices + (grow0 + r) * ts + c0 + cq;
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (lane == 0) scale[row0 + r] = oz_row_scale(m);
+}
+
+// S slices of 16 values (|v| < 1 after scaling) into 16-byte stores.
+__device__ __forceinline__ void oz_emit_slices(double (&v)[16], int8_t* dst, long long slice_stride) {
 #pragma unroll
   for (int p = 0; p < oz::S; ++p) {
     union {
@@ -130,6 +124,50 @@ ozaki_slice_kernel(const double* __restrict__ W, int ts, int t0, int row_tile0, 
     }
     *reinterpret_cast<int4*>(dst + p * slice_stride) = out.q;
   }
+}
+
+// Slices of rows stored row by row (row r at src + r ts) into slice rows row0 + r.
+__global__ void __launch_bounds__(256)
+ozaki_slice_rm_kernel(const double* __restrict__ src, int ts, long long row0, const double* __restrict__ scale,
+                      int8_t* __restrict__ slices, long long slice_stride) {
+  const long long idx = (long long)blockIdx.x * 256 + threadIdx.x;  // one 16-column chunk
+  const int chunks = ts / 16;
+  const int r = (int)(idx / chunks), cq = (int)(idx % chunks) * 16;
+  if (r >= ts) return;
+  const double sc = scale[row0 + r];
+  const double inv = (sc > 0.0) ? 1.0 / sc : 0.0;  // exact: a power of two
+  const double* row = src + (long long)r * ts + cq;
+  double v[16];
+#pragma unroll
+  for (int c = 0; c < 16; ++c) v[c] = row[c] * inv;
+  oz_emit_slices(v, slices + (row0 + r) * ts + cq, slice_stride);
+}
+
+// Slices of 64 x 64 blocks of column-major tiles (tiles0 + t ts^2, global tile
+// row row_tile0 + t), transposed to row-major int8 rows (K contiguous):
+// slices[p][row][c], p = 0..S-1 for 2^-7 .. 2^-7S.
+template <typename T>
+__global__ void __launch_bounds__(256)
+ozaki_slice_kernel(const T* __restrict__ tiles0, int ts, int row_tile0, const double* __restrict__ scale,
+                   int8_t* __restrict__ slices, long long slice_stride) {
+  __shared__ double Sm[64][65];
+  const int t = blockIdx.z;
+  const int r0 = blockIdx.x * 64, c0 = blockIdx.y * 64;
+  const T* src = tiles0 + (long long)t * ts * ts;
+  for (int e = threadIdx.x; e < 64 * 64; e += 256) {
+    const int r = e & 63, c = e >> 6;
+    Sm[r][c] = (double)src[(long long)(c0 + c) * ts + r0 + r];
+  }
+  __syncthreads();
+  const long long grow0 = (long long)(row_tile0 + t) * ts + r0;
+  // thread: row r, 16 consecutive columns (16-byte stores per slice)
+  const int r = threadIdx.x >> 2, cq = (threadIdx.x & 3) * 16;
+  const double sc = scale[grow0 + r];
+  const double inv = (sc > 0.0) ? 1.0 / sc : 0.0;  // exact: a power of two
+  double v[16];
+#pragma unroll
+  for (int c = 0; c < 16; ++c) v[c] = Sm[r][cq + c] * inv;  // |v| < 1
+  oz_emit_slices(v, slices + (grow0 + r) * ts + c0 + cq, slice_stride);
 }
 
 // ---------------------------------------------------------------------------
@@ -182,13 +220,19 @@ __device__ __forceinline__ void tmem_ld16_i32(uint32_t taddr, int (&v)[16]) {
 // items of an off-diagonal target: MB x NB tiles (row block fastest); of a
 // diagonal target: the tiles touching the lower triangle, nb <= 2 mb + 1,
 // enumerated row block by row block.
+// mode 0 (band update): targets (i, j): C_ij -= A_i A_j^T into the band pool.
+// mode 1 (panel solve through the inverse): targets (i, -): W[i - k] =
+// A_i B^T, B = rows b_row_base .. + ts of the slice storage (rows of L_kk^-1).
 struct OzStep {
   const int4* targets;
   int ntargets;
   long long total;
   int ts, band;
+  int mode, k;
+  long long b_row_base;
   double* band_pool;
-  const double* scale;   // per global panel row
+  double* w_out;
+  const double* scale;   // per slice row
   int* err;
 };
 
@@ -256,7 +300,8 @@ ozaki_band_kernel(const __grid_constant__ CUtensorMap tm_s, const __grid_constan
       for (long long L = blockIdx.x; L < P.total && !bail; L += gridDim.x) {
         int i, j, mb, nb;
         oz_decode(P, L, i, j, mb, nb);
-        const int arow = i * P.ts + mb * BM, brow = j * P.ts + nb * BN;
+        const int arow = i * P.ts + mb * BM;
+        const int brow = P.mode == 0 ? j * P.ts + nb * BN : (int)(P.b_row_base + nb * BN);
         for (int kt = 0; kt < ksteps; ++kt, ++it) {
           const uint32_t s = it % STAGES;
           if (it >= (uint32_t)STAGES && !mbar_wait(&empty[s], ((it / STAGES) & 1) ^ 1, P.err)) {
@@ -356,16 +401,23 @@ ozaki_band_kernel(const __grid_constant__ CUtensorMap tm_s, const __grid_constan
       const int r = mb * BM + quarter * 32 + lane;
       const int c0 = nb * BN + half * 32;
       const double sr = P.scale[(long long)i * P.ts + r];
-      const double* sc = P.scale + (long long)j * P.ts + c0;
-      double* C = P.band_pool + ((long long)j * (P.band + 1) + (i - j)) * P.ts * P.ts;
-      double* cp = C + (long long)c0 * P.ts + r;
-      const bool diag = (i == j);
+      if (P.mode == 0) {
+        const double* sc = P.scale + (long long)j * P.ts + c0;
+        double* C = P.band_pool + ((long long)j * (P.band + 1) + (i - j)) * P.ts * P.ts;
+        double* cp = C + (long long)c0 * P.ts + r;
+        const bool diag = (i == j);
 #pragma unroll
-      for (int c = 0; c < 32; ++c) {
-        if (!diag || r >= c0 + c) {
-          double* e = cp + (long long)c * P.ts;
-          *e -= acc[c] * (sr * __ldg(sc + c));
+        for (int c = 0; c < 32; ++c) {
+          if (!diag || r >= c0 + c) {
+            double* e = cp + (long long)c * P.ts;
+            *e -= acc[c] * (sr * __ldg(sc + c));
+          }
         }
+      } else {
+        const double* sc = P.scale + P.b_row_base + c0;
+        double* cp = P.w_out + (long long)(i - P.k) * P.ts * P.ts + (long long)c0 * P.ts + r;
+#pragma unroll
+        for (int c = 0; c < 32; ++c) cp[(long long)c * P.ts] = acc[c] * (sr * __ldg(sc + c));
       }
     }
     if (!ok) bail = 1;
@@ -406,12 +458,32 @@ int ozaki_tensor_map(void* storage, const int8_t* slices, int ts, long long rows
   return EGS_OK;
 }
 
+// Panel tiles W[t0 .. t0+ntiles) = global tile rows row_tile0 + t0 .. (column-major FP64).
 void launch_ozaki_slice(const double* W, int ts, int t0, int ntiles, int row_tile0, double* scale, int8_t* slices,
                         long long rows, cudaStream_t st) {
   if (ntiles <= 0) return;
-  ozaki_rowscale_kernel<<<dim3(ts / 64, ntiles), 256, 0, st>>>(W, ts, t0, row_tile0, scale);
-  ozaki_slice_kernel<<<dim3(ts / 64, ts / 64, ntiles), 256, 0, st>>>(W, ts, t0, row_tile0, scale, slices,
-                                                                      rows * (long long)ts);
+  const double* tiles0 = W + (long long)t0 * ts * ts;
+  ozaki_rowscale_kernel<double><<<dim3(ts / 64, ntiles), 256, 0, st>>>(tiles0, ts, row_tile0 + t0, scale);
+  ozaki_slice_kernel<double><<<dim3(ts / 64, ts / 64, ntiles), 256, 0, st>>>(tiles0, ts, row_tile0 + t0, scale,
+                                                                              slices, rows * (long long)ts);
+}
+
+// Contiguous FP32 column-major tiles (global tile rows row_tile0 ..).
+void launch_ozaki_slice_f32(const float* tiles0, int ts, int ntiles, int row_tile0, double* scale, int8_t* slices,
+                            long long rows, cudaStream_t st) {
+  if (ntiles <= 0) return;
+  ozaki_rowscale_kernel<float><<<dim3(ts / 64, ntiles), 256, 0, st>>>(tiles0, ts, row_tile0, scale);
+  ozaki_slice_kernel<float><<<dim3(ts / 64, ts / 64, ntiles), 256, 0, st>>>(tiles0, ts, row_tile0, scale, slices,
+                                                                             rows * (long long)ts);
+}
+
+// ts rows stored row by row at src into slice rows row0 .. row0 + ts.
+void launch_ozaki_slice_rows(const double* src, int ts, long long row0, double* scale, int8_t* slices,
+                             long long rows, cudaStream_t st) {
+  ozaki_rowscale_rm_kernel<<<(ts + 7) / 8, 256, 0, st>>>(src, ts, row0, scale);
+  const long long chunks = (long long)ts * (ts / 16);
+  ozaki_slice_rm_kernel<<<(unsigned)((chunks + 255) / 256), 256, 0, st>>>(src, ts, row0, scale, slices,
+                                                                          rows * (long long)ts);
 }
 
 // Target table of step k: band targets (i, j), k < j <= i <= min(nt-1, j+band),
@@ -432,28 +504,64 @@ long long ozaki_targets(int ts, int nt, int band, int k, std::vector<int4>& out)
   return items;
 }
 
-int launch_ozaki_band(const void* tm_s, const int4* targets, int ntargets, long long total, int ts, int band,
-                      double* band_pool, const double* scale, int* err, cudaStream_t st) {
+static int launch_ozaki(const void* tm_s, const OzStep& P, cudaStream_t st) {
   using namespace oz;
-  if (ts % BM != 0 || ts / BN > 2 * (ts / BM)) return EGS_ERR_INVALID;
-  if (total <= 0 || ntargets <= 0) return EGS_OK;
   static const bool attr = []() {
     cudaFuncSetAttribute(ozaki_band_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
     return true;
   }();
   (void)attr;
-  OzStep P;
+  const long long grid = P.total < gemm_num_sms() ? P.total : gemm_num_sms();
+  ozaki_band_kernel<<<(unsigned)grid, THREADS, SMEM_BYTES, st>>>(*reinterpret_cast<const CUtensorMap*>(tm_s), P);
+  return cudaGetLastError() == cudaSuccess ? EGS_OK : EGS_ERR_CUDA;
+}
+
+// Targets of the panel solve at step k: off-band tiles i = first .. nt-1, all
+// MB x NB items each.
+long long ozaki_trsm_targets(int ts, int nt, int first, std::vector<int4>& out) {
+  const int MB = ts / oz::BM, NB = ts / oz::BN;
+  long long items = 0;
+  for (int i = first; i < nt; ++i) {
+    out.push_back(make_int4(i, 0, (int)items, 0));
+    items += (long long)MB * NB;
+  }
+  return items;
+}
+
+int launch_ozaki_trsm(const void* tm_s, const int4* targets, int ntargets, long long total, int ts, int k,
+                      long long b_row_base, double* w_out, const double* scale, int* err, cudaStream_t st) {
+  if (ts % oz::BM != 0) return EGS_ERR_INVALID;
+  if (total <= 0 || ntargets <= 0) return EGS_OK;
+  OzStep P{};
+  P.targets = targets;
+  P.ntargets = ntargets;
+  P.total = total;
+  P.ts = ts;
+  P.mode = 1;
+  P.k = k;
+  P.b_row_base = b_row_base;
+  P.w_out = w_out;
+  P.scale = scale;
+  P.err = err;
+  return launch_ozaki(tm_s, P, st);
+}
+
+int launch_ozaki_band(const void* tm_s, const int4* targets, int ntargets, long long total, int ts, int band,
+                      double* band_pool, const double* scale, int* err, cudaStream_t st) {
+  using namespace oz;
+  if (ts % BM != 0 || ts / BN > 2 * (ts / BM)) return EGS_ERR_INVALID;
+  if (total <= 0 || ntargets <= 0) return EGS_OK;
+  OzStep P{};
   P.targets = targets;
   P.ntargets = ntargets;
   P.total = total;
   P.ts = ts;
   P.band = band;
+  P.mode = 0;
   P.band_pool = band_pool;
   P.scale = scale;
   P.err = err;
-  const long long grid = total < gemm_num_sms() ? total : gemm_num_sms();
-  ozaki_band_kernel<<<(unsigned)grid, THREADS, SMEM_BYTES, st>>>(*reinterpret_cast<const CUtensorMap*>(tm_s), P);
-  return cudaGetLastError() == cudaSuccess ? EGS_OK : EGS_ERR_CUDA;
+  return launch_ozaki(tm_s, P, st);
 }
 
 }  // namespace egs

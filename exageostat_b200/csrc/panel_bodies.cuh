@@ -22,13 +22,10 @@ __device__ __forceinline__ double block_sum_256(double v, double* red) {
 }
 
 // Cholesky of the 64x64 block at T (ld ts).  Every thread of the block (NTHR,
-// whole warps) takes part in moving the block between global
-// and shared memory with all loads issued before any is used; warp 0 factors
-// it: lane l owns rows l and l + 32.  Step j: every lane reads the pivot (a
-// broadcast), scales its entries of column j, and applies the rank-1 update to
-// its rows, reading L[c][j] as broadcasts; only __syncwarp separates the
-// steps.  info records the 1-based global column (gcol0 + j + 1) of the first
-// pivot that is not positive (or NaN).
+// whole warps) takes part in moving the block between global and shared memory,
+// with all loads issued before any is used.  Up to four warps factor it; lane l
+// of each owns rows l and l + 32.  info records the 1-based global column
+// (gcol0 + j + 1) of the first pivot that is not positive (or NaN).
 template <int NTHR>
 __device__ __forceinline__ void potrf64_body(double* __restrict__ T, int ts, int gcol0, int* __restrict__ info) {
   static_assert(NTHR % 32 == 0 && NTHR >= 32 && NTHR <= 1024, "whole warps");
@@ -50,30 +47,37 @@ __device__ __forceinline__ void potrf64_body(double* __restrict__ T, int ts, int
     }
   }
   __syncthreads();
-  if (threadIdx.x < 32) {
-    const int lane = threadIdx.x;
-    const int r0 = lane, r1 = lane + 32;
-    for (int j = 0; j < kNB; ++j) {
+  // Factorisation by CW warps: at step j every warp reads the pivot and column
+  // j (unscaled), and warp w applies the rank-1 update to the columns
+  // c > j with c % CW == w of its lanes' rows l and l + 32; after the step's
+  // barrier warp 0 stores the scaled column j (no warp reads it again).
+  constexpr int CW = NTHR / 32 < 4 ? NTHR / 32 : 4;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int r0 = lane, r1 = lane + 32;
+  for (int j = 0; j < kNB; ++j) {
+    double ljj = 0.0, l0 = 0.0, l1 = 0.0;
+    if (warp < CW) {
       const double d = S[j][j];
-      if (lane == 0 && !(d > 0.0)) atomicCAS(info, 0, gcol0 + j + 1);
-      const double ljj = sqrt(d);
+      if (threadIdx.x == 0 && !(d > 0.0)) atomicCAS(info, 0, gcol0 + j + 1);
+      ljj = sqrt(d);
       const double inv = 1.0 / ljj;
-      const double l0 = (r0 > j) ? S[r0][j] * inv : 0.0;
-      const double l1 = (r1 > j) ? S[r1][j] * inv : 0.0;
-      __syncwarp();
+      l0 = (r0 > j) ? S[r0][j] * inv : 0.0;
+      l1 = (r1 > j) ? S[r1][j] * inv : 0.0;
+      // first column of this warp after j
+      const int c1 = j + 1 + ((warp - (j + 1)) % CW + CW) % CW;
+#pragma unroll 4
+      for (int c = c1; c < kNB; c += CW) {
+        const double lcj = S[c][j] * inv;
+        if (r0 >= c) S[r0][c] = fma(-l0, lcj, S[r0][c]);
+        if (r1 >= c) S[r1][c] = fma(-l1, lcj, S[r1][c]);
+      }
+    }
+    __syncthreads();
+    if (warp == 0) {
       if (r0 > j) S[r0][j] = l0;
       if (r1 > j) S[r1][j] = l1;
       if (r0 == j) S[r0][j] = ljj;
       if (r1 == j) S[r1][j] = ljj;
-      __syncwarp();
-      // Independent columns: unrolled so their shared-memory latencies overlap.
-#pragma unroll 8
-      for (int c = j + 1; c < kNB; ++c) {
-        const double lcj = S[c][j];
-        if (r0 >= c) S[r0][c] = fma(-l0, lcj, S[r0][c]);
-        if (r1 >= c) S[r1][c] = fma(-l1, lcj, S[r1][c]);
-      }
-      __syncwarp();
     }
   }
   __syncthreads();

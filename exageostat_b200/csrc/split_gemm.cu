@@ -509,7 +509,8 @@ long long split_targets(int nt, int band, int k) {
 }
 
 int launch_split_update(const void* tm_hi, const void* tm_lo, const void* tm_c, const void* tm_cr, int ts, int nt,
-                        int band, int k, float* c_pool, const float* inv_scale, int* err, cudaStream_t st) {
+                        int band, int k, float* c_pool, const float* inv_scale, int* err, cudaStream_t st,
+                        int max_ctas) {
   using namespace sg;
   if (ts % BN != 0) return EGS_ERR_INVALID;
   const long long targets = split_targets(nt, band, k);
@@ -530,7 +531,8 @@ int launch_split_update(const void* tm_hi, const void* tm_lo, const void* tm_c, 
   P.c_pool = c_pool;
   P.inv_scale = inv_scale;
   P.err = err;
-  const long long grid = P.total < gemm_num_sms() ? P.total : gemm_num_sms();
+  const long long cap = (max_ctas > 0 && max_ctas < gemm_num_sms()) ? max_ctas : gemm_num_sms();
+  const long long grid = P.total < cap ? P.total : cap;
   split_gemm_kernel<<<(unsigned)grid, THREADS, SMEM_BYTES, st>>>(*reinterpret_cast<const CUtensorMap*>(tm_hi),
                                                                  *reinterpret_cast<const CUtensorMap*>(tm_lo),
                                                                  *reinterpret_cast<const CUtensorMap*>(tm_c),

@@ -100,6 +100,14 @@ EGS_API int egs_problem_set_precision(egs_problem* p, int precision, int band_ti
 #define EGS_BAND_FP64_DMMA 1
 EGS_API int egs_problem_set_band_method(egs_problem* p, int method);
 
+/* Look-ahead of a mixed problem (Ozaki band method): the FP64 panel of step
+ * k+1 (diagonal tile, band rows, L^-1) runs on `sms` SMs beside the off-band
+ * update of step k, which keeps the other SMs; 0 runs them one after the
+ * other (the default: at N = 102,400 the off-band update loses as much time
+ * to the reserved SMs as the overlap hides).  A scheduling choice only:
+ * results are bit-identical either way. */
+EGS_API int egs_problem_set_lookahead(egs_problem* p, int sms);
+
 /* Create a problem directly in the given precision (EGS_PRECISION_DOUBLE or
  * EGS_PRECISION_MIXED with band_tiles FP64 tile rows): the same as
  * egs_problem_create followed by egs_problem_set_precision, without ever

@@ -106,3 +106,15 @@ def test_mixed_not_positive_definite_is_reported():
     p = mixed_problem(x, y, z, 256, 1)
     with pytest.raises(egs.NotPositiveDefinite):
         p.mle_eval(theta)
+
+
+def test_lookahead_does_not_change_the_result():
+    n, theta = 3000, (1.0, 0.1, 0.5)
+    x, y, z = O.load_data(n, 13, theta)
+    p = mixed_problem(x, y, z, 256, 2)
+    out = []
+    for sms in (0, 8, 24, 0):
+        p.set_lookahead(sms)
+        out.append(p.mle_eval(theta))
+        out.append(p.mle_eval(theta))   # captured and replayed as a graph
+    assert all(r == out[0] for r in out)
