@@ -519,9 +519,16 @@ def main():
     if stage_ms[up] > 0:
         a = stage_flops[up] / (stage_ms[up] * 1e-3) / 1e12
         n_u = int(stage_launches[up])
-        roofs.append({"bound": "tensor", "kernel": "dgemm_update_kernel (FP64 band update, DMMA)",
+        int8_peak = 2.0 * bf16_peak
+        roofs.append({"bound": "tensor",
+                      "kernel": "ozaki_band_kernel (FP64-class band update: 7 signed 7-bit slices per operand, "
+                                "exact int32 products on tcgen05 kind::i8; stage includes the slicing)",
                       "achieved": a, "peak": fp64_peak, "unit": "TFLOP/s", "frac": a / fp64_peak,
-                      "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 entry)",
+                      "peak_source": "FP64-equivalent flops against cuBLAS DGEMM 8192^3 measured in this run "
+                                     "(MEASURED_PEAKS.json has no FP64 entry)",
+                      "executed_int8_tops": 28.0 * a, "frac_executed_of_int8": 28.0 * a / int8_peak,
+                      "int8_peak_source": "2x MEASURED_PEAKS.json bf16_tflops_sustained (the int8 rate is twice "
+                                          "the bf16 rate on B200)",
                       "traffic": None, "launches": n_u, "ms_per_eval": float(stage_ms[up]) / args.steps,
                       "flops_per_launch": stage_flops[up] / max(n_u, 1)})
     roofs.sort(key=lambda r: -r["ms_per_eval"])

@@ -558,10 +558,13 @@ static int enqueue_offband_update(egs_problem* p, int k, cudaStream_t st, int ma
   return EGS_OK;
 }
 
+// Algorithmic flops of the band update of step k: syrk (ts^3 + ts^2) on the
+// diagonal targets, gemm (2 ts^3) below them.
 static double band_update_flops(int ts, int nt, int b, int k) {
-  double band_tiles = 0.0;
-  for (int j = k + 1; j < nt; ++j) band_tiles += (double)(std::min(nt - 1, j + b) - j + 1);
-  return 2.0 * band_tiles * (double)ts * ts * ts;
+  double f = 0.0;
+  const double t = (double)ts;
+  for (int j = k + 1; j < nt; ++j) f += t * t * (t + 1.0) + 2.0 * (double)(std::min(nt - 1, j + b) - j) * t * t * t;
+  return f;
 }
 
 static double panel_flops(int ts, int n, int k) {
