@@ -296,7 +296,7 @@ def run_serving(args):
     mixed form (FP64 band of 2 tiles)."""
     import numpy as np
     import torch
-    import exageostat_b200 as egs
+    import exageostatcpp_b200 as egs
     torch.cuda.set_device(0)
     rng = np.random.default_rng(12345)
     pool = []
@@ -394,7 +394,7 @@ def main():
 
     import numpy as np
     import torch
-    import exageostat_b200 as egs
+    import exageostatcpp_b200 as egs
 
     rank, world, local = env_rank()
     dist = None

@@ -1,7 +1,7 @@
 """B200 (sm_100a) ExaGeoStat maximum-likelihood path.
 
 Python view of the C ABI declared in ``include/exageostat_b200.h``.  The compute
-lives in ``libexageostat_b200.so`` (built in-tree by ``exageostat_b200.build``);
+lives in ``libexageostat_b200.so`` (built in-tree by ``exageostatcpp_b200.build``);
 this module only marshals numpy arrays through ctypes.  There is no CPU
 fallback: if the shared library is missing, importing the bindings raises.
 """
@@ -128,7 +128,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     if _lib is not None:
         return _lib
     if not os.path.exists(path):
-        raise RuntimeError(f"{path} is missing: build it with `python -m exageostat_b200.build`; "
+        raise RuntimeError(f"{path} is missing: build it with `python -m exageostatcpp_b200.build`; "
                            "this package has no CPU fallback")
     lib = ctypes.CDLL(path)
     for name, (res, args) in SIGNATURES.items():

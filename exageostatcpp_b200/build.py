@@ -1,6 +1,6 @@
 """Build the sm_100a shared library ``libexageostat_b200.so`` in-tree.
 
-Usage: ``python -m exageostat_b200.build`` (or ``python exageostat_b200/build.py``).
+Usage: ``python -m exageostatcpp_b200.build`` (or ``python exageostatcpp_b200/build.py``).
 Each ``csrc/*.cu`` is compiled separately with nvcc for ``sm_100a`` and linked
 into one shared object next to this file; the C ABI is ``include/exageostat_b200.h``.
 """
@@ -72,7 +72,7 @@ def build_host_tests() -> str:
     os.makedirs(os.path.dirname(API_TEST_BIN), exist_ok=True)
     cmd = [nvcc(), "-std=c++17", "-O2", "-x", "c++", "-I", HOST_INCLUDE, "-I", os.path.join(ROOT, "include"),
            *HOST_SOURCES, API_TEST_SRC, "-L", HERE, "-lexageostat_b200",
-           "-Xlinker", "-rpath", "-Xlinker", "$ORIGIN/../../../exageostat_b200", "-o", API_TEST_BIN]
+           "-Xlinker", "-rpath", "-Xlinker", "$ORIGIN/../../../exageostatcpp_b200", "-o", API_TEST_BIN]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError(f"host API test build failed:\n{res.stdout}\n{res.stderr}")

@@ -6,7 +6,7 @@ import re
 
 import pytest
 
-import exageostat_b200 as egs
+import exageostatcpp_b200 as egs
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 

@@ -9,7 +9,7 @@ Tolerances:
 import numpy as np
 import pytest
 
-import exageostat_b200 as egs
+import exageostatcpp_b200 as egs
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu

@@ -16,7 +16,7 @@ BIN = os.path.join(ROOT, "tests", "cpp", "_build", "test_exageostat_api")
 @pytest.fixture(scope="module")
 def driver():
     if not os.path.exists(BIN):
-        from exageostat_b200 import build as b
+        from exageostatcpp_b200 import build as b
         b.build_host_tests()
     return BIN
 

@@ -14,7 +14,7 @@ it at 5e-5.
 import numpy as np
 import pytest
 
-import exageostat_b200 as egs
+import exageostatcpp_b200 as egs
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu

@@ -10,7 +10,7 @@ product would miss the bound by four orders of magnitude).
 import numpy as np
 import pytest
 
-import exageostat_b200 as egs
+import exageostatcpp_b200 as egs
 
 pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")

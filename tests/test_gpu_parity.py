@@ -8,7 +8,7 @@ Tolerances (stated in the MLE contract):
 import numpy as np
 import pytest
 
-import exageostat_b200 as egs
+import exageostatcpp_b200 as egs
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu

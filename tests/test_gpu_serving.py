@@ -10,7 +10,7 @@ log-likelihood), 1e-8 relative (FP64 kriging), 1e-6 (mixed precision).
 import numpy as np
 import pytest
 
-import exageostat_b200 as egs
+import exageostatcpp_b200 as egs
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu

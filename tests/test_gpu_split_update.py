@@ -8,7 +8,7 @@ or TF32 product would miss this by more than an order of magnitude.
 import numpy as np
 import pytest
 
-import exageostat_b200 as egs
+import exageostatcpp_b200 as egs
 
 pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")

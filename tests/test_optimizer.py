@@ -2,7 +2,7 @@
 import numpy as np
 import pytest
 
-import exageostat_b200 as egs
+import exageostatcpp_b200 as egs
 from oracle import oracle as O
 
 

@@ -4,7 +4,7 @@ import ctypes
 
 import pytest
 
-import exageostat_b200 as egs
+import exageostatcpp_b200 as egs
 
 
 def test_footprint_plain_matches_tile_storage():

@@ -16,7 +16,7 @@ import ctypes
 import numpy as np
 import pytest
 
-import exageostat_b200 as egs
+import exageostatcpp_b200 as egs
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
