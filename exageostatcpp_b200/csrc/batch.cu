@@ -69,7 +69,7 @@ trsm_batch_kernel(double* __restrict__ tiles, int ts, int k, int row0, int col0,
   if ((int)blockIdx.y >= ntl) return;
   const long long sl = tile_base[p] + tile_slot(k, k, nt);
   const long long sa = panel ? tile_base[p] + tile_slot(k + 1 + blockIdx.y, k, nt) : sl;
-  trsm_rows_body(tiles + sa * (long long)ts * ts, tiles + sl * (long long)ts * ts, ts,
+  trsm_rows_body<128>(tiles + sa * (long long)ts * ts, tiles + sl * (long long)ts * ts, ts,
                  row0 + blockIdx.x * blockDim.x + threadIdx.x, col0);
 }
 

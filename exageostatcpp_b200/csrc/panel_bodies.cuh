@@ -92,13 +92,26 @@ __device__ __forceinline__ void potrf64_body(double* __restrict__ T, int ts, int
 // X := A * L^-T for the 64 columns [col0, col0+64) of row `row` of tile A
 // (ld ts); L is the factored 64x64 diagonal block at (col0, col0) of tile TL.
 // Called by every thread of a 128-thread block (rows past ts just return).
+template <int NTHR>
 __device__ __forceinline__ void trsm_rows_body(double* __restrict__ A, const double* __restrict__ TL, int ts,
                                                int row, int col0) {
   __shared__ __align__(16) double L[kNB][kNB];
   __shared__ double invd[kNB];
-  for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
-    const int rr = e % kNB, c = e / kNB;
-    L[rr][c] = (rr >= c) ? TL[(long long)(col0 + c) * ts + col0 + rr] : 0.0;
+  {
+    // the 64 x 64 block, all loads issued before any is used
+    constexpr int per = kNB * kNB / NTHR;
+    double v[per];
+#pragma unroll
+    for (int q = 0; q < per; ++q) {
+      const int e = q * NTHR + threadIdx.x;
+      const int rr = e & (kNB - 1), c = e >> 6;
+      v[q] = (rr >= c) ? TL[(long long)(col0 + c) * ts + col0 + rr] : 0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < per; ++q) {
+      const int e = q * NTHR + threadIdx.x;
+      L[e & (kNB - 1)][e >> 6] = v[q];
+    }
   }
   __syncthreads();
   if (threadIdx.x < kNB) invd[threadIdx.x] = 1.0 / L[threadIdx.x][threadIdx.x];

@@ -38,7 +38,7 @@ void launch_potrf_diag_block(double* tiles, int ts, long long slot, int off, int
 __global__ void __launch_bounds__(128)
 trsm_rows_kernel(double* __restrict__ tiles, int ts, long long slot0, int row0, int col0,
                  long long lslot) {
-  trsm_rows_body(tiles + (slot0 + blockIdx.y) * (long long)ts * ts, tiles + lslot * (long long)ts * ts, ts,
+  trsm_rows_body<128>(tiles + (slot0 + blockIdx.y) * (long long)ts * ts, tiles + lslot * (long long)ts * ts, ts,
                  row0 + blockIdx.x * blockDim.x + threadIdx.x, col0);
 }
 
