@@ -33,6 +33,8 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from exageostatcpp_b200 import replicas as R  # noqa: E402  (pure Python, no GPU needed to import)
+
 N = 102400
 DTS = 1024
 BAND = 2
@@ -255,11 +257,7 @@ def timed_evals(torch, p, stream, theta, steps, dist=None):
         lat.append(1e3 * (time.perf_counter() - t))
     e1.record(stream)
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    if dist:
-        tt = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = R.max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
     return ms, lat, r
 
 
@@ -467,11 +465,7 @@ def main():
         q.set_locations(xh, yh)
         q.set_observations(zh)
         ll_e2e = q.mle_eval(THETA)[0]
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        tt = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
+    e2e_s = R.max_over_ranks(time.perf_counter() - t0, dist, "cuda")
     e2e = {"value": world * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 3 * N * 8 + 64,
            "d2h_bytes_per_step": 4 * 8 + 8,
            "api": "egs_problem_set_locations + egs_problem_set_observations + egs_mle_eval "

@@ -43,6 +43,7 @@ class Configurations {
   EGS_PROP(int, ObservationNumber, 0)
   EGS_PROP(int, TimeSlot, 1)
   EGS_PROP(int, Band, 0)
+  EGS_PROP(int, MixedPrecisionBand, 2)  // FP64 tile rows below the diagonal with --precision=mixed
   EGS_PROP(int, MaxRank, 0)
   EGS_PROP(int, CoresNumber, 1)
   EGS_PROP(int, GPUsNumbers, 1)

@@ -48,13 +48,21 @@ class DescriptorData {
 
   // Creates the device problem of n points (dts: the dense tile size); replaces the
   // descriptors InitiateDescriptors makes (LinearAlgebraMethods.cpp:36-118).
-  egs_problem* EnsureProblem(int n, int dts) {
-    if (mProblem && mN == n && mDts == dts) return mProblem;
+  // precision: EGS_PRECISION_DOUBLE or EGS_PRECISION_MIXED (band_tiles FP64 tile
+  // rows); a different shape or precision replaces the problem.
+  // *created (optional) tells whether a new problem was made.
+  egs_problem* EnsureProblem(int n, int dts, int precision = EGS_PRECISION_DOUBLE, int band_tiles = 0,
+                             bool* created = nullptr) {
+    if (created) *created = false;
+    if (mProblem && mN == n && mDts == dts && mPrecision == precision && mBandTiles == band_tiles) return mProblem;
+    if (created) *created = true;
     if (mProblem) egs_problem_destroy(mProblem);
     mProblem = nullptr;
-    EgsCheck(egs_problem_create(&mProblem, n, dts), "egs_problem_create");
+    EgsCheck(egs_problem_create_ex(&mProblem, n, dts, precision, band_tiles), "egs_problem_create_ex");
     mN = n;
     mDts = dts;
+    mPrecision = precision;
+    mBandTiles = band_tiles;
     mIsDescriptorInitiated = true;
     return mProblem;
   }
@@ -93,6 +101,7 @@ class DescriptorData {
  private:
   egs_problem* mProblem = nullptr;
   int mN = 0, mDts = 0;
+  int mPrecision = EGS_PRECISION_DOUBLE, mBandTiles = 0;
   bool mIsDescriptorInitiated = false;
   std::map<int, std::vector<T>> mHost;
   std::map<int, DescriptorView<T>> mViews;

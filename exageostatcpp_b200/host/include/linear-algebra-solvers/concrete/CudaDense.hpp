@@ -22,13 +22,24 @@ class CudaDense : public LinearAlgebraMethods<T> {
     static_assert(sizeof(T) == sizeof(double), "the device path is FP64");
     const int n = aConfigurations.GetProblemSize();
     auto* dd = aData->GetDescriptorData();
-    egs_problem* p = dd->EnsureProblem(n, aConfigurations.GetDenseTileSize());
-    // DIAGONAL_APPROX: ChameleonDST with --band (a band of 0 or 1 keeps only the diagonal tiles)
-    const int band = aConfigurations.GetComputation() == common::DIAGONAL_APPROX
-                         ? (aConfigurations.GetBand() > 1 ? aConfigurations.GetBand() : 1)
-                         : 0;
-    dataunits::EgsCheck(egs_problem_set_band(p, band), "egs_problem_set_band");
-    if (aData->GetMleIterations() == 0) {
+    // --precision: MIXED keeps the diagonal and MixedPrecisionBand tile rows in FP64
+    // and the other tiles in FP32 (Definitions.hpp Precision; the reference declares
+    // the option without a dense mixed implementation)
+    const bool mixed = aConfigurations.GetPrecision() == common::MIXED;
+    if (mixed && aConfigurations.GetComputation() == common::DIAGONAL_APPROX)
+      throw std::domain_error("--precision=mixed and --computation=diag_approx are exclusive");
+    const int precision = mixed ? EGS_PRECISION_MIXED : EGS_PRECISION_DOUBLE;
+    const int mband = mixed ? aConfigurations.GetMixedPrecisionBand() : 0;
+    bool created = false;
+    egs_problem* p = dd->EnsureProblem(n, aConfigurations.GetDenseTileSize(), precision, mband, &created);
+    if (!mixed) {
+      // DIAGONAL_APPROX: ChameleonDST with --band (a band of 0 or 1 keeps only the diagonal tiles)
+      const int band = aConfigurations.GetComputation() == common::DIAGONAL_APPROX
+                           ? (aConfigurations.GetBand() > 1 ? aConfigurations.GetBand() : 1)
+                           : 0;
+      dataunits::EgsCheck(egs_problem_set_band(p, band), "egs_problem_set_band");
+    }
+    if (aData->GetMleIterations() == 0 || created) {
       // first evaluation: upload locations and save Z into Zcpy (:113-119)
       dataunits::EgsCheck(egs_problem_set_locations(p, aData->GetLocations()->GetLocationX(),
                                                     aData->GetLocations()->GetLocationY()),

@@ -116,6 +116,27 @@ void generate_and_model() {
             << std::endl;
 }
 
+// --precision=mixed through the API: the same synthetic data modelled with
+// three BOBYQA evaluations in FP64 and in mixed precision (FP64 band of 2 tiles).
+void mixed_modeling() {
+  Configurations c = modeling_config();
+  c.SetProblemSize(3000);
+  c.SetDenseTileSize(256);
+  auto hardware = ExaGeoStatHardware(EXACT_DENSE, 4, 0);
+  std::unique_ptr<ExaGeoStatData<double>> data;
+  api::ExaGeoStat<double>::ExaGeoStatLoadData(c, data);
+  const double ll_double = api::ExaGeoStat<double>::ExaGeoStatDataModeling(c, data);
+  const std::vector<double> th_double = c.GetEstimatedTheta();
+  c.SetPrecision(MIXED);
+  c.SetStartingTheta({0.1, 0.1, 0.1});
+  data->SetMleIterations(0);
+  const double ll_mixed = api::ExaGeoStat<double>::ExaGeoStatDataModeling(c, data);
+  std::cout.precision(17);
+  std::cout << "{\"loglik_double\": " << ll_double << ", \"loglik_mixed\": " << ll_mixed
+            << ", \"theta_double\": " << json_array(th_double.data(), 3)
+            << ", \"theta_mixed\": " << json_array(c.GetEstimatedTheta().data(), 3) << "}" << std::endl;
+}
+
 // TestPrediction.cpp TEST_PREDICTION_MISSING_DATA, section "Test Prediction - MSPE"
 void prediction_mspe(const Fixture& f) {
   Configurations c;
@@ -241,6 +262,7 @@ int main(int argc, char** argv) {
     else if (which == "generate_n9") generate(9, 5);
     else if (which == "modeling_fixture") modeling_fixture(read_fixture(argv[2]));
     else if (which == "generate_and_model") generate_and_model();
+    else if (which == "mixed_modeling") mixed_modeling();
     else if (which == "prediction_mspe") prediction_mspe(read_fixture(argv[2]));
     else if (which == "generated_locations") generated_locations();
     else if (which == "plugin_and_errors") plugin_and_errors(read_fixture(argv[2]));

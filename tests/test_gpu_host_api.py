@@ -84,3 +84,12 @@ def test_kernel_plugin_and_error_behaviour(driver, fixture_file):
     assert "NoSuchKernel" in out["unknown_kernel"]
     assert out["non_spd"] == "Matrix is not positive definite"
     assert out["no_theta"].startswith("Can't predict without an estimated")
+
+
+@pytest.mark.gpu
+def test_mixed_precision_through_the_api(driver):
+    # Configurations::SetPrecision(MIXED): the same three BOBYQA evaluations as in
+    # FP64; the best log-likelihood within the mixed-precision tolerance (1e-6)
+    out = run(driver, "mixed_modeling")
+    assert abs(out["loglik_mixed"] - out["loglik_double"]) <= 1e-6 * abs(out["loglik_double"])
+    assert out["theta_mixed"] == pytest.approx(out["theta_double"], abs=1e-12)
