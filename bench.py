@@ -354,6 +354,7 @@ def run_serving(args):
             lines.append({"form": label, "rate_per_s": rate, "requests": len(res),
                           "failed": int(sum(r.status != 0 for r in res)),
                           "failed_not_positive_definite": int(sum(r.status > 0 for r in res)),
+                          "answered_in_fp64": int(sum(r.precision_used != precision for r in res)),
                           "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                           "evals_per_s": st["evals"] / span, "span_s": span, "per_kind": per,
                           "peak_active": st["peak_active"], "peak_reserved_gb": st["peak_reserved"] / 1e9})

@@ -89,6 +89,7 @@ SIGNATURES = {
     "egs_ozaki_band_update": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P, _D]),
     "egs_problem_set_band_method": (ctypes.c_int, [_P, ctypes.c_int]),
     "egs_problem_set_lookahead": (ctypes.c_int, [_P, ctypes.c_int]),
+    "egs_mloe_mmom_host": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _D, _D, _D, _D]),
 }
 
 
@@ -104,7 +105,7 @@ class Result(ctypes.Structure):
     """egs_result of the serving API."""
     _fields_ = [("status", ctypes.c_int), ("kind", ctypes.c_int), ("loglik", ctypes.c_double),
                 ("theta", ctypes.c_double * 3), ("evals", ctypes.c_int), ("queue_ms", ctypes.c_double),
-                ("latency_ms", ctypes.c_double), ("footprint", ctypes.c_longlong)]
+                ("latency_ms", ctypes.c_double), ("footprint", ctypes.c_longlong), ("precision_used", ctypes.c_int)]
 
 
 SIGNATURES.update({
@@ -449,6 +450,17 @@ def ozaki_band_update(ts: int, nt: int, band: int, k: int, w_ptr: int, band_ptr:
     _check(load_library().egs_ozaki_band_update(int(ts), int(nt), int(band), int(k), _P(w_ptr), _P(band_ptr),
                                                 ctypes.byref(ms)), "egs_ozaki_band_update")
     return ms.value
+
+
+def mloe_mmom_host(x_obs, y_obs, x_miss, y_miss, theta_true, theta_est, dts: int):
+    """(MLOE, MMOM) of kriging with theta_est when theta_true holds (egs_mloe_mmom_host)."""
+    xo, yo, xm, ym = _f64(x_obs), _f64(y_obs), _f64(x_miss), _f64(y_miss)
+    tt, te = _f64(theta_true), _f64(theta_est)
+    a, b = ctypes.c_double(), ctypes.c_double()
+    _check(load_library().egs_mloe_mmom_host(len(xo), len(xm), int(dts), _dptr(xo), _dptr(yo), _dptr(xm), _dptr(ym),
+                                             _dptr(tt), _dptr(te), ctypes.byref(a), ctypes.byref(b)),
+           "egs_mloe_mmom_host")
+    return a.value, b.value
 
 
 def footprint(n: int, dts: int, precision: int = EGS_PRECISION_DOUBLE, band_tiles: int = 0) -> int:

@@ -1678,3 +1678,110 @@ int egs_problem_predict(egs_problem* p, const double* theta, int n_miss, const d
   if (cudaStreamSynchronize(st) != cudaSuccess && rc == EGS_OK) rc = check_cuda("egs_problem_predict/sync");
   return rc;
 }
+
+// ---------------------------------------------------------------------------
+// MLOE / MMOM (LinearAlgebraMethods<T>::ExaGeoStatMLETileMLOEMMOM,
+// src/linear-algebra-solvers/LinearAlgebraMethods.cpp:802-1131, and the
+// dmloe-mmom codelet, src/runtime/starpu/concrete/dmloe-mmom-codelet.cpp:73-102)
+// ---------------------------------------------------------------------------
+
+int egs_mloe_mmom_host(int n_obs, int n_miss, int dts, const double* x_obs, const double* y_obs,
+                       const double* x_miss, const double* y_miss, const double* theta_true,
+                       const double* theta_est, double* mloe, double* mmom) {
+  if (n_obs <= 0 || n_miss <= 0 || dts <= 0 || !x_obs || !y_obs || !x_miss || !y_miss || !theta_true ||
+      !theta_est || !mloe || !mmom)
+    return EGS_ERR_INVALID;
+  MaternParams mt, ma;
+  if (make_matern_params(theta_true, &mt) != EGS_OK || make_matern_params(theta_est, &ma) != EGS_OK) {
+    set_last_error("theta outside the Matern domain (sigma2 > 0, beta > 0, nu > 0)", "egs_mloe_mmom_host");
+    return EGS_ERR_INVALID;
+  }
+  // K_t, K_a: the observed covariance under the true / the estimated theta, factored
+  // pa is created first so that pt, which borrows pa's stream below, is destroyed first
+  egs_problem *pt = nullptr, *pa = nullptr;
+  int rc = egs_problem_create(&pa, n_obs, dts);
+  if (rc != EGS_OK) return rc;
+  std::unique_ptr<egs_problem, int (*)(egs_problem*)> ga(pa, egs_problem_destroy);
+  if ((rc = egs_problem_create(&pt, n_obs, dts)) != EGS_OK) return rc;
+  std::unique_ptr<egs_problem, int (*)(egs_problem*)> gt(pt, egs_problem_destroy);
+  for (egs_problem* p : {pt, pa}) {
+    if ((rc = egs_problem_set_locations(p, x_obs, y_obs)) != EGS_OK) return rc;
+    p->have_observations = true;  // the solves below set z themselves
+  }
+  if ((rc = egs_covariance_generate(pt, theta_true)) != EGS_OK || (rc = egs_potrf(pt)) != EGS_OK) return rc;
+  if ((rc = egs_covariance_generate(pa, theta_est)) != EGS_OK || (rc = egs_potrf(pa)) != EGS_OK) return rc;
+  // both problems run on pa's stream from here
+  cudaStream_t st = pa->stream;
+  const long long np = pa->np;
+  double *kt = nullptr, *ka = nullptr, *dxm = nullptr, *dym = nullptr, *ya = nullptr, *u = nullptr, *dots = nullptr;
+  long long dummy = 0;
+  auto cleanup = [&]() {
+    for (void* b : {(void*)kt, (void*)ka, (void*)dxm, (void*)dym, (void*)ya, (void*)u, (void*)dots}) dev_free(b, st);
+    cudaStreamSynchronize(st);
+  };
+  if ((rc = dev_alloc(&kt, (size_t)np * n_miss, &dummy, st)) || (rc = dev_alloc(&ka, (size_t)np * n_miss, &dummy, st)) ||
+      (rc = dev_alloc(&dxm, n_miss, &dummy, st)) || (rc = dev_alloc(&dym, n_miss, &dummy, st)) ||
+      (rc = dev_alloc(&ya, np, &dummy, st)) || (rc = dev_alloc(&u, np, &dummy, st)) ||
+      (rc = dev_alloc(&dots, (size_t)4 * n_miss, &dummy, st))) {
+    cleanup();
+    return rc;
+  }
+  cudaMemsetAsync(kt, 0, (size_t)np * n_miss * sizeof(double), st);
+  cudaMemsetAsync(ka, 0, (size_t)np * n_miss * sizeof(double), st);
+  cudaMemcpyAsync(dxm, x_miss, n_miss * sizeof(double), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(dym, y_miss, n_miss * sizeof(double), cudaMemcpyHostToDevice, st);
+  // k_t, k_a for every target: columns of leading dimension np (padding rows stay 0)
+  launch_matern_block(kt, (int)np, n_obs, n_miss, pa->x, pa->y, dxm, dym, mt, st);
+  launch_matern_block(ka, (int)np, n_obs, n_miss, pa->x, pa->y, dxm, dym, ma, st);
+  if ((rc = egs_problem_set_stream(pt, st)) != EGS_OK) {
+    cleanup();
+    return rc;
+  }
+  for (int q = 0; q < n_miss; ++q) {
+    const double* ktq = kt + (long long)q * np;
+    const double* kaq = ka + (long long)q * np;
+    double* d = dots + 4ll * q;
+    // y_a = L_a^-1 k_a
+    cudaMemcpyAsync(pa->z, kaq, np * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    enqueue_trsv(pa);
+    cudaMemcpyAsync(ya, pa->z, np * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    launch_dot(ya, ya, (int)np, d + 0, st);                       // k_a' K_a^-1 k_a
+    // L_a^-1 k_t . y_a = k_t' K_a^-1 k_a
+    cudaMemcpyAsync(pa->z, ktq, np * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    enqueue_trsv(pa);
+    launch_dot(pa->z, ya, (int)np, d + 1, st);
+    // k_t' K_t^-1 k_t
+    cudaMemcpyAsync(pt->z, ktq, np * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    enqueue_trsv(pt);
+    launch_dot(pt->z, pt->z, (int)np, d + 2, st);
+    // w_a = L_a^-T y_a; w_a' K_t w_a = |L_t^T w_a|^2
+    cudaMemcpyAsync(pa->z, ya, np * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    enqueue_trsv_t(pa);
+    launch_trmv_t(pt->tiles, pt->ts, pt->nt, pa->z, u, st);
+    launch_dot(u, u, (int)np, d + 3, st);
+  }
+  std::vector<double> h(4ll * n_miss);
+  cudaMemcpyAsync(h.data(), dots, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st);
+  rc = check_cuda("egs_mloe_mmom_host");
+  if (cudaStreamSynchronize(st) != cudaSuccess && rc == EGS_OK) rc = check_cuda("egs_mloe_mmom_host/sync");
+  cleanup();
+  if (rc != EGS_OK) return rc;
+  const double s2t = theta_true[0], s2a = theta_est[0];
+  double loe = 0.0, mom = 0.0;
+  for (int q = 0; q < n_miss; ++q) {
+    const double aka = h[4 * q], tka = h[4 * q + 1], tkt = h[4 * q + 2], wkw = h[4 * q + 3];
+    const double e2 = s2t - 2.0 * tka + wkw;  // MSE of the predictor built with theta_est
+    const double e3 = s2t - tkt;              // MSE of the predictor built with theta_true
+    const double e4 = s2a - aka;              // MSE the estimated model claims
+    if (e3 == 0.0) {
+      loe -= 1.0;
+      mom -= 1.0;
+    } else {
+      loe += e2 / e3 - 1.0;
+      mom += e4 / e2 - 1.0;
+    }
+  }
+  *mloe = loe / n_miss;
+  *mmom = mom / n_miss;
+  return EGS_OK;
+}

@@ -100,18 +100,17 @@ struct egs_server {
     return nullptr;
   }
 
-  void run(Request* q) {
+  // One attempt of a request in the given precision; returns its status.
+  int attempt(Request* q, int precision) {
     egs_result& out = q->res;
-    out.kind = q->r.kind;
-    std::memcpy(out.theta, q->r.theta, sizeof(out.theta));
     egs_problem* p = nullptr;
-    int rc = egs_problem_create_ex(&p, q->r.n, q->r.dts, q->r.precision, q->r.band_tiles);
+    int rc = egs_problem_create_ex(&p, q->r.n, q->r.dts, precision, q->r.band_tiles);
     if (rc == EGS_OK) rc = egs_problem_set_locations(p, q->x.data(), q->y.data());
     if (rc == EGS_OK) rc = egs_problem_set_observations(p, q->z.data());
     if (rc == EGS_OK) {
       if (q->r.kind == EGS_REQ_LOGLIK) {
         rc = egs_mle_eval(p, q->r.theta, &out.loglik, nullptr, nullptr);
-        out.evals = 1;
+        out.evals += 1;
       } else if (q->r.kind == EGS_REQ_FIT) {
         FitCtx ctx{p, EGS_OK, 0};
         double th[3];
@@ -123,14 +122,30 @@ struct egs_server {
         if (rc == EGS_OK && ctx.status != EGS_OK && !(best > -1e299)) rc = ctx.status;
         out.loglik = best;
         std::memcpy(out.theta, th, sizeof(th));
-        out.evals = ctx.evals;
+        out.evals += ctx.evals;
       } else {
         q->zm.assign(q->r.n_miss, 0.0);
         rc = egs_problem_predict(p, q->r.theta, q->r.n_miss, q->xm.data(), q->ym.data(), q->zm.data());
-        out.evals = 1;
+        out.evals += 1;
       }
     }
     if (p) egs_problem_destroy(p);
+    return rc;
+  }
+
+  void run(Request* q) {
+    egs_result& out = q->res;
+    out.kind = q->r.kind;
+    std::memcpy(out.theta, q->r.theta, sizeof(out.theta));
+    out.precision_used = q->r.precision;
+    int rc = attempt(q, q->r.precision);
+    if (rc > 0 && q->r.precision == EGS_PRECISION_MIXED) {
+      // the FP32 off-band storage lost positive definiteness (a very smooth or
+      // long-range kernel): answer the request with the FP64 path instead
+      std::memcpy(out.theta, q->r.theta, sizeof(out.theta));
+      out.precision_used = EGS_PRECISION_DOUBLE;
+      rc = attempt(q, EGS_PRECISION_DOUBLE);
+    }
     out.status = rc;
   }
 

@@ -91,6 +91,8 @@ void launch_scatter_panel(const double* W2, double* band, double* inv, double* W
                           cudaStream_t st);
 void launch_scatter_offband(const double* W, float* off, int ts, int nt, int b, int nb, int k, cudaStream_t st);
 const float* offband_tile(const float* off, int ts, int nt, int b, int i, int k);
+void launch_trmv_t(const double* tiles, int ts, int nt, const double* w, double* out, cudaStream_t st);
+void launch_dot(const double* a, const double* b, int n, double* out, cudaStream_t st);
 long long residual_scratch_doubles(int n);
 void launch_add_inplace(double* a, const double* b, int n, cudaStream_t st);
 void launch_matern_residual(const double* x, const double* y, const double* z, const double* v, int n, int np,

@@ -269,3 +269,45 @@ void launch_trmv(const double* tiles, int ts, int nt, const double* e, double* p
 }
 
 }  // namespace egs
+
+namespace egs {
+
+// out = L^T w for the lower tiled factor (global row r = j ts + c):
+// out[r] = sum_{i > j} (column c of tile (i, j)) . w_i + sum_{rr >= c} L_jj(rr, c) w_j(rr);
+// one warp per output element, fixed summation order.
+__global__ void __launch_bounds__(256)
+trmv_t_kernel(const double* __restrict__ tiles, int ts, int nt, const double* __restrict__ w,
+              double* __restrict__ out) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int j = blockIdx.y, c = blockIdx.x * 8 + warp;
+  if (c >= ts) return;
+  double acc = 0.0;
+  for (int i = j; i < nt; ++i) {
+    const double* col = tiles + tile_slot(i, j, nt) * (long long)ts * ts + (long long)c * ts;
+    const double* wi = w + (long long)i * ts;
+    for (int rr = (i == j ? c : 0) + lane; rr < ts; rr += 32) acc = fma(col[rr], wi[rr], acc);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0) out[(long long)j * ts + c] = acc;
+}
+
+void launch_trmv_t(const double* tiles, int ts, int nt, const double* w, double* out, cudaStream_t st) {
+  trmv_t_kernel<<<dim3((ts + 7) / 8, nt), 256, 0, st>>>(tiles, ts, nt, w, out);
+}
+
+// out[slot] = a . b over n entries (one block, fixed order).
+__global__ void __launch_bounds__(256)
+dot_kernel(const double* __restrict__ a, const double* __restrict__ b, int n, double* __restrict__ out) {
+  __shared__ double red[256];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < n; i += 256) acc = fma(a[i], b[i], acc);
+  const double s = block_sum_256(acc, red);
+  if (threadIdx.x == 0) *out = s;
+}
+
+void launch_dot(const double* a, const double* b, int n, double* out, cudaStream_t st) {
+  dot_kernel<<<1, 256, 0, st>>>(a, b, n, out);
+}
+
+}  // namespace egs

@@ -343,6 +343,18 @@ EGS_API int egs_predict_host(int n_obs, int n_miss, int dts, const double* x_obs
                      const double* z_obs, const double* x_miss, const double* y_miss,
                      const double* z_actual, const double* theta, double* z_miss, double* mspe);
 
+/* Mean loss of efficiency (MLOE) and mean misspecification of the mean square
+ * error (MMOM) of kriging with theta_est when theta_true holds, over n_miss
+ * target locations (host arrays).  Replaces
+ * LinearAlgebraMethods<T>::ExaGeoStatMLETileMLOEMMOM
+ * (src/linear-algebra-solvers/LinearAlgebraMethods.cpp:802-1131) with the
+ * dmloe-mmom codelet (src/runtime/starpu/concrete/dmloe-mmom-codelet.cpp:73-102);
+ * univariate: the sill is sigma^2.  Both observed covariances are factored
+ * once; each target costs four triangular solves and one L^T product. */
+EGS_API int egs_mloe_mmom_host(int n_obs, int n_miss, int dts, const double* x_obs, const double* y_obs,
+                               const double* x_miss, const double* y_miss, const double* theta_true,
+                               const double* theta_est, double* mloe, double* mmom);
+
 /* ---- serving ------------------------------------------------------------ */
 
 /* A request loop on one GPU: likelihood, fit and predict requests of any N are
@@ -392,6 +404,9 @@ typedef struct egs_result {
   double queue_ms;     /* submission -> admission */
   double latency_ms;   /* submission -> completion */
   long long footprint; /* HBM bytes reserved at admission */
+  int precision_used;  /* the precision that produced the result: a mixed request whose
+                          factorisation is not positive definite (FP32 off-band storage
+                          of a very smooth kernel) is answered by the FP64 path */
 } egs_result;
 
 /* Start a server on `device` with hbm_budget bytes of admission budget and at

@@ -334,3 +334,106 @@ def predict(x_obs, y_obs, z_obs, x_miss, y_miss, theta, z_actual=None):
 def flops_potrf(n: float) -> float:
     """Chameleon's flops_dpotrf for real arithmetic: n^3/3 + n^2/2 + n/6."""
     return n ** 3 / 3.0 + n ** 2 / 2.0 + n / 6.0
+
+
+# --------------------------------------------------------------------------
+# MLOE / MMOM: LinearAlgebraMethods.cpp:802-1131, dmloe-mmom-codelet.cpp:73-102
+# --------------------------------------------------------------------------
+def mloe_mmom(x_obs, y_obs, x_miss, y_miss, theta_true, theta_est):
+    """Mean loss of efficiency and mean misspecification of the mean square error
+    of kriging with theta_est when theta_true holds, over the target points.
+
+    Per target p, with k_t, k_a the covariances between the observed points
+    and target p under theta_true / theta_est and K_t, K_a the observed
+    covariance matrices (univariate: alpha = sigma^2):
+        w_a   = K_a^-1 k_a
+        e2    = sigma2_t - 2 k_t.w_a + w_a' K_t w_a    (MSE of the misspecified predictor)
+        e3    = sigma2_t - k_t' K_t^-1 k_t               (MSE of the right predictor)
+        e4    = sigma2_a - k_a' K_a^-1 k_a               (MSE the misspecified model claims)
+        loe_p = e2 / e3 - 1,  mom_p = e4 / e2 - 1  (both -1 when e3 == 0)
+    and MLOE, MMOM are the means over the targets."""
+    kt_all = matern_block(x_obs, y_obs, x_miss, y_miss, theta_true)
+    ka_all = matern_block(x_obs, y_obs, x_miss, y_miss, theta_est)
+    Kt = covariance(x_obs, y_obs, theta_true)
+    Ka = covariance(x_obs, y_obs, theta_est)
+    ct = scipy.linalg.cho_factor(Kt, lower=True, check_finite=False)
+    ca = scipy.linalg.cho_factor(Ka, lower=True, check_finite=False)
+    s2t, s2a = float(theta_true[0]), float(theta_est[0])
+    loe = mom = 0.0
+    m = kt_all.shape[1]
+    for p in range(m):
+        kt, ka = kt_all[:, p], ka_all[:, p]
+        wa = scipy.linalg.cho_solve(ca, ka, check_finite=False)
+        e2 = s2t - 2.0 * kt @ wa + wa @ (Kt @ wa)
+        e3 = s2t - kt @ scipy.linalg.cho_solve(ct, kt, check_finite=False)
+        e4 = s2a - ka @ wa
+        if e3 == 0.0:
+            loe -= 1.0
+            mom -= 1.0
+        else:
+            loe += e2 / e3 - 1.0
+            mom += e4 / e2 - 1.0
+    return loe / m, mom / m
+
+
+# --------------------------------------------------------------------------
+# Fisher information: LinearAlgebraMethods.cpp:1133-1306 with the derivative
+# kernels UnivariateMaternDdsigmaSquare / Dbeta / Dnu
+# (src/kernels/concrete/UnivariateMaternD*.cpp) and BasselFunction.cpp:23-33.
+# --------------------------------------------------------------------------
+def dkv_dnu(nu: float, x: np.ndarray) -> np.ndarray:
+    """d K_nu(x) / d nu from K_nu(x) = int_0^inf exp(-x cosh t) cosh(nu t) dt:
+    d/dnu = int_0^inf t sinh(nu t) exp(-x cosh t) dt.  The integrand is smooth and
+    decays double-exponentially, so the trapezoid rule on a fine grid converges
+    to full double precision (checked against mpmath.diff(besselk) in the tests).
+    The reference takes a forward difference with step 1e-9
+    (BasselFunction.cpp:23-33), which carries ~1e-7 relative rounding noise."""
+    xs = np.asarray(x, dtype=np.float64)
+    flat = xs.reshape(-1)
+    out = np.empty_like(flat)
+    h = 1.0 / 256.0
+    for i, xv in enumerate(flat):
+        # stop where exp(-x cosh t) < 1e-300 relative to the peak
+        tmax = np.arccosh(max(1.0, 700.0 / max(xv, 1e-300) + 1.0)) + 1.0
+        t = np.arange(0.0, tmax + h, h)
+        f = t * np.sinh(nu * t) * np.exp(-xv * (np.cosh(t) - 1.0))
+        out[i] = np.exp(-xv) * h * (f.sum() - 0.5 * f[-1])  # f(0) = 0
+    return out.reshape(xs.shape)
+
+
+def matern_derivatives(x, y, theta):
+    """dC/dsigma2, dC/dbeta, dC/dnu on all pairs (full matrices), as the reference's kernels:
+    at distance 0 they are 1, 0, 0."""
+    from scipy.special import kv, gamma, digamma
+    sigma2, beta, nu = float(theta[0]), float(theta[1]), float(theta[2])
+    x = np.asarray(x, dtype=np.float64)
+    y = np.asarray(y, dtype=np.float64)
+    d = np.sqrt((x[None, :] - x[:, None]) ** 2 + (y[None, :] - y[:, None]) ** 2)
+    e = d / beta
+    zero = e == 0
+    es = np.where(zero, 1.0, e)
+    con = 1.0 / (2.0 ** (nu - 1.0) * gamma(nu))
+    k0 = kv(nu, es)
+    k1 = kv(nu + 1.0, es)
+    dsig = np.where(zero, 1.0, con * es ** nu * k0)
+    beta_expr = -nu / beta * es ** nu * k0 - es ** nu * (nu / es * k0 - k1) * es / beta
+    dbeta = np.where(zero, 0.0, sigma2 * con * beta_expr)
+    dk = dkv_dnu(nu, es)
+    nu_expr = (-2.0 * np.log(2.0) * 2.0 ** (-nu) / gamma(nu) * es ** nu * k0
+               + 2.0 ** (1.0 - nu) * (-digamma(nu) / gamma(nu) * es ** nu * k0
+                                       + (es ** nu * np.log(es) * k0 + es ** nu * dk) / gamma(nu)))
+    dnu = np.where(zero, 0.0, sigma2 * nu_expr)
+    return dsig, dbeta, dnu
+
+
+def fisher_inverse(x, y, theta) -> np.ndarray:
+    """Inverse of the Fisher information A_jk = 1/2 tr(C^-1 C_j C^-1 C_k) (3 x 3, column-major list)."""
+    c = covariance(x, y, theta)
+    cf = scipy.linalg.cho_factor(c, lower=True, check_finite=False)
+    ders = matern_derivatives(x, y, theta)
+    sol = [scipy.linalg.cho_solve(cf, dj, check_finite=False) for dj in ders]
+    a = np.empty((3, 3))
+    for j in range(3):
+        for k in range(3):
+            a[j, k] = 0.5 * np.sum(sol[j] * sol[k].T)
+    return np.linalg.inv(a)

@@ -72,6 +72,21 @@ def main(ref: str) -> None:
         "source": f"{p}:{_line_of(src, m.start())}", "mspe": float(m.group(1)), "z_miss_number": 4,
         "estimated_theta": _numbers(et.group(1)), "dts": 8,
         "note": "Catch::Approx default relative epsilon is ~1.19e-5 (float epsilon * 100)"}
+    # MLOE/MMOM: the third PickRandomPoints split of the test case (Catch re-runs the
+    # body for each SECTION; the MSPE and IDW sections split first), truth theta =
+    # the initial theta, estimated theta = (0.9, 0.09, 0.4)
+    m1 = re.search(r"GetMLOE\(\) == Catch::Approx\((-?\d+\.\d+)\)\.margin\((\d+\.\d+)\)", src)
+    m2 = re.search(r"GetMMOM\(\) == Catch::Approx\((-?\d+\.\d+)\)\.margin\((\d+\.\d+)\)", src)
+    out["prediction_mloe_mmom_n16"] = {
+        "source": f"{p}:{_line_of(src, m1.start())}", "mloe": float(m1.group(1)), "mmom": float(m2.group(1)),
+        "margin": float(m1.group(2)), "z_miss_number": 4, "split_index": 2,
+        "truth_theta": [1.0, 0.1, 0.5], "estimated_theta": [0.9, 0.09, 0.4]}
+    i = src.index("required_fisher = {")
+    fisher, _ = _array_after(src, "required_fisher = {")
+    out["prediction_fisher_n16"] = {
+        "source": f"{p}:{_line_of(src, i)}", "fisher_inverse": fisher, "margin": 1e-6,
+        "estimated_theta": [0.9, 0.09, 0.4], "n": 16,
+        "note": "inverse of the 3x3 Fisher information at the estimated theta on all 16 fixture locations"}
 
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_goldens.json")
     with open(dst, "w") as f:

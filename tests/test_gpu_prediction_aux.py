@@ -1,0 +1,37 @@
+"""Auxiliary prediction measures on the GPU against the oracle and the
+reference goldens: MLOE / MMOM (egs_mloe_mmom_host).
+
+Tolerances: the golden values to 1e-6 (the reference asks 1e-3); the oracle to
+1e-10 absolute (both compute the same FP64 quantities; MLOE/MMOM are O(0.01))."""
+import numpy as np
+import pytest
+
+import exageostatcpp_b200 as egs
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def test_mloe_mmom_golden(goldens):
+    f = goldens["fixture_n16"]
+    g = goldens["prediction_mloe_mmom_n16"]
+    rng = O.GlibcRand(1)
+    for _ in range(g["split_index"]):
+        O.shuffle_split(f["z"], f["x"], f["y"], g["z_miss_number"], rng)
+    zo, xo, yo, za, xm, ym = O.shuffle_split(f["z"], f["x"], f["y"], g["z_miss_number"], rng)
+    mloe, mmom = egs.mloe_mmom_host(xo, yo, xm, ym, g["truth_theta"], g["estimated_theta"], 8)
+    assert abs(mloe - g["mloe"]) < 1e-6 and abs(mmom - g["mmom"]) < 1e-6
+    mloe0, mmom0 = egs.mloe_mmom_host(xo, yo, xm, ym, g["truth_theta"], g["truth_theta"], 8)
+    assert abs(mloe0) < 1e-12 and abs(mmom0) < 1e-12
+
+
+@pytest.mark.parametrize("n,m,dts", [(1500, 40, 256), (700, 9, 128)])
+def test_mloe_mmom_matches_oracle(n, m, dts):
+    tt, te = (1.0, 0.1, 0.5), (0.8, 0.12, 0.6)
+    x, y, z = O.load_data(n + m, 5, tt)
+    rng = np.random.default_rng(3)
+    miss = np.sort(rng.choice(n + m, m, replace=False))
+    obs = np.setdiff1d(np.arange(n + m), miss)
+    got = egs.mloe_mmom_host(x[obs], y[obs], x[miss], y[miss], tt, te, dts)
+    ref = O.mloe_mmom(x[obs], y[obs], x[miss], y[miss], tt, te)
+    assert abs(got[0] - ref[0]) < 1e-10 and abs(got[1] - ref[1]) < 1e-10, (got, ref)

@@ -161,3 +161,26 @@ def test_oversized_request_is_refused():
         with pytest.raises(egs.EgsError) as ei:
             s.submit(egs.EGS_REQ_LOGLIK, x, y, z, 256)
         assert ei.value.status == egs.EGS_ERR_OOM
+
+
+def test_mixed_request_that_loses_definiteness_is_answered_in_fp64():
+    # Very smooth, long-range kernels on a dense grid: kappa(Sigma) ~ 1e10 and more,
+    # beyond FP32 off-band storage; the server answers such mixed requests with the
+    # FP64 path (precision_used) instead of failing them.
+    x, y = egs.generate_locations(1600, 0)
+    z = egs.dlarnv_normal(0, 1600)
+    fell_back = 0
+    with egs.Server(hbm_budget=16 << 30, max_active=2) as s:
+        for theta in [(1.2, 0.2, 2.5), (1.0, 0.3, 2.5), (1.0, 0.5, 2.0)]:
+            tp = s.submit(egs.EGS_REQ_LOGLIK, x, y, z, 256, theta=theta)
+            tm = s.submit(egs.EGS_REQ_LOGLIK, x, y, z, 256, theta=theta, precision=M, band_tiles=1)
+            (rp, _), (rm, _) = s.wait(tp), s.wait(tm)
+            if rp.status != 0:
+                continue
+            assert rm.status == 0
+            if rm.precision_used == D:
+                fell_back += 1
+                assert rm.loglik == rp.loglik
+            else:
+                assert abs(rm.loglik - rp.loglik) <= 1e-4 * abs(rp.loglik)
+    assert fell_back >= 1
