@@ -90,6 +90,7 @@ SIGNATURES = {
     "egs_problem_set_band_method": (ctypes.c_int, [_P, ctypes.c_int]),
     "egs_problem_set_lookahead": (ctypes.c_int, [_P, ctypes.c_int]),
     "egs_mloe_mmom_host": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _D, _D, _D, _D]),
+    "egs_fisher_host": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _D, _D, _D, _D]),
 }
 
 
@@ -461,6 +462,15 @@ def mloe_mmom_host(x_obs, y_obs, x_miss, y_miss, theta_true, theta_est, dts: int
                                              _dptr(tt), _dptr(te), ctypes.byref(a), ctypes.byref(b)),
            "egs_mloe_mmom_host")
     return a.value, b.value
+
+
+def fisher_host(x, y, theta, dts: int) -> np.ndarray:
+    """Inverse Fisher information (3 x 3) of (sigma^2, beta, nu) at theta (egs_fisher_host)."""
+    xx, yy, th = _f64(x), _f64(y), _f64(theta)
+    out = np.zeros(9)
+    _check(load_library().egs_fisher_host(len(xx), int(dts), _dptr(xx), _dptr(yy), _dptr(th), _dptr(out)),
+           "egs_fisher_host")
+    return out.reshape(3, 3).T
 
 
 def footprint(n: int, dts: int, precision: int = EGS_PRECISION_DOUBLE, band_tiles: int = 0) -> int:

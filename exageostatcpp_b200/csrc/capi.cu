@@ -365,12 +365,13 @@ int enqueue_panel(double* tiles, const void* tmap, int ts, int nt, int k, int co
 // row solve below it, tensor-core syrk of the rest of the tile), solve the tile
 // column below it (64-wide blocked: row solve + tensor-core update), then the
 // tensor-core trailing update of every tile (i, j), k < j <= i.
-int enqueue_potrf(egs_problem* p) {
+int enqueue_potrf(egs_problem* p, int steps = -1) {
   const int ts = p->ts, nt = p->nt, n = p->n;
   cudaStream_t st = p->stream;
   int* info = p->flags;
   int* err = p->flags + 1;
-  for (int k = 0; k < nt; ++k) {
+  const int kend = (steps >= 0 && steps < nt) ? steps : nt;
+  for (int k = 0; k < kend; ++k) {
     const long long skk = tile_slot(k, k, nt);
     int sp = span_begin(p, EGS_STAGE_PANEL);
     long long nl = 0;
@@ -1785,3 +1786,36 @@ int egs_mloe_mmom_host(int n_obs, int n_miss, int dts, const double* x_obs, cons
   *mmom = mom / n_miss;
   return EGS_OK;
 }
+
+namespace egs {
+
+// The first `steps` tile steps of the factorisation of p's tiles as they are
+// (no generation): the panels of columns 0 .. steps-1 and their trailing
+// updates of every later tile.  Used by the Fisher information
+// (augmented matrices).  Returns the LAPACK-style info or an error.
+int enqueue_potrf_steps(egs_problem* p, int steps) {
+  EGS_CUDA_TRY(cudaMemsetAsync(p->flags, 0, 2 * sizeof(int), p->stream));
+  int rc = enqueue_potrf(p, steps);
+  if (rc != EGS_OK) return rc;
+  EGS_CUDA_TRY(cudaMemcpyAsync(p->hflags, p->flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+  EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  if (p->hflags[1] != 0) {
+    set_last_error("a device-side wait exceeded its limit", "enqueue_potrf_steps");
+    return EGS_ERR_TIMEOUT;
+  }
+  if (p->hflags[0] > 0) {
+    set_last_error("Matrix is not positive definite", "enqueue_potrf_steps");
+    return p->hflags[0];
+  }
+  return check_cuda("enqueue_potrf_steps");
+}
+
+int problem_tiles(egs_problem* p, double** tiles, int* ts, int* nt, cudaStream_t* st) {
+  *tiles = p->tiles;
+  *ts = p->ts;
+  *nt = p->nt;
+  *st = p->stream;
+  return EGS_OK;
+}
+
+}  // namespace egs

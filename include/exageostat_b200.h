@@ -355,6 +355,18 @@ EGS_API int egs_mloe_mmom_host(int n_obs, int n_miss, int dts, const double* x_o
                                const double* x_miss, const double* y_miss, const double* theta_true,
                                const double* theta_est, double* mloe, double* mmom);
 
+/* Inverse of the Fisher information of (sigma^2, beta, nu) at theta for n
+ * host locations: A_jk = 1/2 tr(C^-1 dC/dtheta_j C^-1 dC/dtheta_k), written
+ * column-major (3 x 3).  Replaces LinearAlgebraMethods<T>::ExaGeoStatFisherTile
+ * (src/linear-algebra-solvers/LinearAlgebraMethods.cpp:1133-1306) with the
+ * derivative kernels UnivariateMaternDdsigmaSquare / Dbeta / Dnu
+ * (src/kernels/concrete/); d K_nu / d nu by Richardson-extrapolated central
+ * differences (steps 1e-3, 5e-4) where the reference takes a forward one
+ * (step 1e-9, BasselFunction.cpp:23-33).
+ * Works in dense n x n buffers (about 8 n^2 doubles). */
+EGS_API int egs_fisher_host(int n, int dts, const double* x, const double* y, const double* theta,
+                            double* fisher_inverse);
+
 /* ---- serving ------------------------------------------------------------ */
 
 /* A request loop on one GPU: likelihood, fit and predict requests of any N are

@@ -35,3 +35,22 @@ def test_mloe_mmom_matches_oracle(n, m, dts):
     got = egs.mloe_mmom_host(x[obs], y[obs], x[miss], y[miss], tt, te, dts)
     ref = O.mloe_mmom(x[obs], y[obs], x[miss], y[miss], tt, te)
     assert abs(got[0] - ref[0]) < 1e-10 and abs(got[1] - ref[1]) < 1e-10, (got, ref)
+
+
+def test_fisher_golden(goldens):
+    # TestPrediction.cpp:167-168 on all 16 fixture locations; the reference's own
+    # forward-difference dK/dnu limits the agreement to ~1.5e-5 (see the oracle test)
+    f = goldens["fixture_n16"]
+    g = goldens["prediction_fisher_n16"]
+    inv = egs.fisher_host(f["x"], f["y"], g["estimated_theta"], 8)
+    assert np.abs(inv.T.reshape(-1) - np.array(g["fisher_inverse"])).max() < 2e-5
+    ref = O.fisher_inverse(f["x"], f["y"], g["estimated_theta"])
+    assert np.abs(inv - ref).max() <= 1e-7 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("theta,dts", [((1.0, 0.1, 1.3), 64), ((1.5, 0.05, 0.5), 128)])
+def test_fisher_matches_oracle(theta, dts):
+    x, y, _ = O.load_data(200, 8, (1.0, 0.1, 0.5))
+    inv = egs.fisher_host(x, y, theta, dts)
+    ref = O.fisher_inverse(x, y, theta)
+    assert np.abs(inv - ref).max() <= 1e-7 * np.abs(ref).max(), (inv, ref)
