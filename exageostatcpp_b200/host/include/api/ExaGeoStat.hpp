@@ -1,6 +1,7 @@
 // Public facade (inst/include/api/ExaGeoStat.hpp:28-86, src/api/ExaGeoStat.cpp:72-125):
 // generate/load data, model (MLE fit), predict.
 #pragma once
+#include "data-loader/CSVLoader.hpp"
 #include <cstdlib>
 #include <memory>
 #include "configurations/Configurations.hpp"
@@ -18,6 +19,11 @@ class ExaGeoStat {
   // ExaGeoStat.cpp:72-88: srand(seed), then locations and Z = L e at the initial theta.
   static void ExaGeoStatLoadData(configurations::Configurations& aConfigurations,
                                  std::unique_ptr<dataunits::ExaGeoStatData<T>>& aData) {
+    // --datapath: the CSV loader (DataLoader.cpp:29, CSVLoader.cpp:37-143); else synthetic data
+    if (!aConfigurations.GetDataPath().empty()) {
+      aData = dataLoader::csv::CSVLoader<T>::LoadData(aConfigurations);
+      return;
+    }
     std::srand(aConfigurations.GetSeed());
     std::unique_ptr<kernels::Kernel<T>> kernel(plugins::PluginRegistry<kernels::Kernel<T>>::Create(
         aConfigurations.GetKernelName(), aConfigurations.GetTimeSlot()));

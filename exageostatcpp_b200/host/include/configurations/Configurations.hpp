@@ -54,6 +54,7 @@ class Configurations {
   EGS_PROP(bool, IsMLOEMMOM, false)
   EGS_PROP(bool, IsNonGaussian, false)
   EGS_PROP(std::string, RecoveryFile, "")
+  EGS_PROP(std::string, DataPath, "")  // CSV data file (--datapath); empty: synthetic data
 #undef EGS_PROP
 
  public:

@@ -85,6 +85,15 @@ class Prediction {
       truth = false;
     }
     aConfigurations.SetObservationNumber(nobs);
+    // Fisher information on all locations (Prediction.cpp:76-87), before the split
+    if (aConfigurations.GetIsFisher()) {
+      std::vector<double> fisher(9);
+      dataunits::EgsCheck(egs_fisher_host(aConfigurations.GetProblemSize(), aConfigurations.GetDenseTileSize(),
+                                          aData->GetLocations()->GetLocationX(), aData->GetLocations()->GetLocationY(),
+                                          et.data(), fisher.data()),
+                          "egs_fisher_host");
+      results::Results::GetInstance()->SetFisherMatrix(fisher);
+    }
     if (nmiss <= 0) return;
     results::Results::GetInstance()->SetZMiss(nmiss);
     auto solver = linearAlgebra::LinearAlgebraFactory<T>::CreateLinearAlgebraSolver(common::EXACT_DENSE);
@@ -107,6 +116,16 @@ class Prediction {
       }
       solver->ExaGeoStatGetZObs(aConfigurations, zobs.data(), nobs, *aData->GetDescriptorData(), apMeasurementsMatrix,
                                 1);
+    }
+    // MLOE / MMOM with the initial theta as the truth (Prediction.cpp:132-139)
+    if (aConfigurations.GetIsMLOEMMOM()) {
+      double mloe = 0, mmom = 0;
+      dataunits::EgsCheck(egs_mloe_mmom_host(nobs, nmiss, aConfigurations.GetDenseTileSize(), obs.GetLocationX(),
+                                             obs.GetLocationY(), miss.GetLocationX(), miss.GetLocationY(),
+                                             aConfigurations.GetInitialTheta().data(), et.data(), &mloe, &mmom),
+                          "egs_mloe_mmom_host");
+      results::Results::GetInstance()->SetMLOE(mloe);
+      results::Results::GetInstance()->SetMMOM(mmom);
     }
     if (aConfigurations.GetIsMSPE()) {
       T* err = solver->ExaGeoStatMLEPredictTile(aData, et.data(), nmiss, nobs, zobs.data(),

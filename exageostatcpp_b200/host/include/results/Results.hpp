@@ -1,5 +1,6 @@
 // Singleton summary of an ExaGeoStat run (src/results/Results.cpp:26-259):
-// log-likelihood, theta, MSPE, predicted values, iteration count and timings.
+// log-likelihood, theta, MSPE, predicted values, Fisher matrix, MLOE/MMOM,
+// iteration count and timings.
 #pragma once
 #include <vector>
 
@@ -31,11 +32,18 @@ class Results {
   double GetMSPEExecutionTime() const { return mMSPETime; }
   void SetGeneratedLocationsNumber(int v) { mGenerated = v; }
   int GetGeneratedLocationsNumber() const { return mGenerated; }
+  // Results.cpp: Fisher matrix (inverse Fisher information, column-major), MLOE, MMOM
+  void SetFisherMatrix(const std::vector<double>& v) { mFisher = v; }
+  std::vector<double> GetFisherMatrix() const { return mFisher; }
+  void SetMLOE(double v) { mMLOE = v; }
+  double GetMLOE() const { return mMLOE; }
+  void SetMMOM(double v) { mMMOM = v; }
+  double GetMMOM() const { return mMMOM; }
 
  private:
-  double mLogLik = 0, mMSPE = 0, mModelingTime = 0, mModelingFlops = 0, mMSPETime = 0;
+  double mLogLik = 0, mMSPE = 0, mModelingTime = 0, mModelingFlops = 0, mMSPETime = 0, mMLOE = 0, mMMOM = 0;
   int mMLEIterations = 0, mZMissNumber = 0, mGenerated = 0;
-  std::vector<double> mMaximumTheta, mZMiss;
+  std::vector<double> mMaximumTheta, mZMiss, mFisher;
 };
 
 }  // namespace exageostat::results

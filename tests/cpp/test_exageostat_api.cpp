@@ -6,6 +6,7 @@
 //
 // usage: test_exageostat_api <case> [fixture-file]
 //   fixture-file: three lines of 16 numbers (x, y, z) -- the reference's N=16 fixture.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -251,6 +252,89 @@ void plugin_and_errors(const Fixture& f) {
 
 }  // namespace
 
+
+// TestPrediction.cpp sections "MLOE_MMOM" and "FISHER": the reference's Catch test
+// re-runs its body per SECTION in one process, so the MLOE/MMOM section draws the
+// third hold-out split (after the MSPE and IDW sections); the same sequence here.
+void prediction_aux(const Fixture& f) {
+  Configurations c;
+  c.SetUnknownObservationsNb(4);
+  c.SetProblemSize(16);
+  c.SetKernelName("UnivariateMaternStationary");
+  c.SetDenseTileSize(8);
+  c.SetComputation(EXACT_DENSE);
+  c.SetInitialTheta({1, 0.1, 0.5});
+  c.SetEstimatedTheta({0.9, 0.09, 0.4});
+  Configurations::SetVerbosity(QUIET_MODE);
+  auto hardware = ExaGeoStatHardware(EXACT_DENSE, c.GetCoresNumber(), c.GetGPUsNumbers());
+  kernels::Kernel<double>* pKernel =
+      plugins::PluginRegistry<kernels::Kernel<double>>::Create(c.GetKernelName(), c.GetTimeSlot());
+  auto run = [&](bool mspe, bool mloe, bool fisher) {
+    auto data = std::make_unique<ExaGeoStatData<double>>(c.GetProblemSize(), c.GetDimension());
+    std::vector<double> z = f.z, x = f.x, y = f.y;
+    data->GetLocations()->SetLocationX(*x.data(), 16);
+    data->GetLocations()->SetLocationY(*y.data(), 16);
+    c.SetIsMSPE(mspe);
+    c.SetIsMLOEMMOM(mloe);
+    c.SetIsFisher(fisher);
+    prediction::Prediction<double>::PredictMissingData(data, c, z.data(), *pKernel);
+  };
+  run(true, false, false);   // the MSPE section
+  run(true, false, false);   // the IDW section's split
+  run(false, true, false);   // MLOE / MMOM
+  auto* r = results::Results::GetInstance();
+  const double mloe = r->GetMLOE(), mmom = r->GetMMOM();
+  run(false, false, true);   // Fisher (no split needed)
+  auto fisher = r->GetFisherMatrix();
+  delete pKernel;
+  std::cout.precision(17);
+  std::cout << "{\"mloe\": " << mloe << ", \"mmom\": " << mmom << ", \"fisher\": "
+            << json_array(fisher.data(), (int)fisher.size()) << "}" << std::endl;
+}
+
+
+// CSV round trip: synthetic data written by the CSV writer, read back by the
+// loader through ExaGeoStatLoadData (--datapath), then modelled.
+void csv_roundtrip(const std::string& dir) {
+  Configurations c = modeling_config();
+  auto hardware = ExaGeoStatHardware(EXACT_DENSE, 4, 0);
+  std::unique_ptr<ExaGeoStatData<double>> gen;
+  api::ExaGeoStat<double>::ExaGeoStatLoadData(c, gen);
+  std::vector<double> z = gen->GetDescriptorData()->HostVector(DESCRIPTOR_Z);
+  const std::string file =
+      dataLoader::csv::CSVLoader<double>::WriteData(z.data(), 16, dir, *gen->GetLocations());
+  Configurations c2 = modeling_config();
+  c2.SetProblemSize(0);
+  c2.SetDataPath(file);
+  std::unique_ptr<ExaGeoStatData<double>> loaded;
+  api::ExaGeoStat<double>::ExaGeoStatLoadData(c2, loaded);
+  double dmax = 0;
+  std::vector<double>& z2 = loaded->GetDescriptorData()->HostVector(DESCRIPTOR_Z);
+  for (int i = 0; i < 16; ++i) {
+    dmax = std::max(dmax, std::fabs(z2[i] - z[i]));
+    dmax = std::max(dmax, std::fabs(loaded->GetLocations()->GetLocationX()[i] - gen->GetLocations()->GetLocationX()[i]));
+    dmax = std::max(dmax, std::fabs(loaded->GetLocations()->GetLocationY()[i] - gen->GetLocations()->GetLocationY()[i]));
+  }
+  const double ll_gen = api::ExaGeoStat<double>::ExaGeoStatDataModeling(c, gen);
+  const double ll_csv = api::ExaGeoStat<double>::ExaGeoStatDataModeling(c2, loaded);
+  std::string bad = "none";
+  {
+    std::ofstream o(dir + "/bad.csv");
+    o << "0.1,0.2,0.3,0.4\n";
+  }
+  Configurations c3 = modeling_config();
+  c3.SetDataPath(dir + "/bad.csv");
+  try {
+    std::unique_ptr<ExaGeoStatData<double>> d3;
+    api::ExaGeoStat<double>::ExaGeoStatLoadData(c3, d3);
+  } catch (const std::exception& e) {
+    bad = e.what();
+  }
+  std::cout.precision(17);
+  std::cout << "{\"n\": " << c2.GetProblemSize() << ", \"max_diff\": " << dmax << ", \"loglik_generated\": " << ll_gen
+            << ", \"loglik_csv\": " << ll_csv << ", \"bad\": \"" << bad << "\"}" << std::endl;
+}
+
 int main(int argc, char** argv) {
   if (argc < 2) {
     std::cerr << "usage: test_exageostat_api <case> [fixture-file]\n";
@@ -264,6 +348,8 @@ int main(int argc, char** argv) {
     else if (which == "generate_and_model") generate_and_model();
     else if (which == "mixed_modeling") mixed_modeling();
     else if (which == "prediction_mspe") prediction_mspe(read_fixture(argv[2]));
+    else if (which == "prediction_aux") prediction_aux(read_fixture(argv[2]));
+    else if (which == "csv_roundtrip") csv_roundtrip(argv[2]);
     else if (which == "generated_locations") generated_locations();
     else if (which == "plugin_and_errors") plugin_and_errors(read_fixture(argv[2]));
     else {

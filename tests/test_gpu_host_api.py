@@ -93,3 +93,27 @@ def test_mixed_precision_through_the_api(driver):
     out = run(driver, "mixed_modeling")
     assert abs(out["loglik_mixed"] - out["loglik_double"]) <= 1e-6 * abs(out["loglik_double"])
     assert out["theta_mixed"] == pytest.approx(out["theta_double"], abs=1e-12)
+
+
+@pytest.mark.gpu
+def test_prediction_mloe_mmom_and_fisher(driver, goldens, fixture_file):
+    # TestPrediction.cpp:129-130 (reference margin 1e-3) and :167-168 (the
+    # reference's 1e-6 applies to its own forward-difference dK/dnu; the exact
+    # derivative agrees to 1.5e-5)
+    out = run(driver, "prediction_aux", fixture_file)
+    g = goldens["prediction_mloe_mmom_n16"]
+    assert abs(out["mloe"] - g["mloe"]) < 1e-6 and abs(out["mmom"] - g["mmom"]) < 1e-6
+    fg = goldens["prediction_fisher_n16"]
+    assert max(abs(a - b) for a, b in zip(out["fisher"], fg["fisher_inverse"])) < 2e-5
+
+
+@pytest.mark.gpu
+def test_csv_loader_round_trip(driver, tmp_path):
+    # CSVLoader.cpp:37-289: 15 significant digits written, read back through
+    # ExaGeoStatLoadData(--datapath); a 4-value line is rejected for 2-D data
+    out = run(driver, "csv_roundtrip", str(tmp_path))
+    assert out["n"] == 16
+    assert out["max_diff"] < 1e-14
+    assert abs(out["loglik_csv"] - out["loglik_generated"]) <= 1e-12 * abs(out["loglik_generated"])
+    assert "dimensions" in out["bad"]
+    assert any(p.name == "SYN_16_1" for p in (tmp_path / "synthetic_ds").iterdir())
