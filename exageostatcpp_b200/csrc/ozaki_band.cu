@@ -182,13 +182,42 @@ __device__ __forceinline__ uint64_t sdesc_sw64(uint32_t addr) {
   d |= (uint64_t)4 << 61;            // SWIZZLE_64B
   return d;
 }
+// One int8 MMA.  COLLECT selects the use of the tensor core's A collector
+// buffer: 0 reads A from shared memory only, 1 reads it and keeps it in the
+// collector (fill), 2 takes A from the collector and keeps it (use), 3 takes
+// it from the collector and releases it (lastuse).  Consecutive MMAs with the
+// same A slice read it from shared memory once.
+template <int COLLECT>
 __device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-      "l"(adesc), "l"(bdesc), "r"(oz::IDESC), "r"(accumulate)
-      : "memory");
+  if constexpr (COLLECT == 0) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(oz::IDESC), "r"(accumulate)
+        : "memory");
+  } else if constexpr (COLLECT == 1) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8.collector::a::fill [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(oz::IDESC), "r"(accumulate)
+        : "memory");
+  } else if constexpr (COLLECT == 2) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8.collector::a::use [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(oz::IDESC), "r"(accumulate)
+        : "memory");
+  } else {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8.collector::a::lastuse [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(oz::IDESC), "r"(accumulate)
+        : "memory");
+  }
 }
 __device__ __forceinline__ void oz_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
@@ -341,18 +370,24 @@ ozaki_band_kernel(const __grid_constant__ CUtensorMap tm_s, const __grid_constan
           oz_fence_after();
           const uint32_t sa = smem_u32(smem + s * STAGE_BYTES);
           const uint32_t sb = sa + S * A_SLICE;
+          // A slice p outermost: its products with B slices q = 1 .. S+1-p go to
+          // the groups d = p + q and take A from the collector after the first
+          // (integer sums are exact, so the order within a group is free).
 #pragma unroll
           for (int kk = 0; kk < BK / 32; ++kk) {
 #pragma unroll
-            for (int d = 2; d <= S + 1; ++d) {
-              const uint32_t dcol = tmem_base + (uint32_t)((d - 2) * BN);
+            for (int p = 1; p <= S; ++p) {
+              const uint64_t ad = sdesc_sw64(sa + (p - 1) * A_SLICE + kk * 32);
+              const uint32_t acc = (kt > 0 || kk > 0 || p > 1) ? 1u : 0u;  // p = 1 opens every group
+              const int qmax = S + 1 - p;
 #pragma unroll
-              for (int p = 1; p <= S; ++p) {
-                const int q = d - p;
-                if (q < 1 || q > S) continue;
-                const uint32_t acc = (kt > 0 || kk > 0 || p > 1) ? 1u : 0u;  // p = 1 opens group d
-                umma_i8(dcol, sdesc_sw64(sa + (p - 1) * A_SLICE + kk * 32), sdesc_sw64(sb + (q - 1) * B_SLICE + kk * 32),
-                        acc);
+              for (int q = 1; q <= qmax; ++q) {
+                const uint32_t dcol = tmem_base + (uint32_t)((p + q - 2) * BN);
+                const uint64_t bd = sdesc_sw64(sb + (q - 1) * B_SLICE + kk * 32);
+                if (qmax == 1) umma_i8<0>(dcol, ad, bd, acc);
+                else if (q == 1) umma_i8<1>(dcol, ad, bd, acc);
+                else if (q < qmax) umma_i8<2>(dcol, ad, bd, acc);
+                else umma_i8<3>(dcol, ad, bd, acc);
               }
             }
           }

@@ -23,13 +23,20 @@ __device__ __forceinline__ double block_sum_256(double v, double* red) {
 
 // Cholesky of the 64x64 block at T (ld ts).  Every thread of the block (NTHR,
 // whole warps) takes part in moving the block between global and shared memory,
-// with all loads issued before any is used.  Up to four warps factor it; lane l
-// of each owns rows l and l + 32.  info records the 1-based global column
-// (gcol0 + j + 1) of the first pivot that is not positive (or NaN).
+// with all loads issued before any is used.  Up to eight warps factor it; lane
+// l of each owns rows l and l + 32, and warp w the columns c with c % CW == w.
+// At step j every warp scales column j with the reciprocal pivot and applies
+// the rank-1 update to its columns c > j; the owner of column j + 1 updates
+// that column first and computes the next pivot's square root and reciprocal
+// before the step's barrier, so no warp waits on them after it.  Warp 0 stores
+// the scaled column j after the barrier (no warp reads it again).  info
+// records the 1-based global column (gcol0 + j + 1) of the first pivot that is
+// not positive (or NaN).
 template <int NTHR>
 __device__ __forceinline__ void potrf64_body(double* __restrict__ T, int ts, int gcol0, int* __restrict__ info) {
   static_assert(NTHR % 32 == 0 && NTHR >= 32 && NTHR <= 1024, "whole warps");
   __shared__ double S[kNB][kNB + 1];
+  __shared__ double piv[kNB], pinv[kNB];  // L_jj and 1 / L_jj
   constexpr int per = kNB * kNB / NTHR;
   {
     // column-major block: element e = c * 64 + r; all loads issued first
@@ -47,24 +54,39 @@ __device__ __forceinline__ void potrf64_body(double* __restrict__ T, int ts, int
     }
   }
   __syncthreads();
-  // Factorisation by CW warps: at step j every warp reads the pivot and column
-  // j (unscaled), and warp w applies the rank-1 update to the columns
-  // c > j with c % CW == w of its lanes' rows l and l + 32; after the step's
-  // barrier warp 0 stores the scaled column j (no warp reads it again).
-  constexpr int CW = NTHR / 32 < 4 ? NTHR / 32 : 4;
+  if (threadIdx.x == 0) {
+    const double d = S[0][0];
+    if (!(d > 0.0)) atomicCAS(info, 0, gcol0 + 1);
+    const double ljj = sqrt(d);
+    piv[0] = ljj;
+    pinv[0] = 1.0 / ljj;
+  }
+  __syncthreads();
+  constexpr int CW = NTHR / 32 < 8 ? NTHR / 32 : 8;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int r0 = lane, r1 = lane + 32;
   for (int j = 0; j < kNB; ++j) {
-    double ljj = 0.0, l0 = 0.0, l1 = 0.0;
+    double l0 = 0.0, l1 = 0.0;
     if (warp < CW) {
-      const double d = S[j][j];
-      if (threadIdx.x == 0 && !(d > 0.0)) atomicCAS(info, 0, gcol0 + j + 1);
-      ljj = sqrt(d);
-      const double inv = 1.0 / ljj;
+      const double inv = pinv[j];
       l0 = (r0 > j) ? S[r0][j] * inv : 0.0;
       l1 = (r1 > j) ? S[r1][j] * inv : 0.0;
       // first column of this warp after j
-      const int c1 = j + 1 + ((warp - (j + 1)) % CW + CW) % CW;
+      int c1 = j + 1 + ((warp - (j + 1)) % CW + CW) % CW;
+      if (c1 == j + 1 && c1 < kNB) {
+        const double lcj = S[c1][j] * inv;
+        if (r0 >= c1) S[r0][c1] = fma(-l0, lcj, S[r0][c1]);
+        if (r1 >= c1) S[r1][c1] = fma(-l1, lcj, S[r1][c1]);
+        __syncwarp();
+        if (lane == 0) {
+          const double d = S[c1][c1];
+          if (!(d > 0.0)) atomicCAS(info, 0, gcol0 + c1 + 1);
+          const double ljj = sqrt(d);
+          piv[c1] = ljj;
+          pinv[c1] = 1.0 / ljj;
+        }
+        c1 += CW;
+      }
 #pragma unroll 4
       for (int c = c1; c < kNB; c += CW) {
         const double lcj = S[c][j] * inv;
@@ -76,8 +98,8 @@ __device__ __forceinline__ void potrf64_body(double* __restrict__ T, int ts, int
     if (warp == 0) {
       if (r0 > j) S[r0][j] = l0;
       if (r1 > j) S[r1][j] = l1;
-      if (r0 == j) S[r0][j] = ljj;
-      if (r1 == j) S[r1][j] = ljj;
+      if (r0 == j) S[r0][j] = piv[j];
+      if (r1 == j) S[r1][j] = piv[j];
     }
   }
   __syncthreads();
@@ -92,10 +114,13 @@ __device__ __forceinline__ void potrf64_body(double* __restrict__ T, int ts, int
 // X := A * L^-T for the 64 columns [col0, col0+64) of row `row` of tile A
 // (ld ts); L is the factored 64x64 diagonal block at (col0, col0) of tile TL.
 // Called by every thread of a 128-thread block (rows past ts just return).
+// Right-looking: once x_c is final, it is applied to every later column, so
+// the multiply-adds of a step are independent; each x_c still receives its
+// terms in the order q = 0 .. c-1, as in forward substitution.
 template <int NTHR>
 __device__ __forceinline__ void trsm_rows_body(double* __restrict__ A, const double* __restrict__ TL, int ts,
                                                int row, int col0) {
-  __shared__ __align__(16) double L[kNB][kNB];
+  __shared__ __align__(16) double LT[kNB][kNB];  // LT[c][r] = L(r, c): column c of L
   __shared__ double invd[kNB];
   {
     // the 64 x 64 block, all loads issued before any is used
@@ -110,11 +135,11 @@ __device__ __forceinline__ void trsm_rows_body(double* __restrict__ A, const dou
 #pragma unroll
     for (int q = 0; q < per; ++q) {
       const int e = q * NTHR + threadIdx.x;
-      L[e & (kNB - 1)][e >> 6] = v[q];
+      LT[e >> 6][e & (kNB - 1)] = v[q];
     }
   }
   __syncthreads();
-  if (threadIdx.x < kNB) invd[threadIdx.x] = 1.0 / L[threadIdx.x][threadIdx.x];
+  if (threadIdx.x < kNB) invd[threadIdx.x] = 1.0 / LT[threadIdx.x][threadIdx.x];
   __syncthreads();
   if (row >= ts) return;
   double* a = A + (long long)col0 * ts + row;
@@ -123,18 +148,15 @@ __device__ __forceinline__ void trsm_rows_body(double* __restrict__ A, const dou
   for (int c = 0; c < kNB; ++c) x[c] = a[(long long)c * ts];
 #pragma unroll
   for (int c = 0; c < kNB; ++c) {
-    double s = x[c];
+    x[c] *= invd[c];
+    const double xc = x[c];
+    if (c + 1 < kNB && ((c + 1) & 1)) x[c + 1] = fma(-xc, LT[c][c + 1], x[c + 1]);
 #pragma unroll
-    for (int q = 0; q < c; q += 2) {
-      if (q + 1 < c) {
-        const double2 l2 = *reinterpret_cast<const double2*>(&L[c][q]);
-        s = fma(-x[q], l2.x, s);
-        s = fma(-x[q + 1], l2.y, s);
-      } else {
-        s = fma(-x[q], L[c][q], s);
-      }
+    for (int q = (c + 2) & ~1; q < kNB; q += 2) {
+      const double2 l2 = *reinterpret_cast<const double2*>(&LT[c][q]);
+      x[q] = fma(-xc, l2.x, x[q]);
+      x[q + 1] = fma(-xc, l2.y, x[q + 1]);
     }
-    x[c] = s * invd[c];
   }
 #pragma unroll
   for (int c = 0; c < kNB; ++c) a[(long long)c * ts] = x[c];
