@@ -658,11 +658,14 @@ int enqueue_eval_mixed_ozaki(egs_problem* p) {
                                      p->oz_scale, err, st))
         return rc;
       launch_scatter_offband(p->W, p->off_pool, ts, nt, b, nb, k, st);
-      nl += 6;
+      nl += 5;
     }
     if (ntp > 1) {
-      launch_panel_split(p->W, ts, 1, ntp - 1, k, p->inv_scale, p->ph, p->pl, st);
-      nl += 2;
+      // one read of the solved rows: FP16 hi/lo for the off-band update, int8
+      // slices for the band update
+      launch_panel_prepare(p->W, ts, 1, ntp - 1, k, p->oz_scale, p->oz_slices, (long long)p->np + ts,
+                           p->inv_scale, p->ph, p->pl, st);
+      nl += 1;
     }
     count_launches(p, EGS_STAGE_PANEL, nl);
     span_end(p, sp, 0.0);
@@ -670,11 +673,10 @@ int enqueue_eval_mixed_ozaki(egs_problem* p) {
     sp = span_begin(p, EGS_STAGE_UPDATE);
     const egs_problem::OzLaunch& O = p->oz_launch[k];
     if (O.count > 0) {
-      launch_ozaki_slice(p->W, ts, 1, ntp - 1, k, p->oz_scale, p->oz_slices, (long long)p->np + ts, st);
       if (int rc = launch_ozaki_band(p->tm_oz, p->oz_targets + O.off, O.count, O.items, ts, b, p->band_pool,
                                      p->oz_scale, err, st))
         return rc;
-      count_launches(p, EGS_STAGE_UPDATE, 3);
+      count_launches(p, EGS_STAGE_UPDATE, 1);
     }
     span_end(p, sp, band_update_flops(ts, nt, b, k));
     const int la = p->lookahead_sms;

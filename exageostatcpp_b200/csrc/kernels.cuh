@@ -114,6 +114,8 @@ void launch_ozaki_slice(const double* W, int ts, int t0, int ntiles, int row_til
 namespace egs {
 long long ozaki_targets(int ts, int nt, int band, int k, std::vector<int4>& out);
 long long ozaki_trsm_targets(int ts, int nt, int first, std::vector<int4>& out);
+void launch_panel_prepare(const double* W, int ts, int t0, int ntiles, int row_tile0, double* oz_scale,
+                          int8_t* slices, long long rows, float* inv_scale, __half* Ph, __half* Pl, cudaStream_t st);
 void launch_ozaki_slice_f32(const float* tiles0, int ts, int ntiles, int row_tile0, double* scale, int8_t* slices,
                             long long rows, cudaStream_t st);
 void launch_ozaki_slice_rows(const double* src, int ts, long long row0, double* scale, int8_t* slices,

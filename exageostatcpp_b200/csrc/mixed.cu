@@ -269,12 +269,26 @@ inv_apply_kernel(const double* __restrict__ X, int ts, const double* __restrict_
   __syncthreads();
   const int rl = threadIdx.x & (kNB - 1), g = threadIdx.x / kNB;
   const int i = blockIdx.x * kNB + rl;
-  double acc = 0.0;
+  // four interleaved sums per thread keep sixteen loads in flight; the column
+  // order within each sum and the final combination are fixed
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
   if (i < ts) {
-    for (int j = blockIdx.x * kNB + g; j < ts; j += 4)
-      if (j >= i) acc = fma(X[i + (long long)j * ts], ins[j], acc);
+    const double* xr = X + i;
+    int j = blockIdx.x * kNB + g;
+    for (; j + 12 < ts; j += 16) {
+      const double x0 = (j >= i) ? xr[(long long)j * ts] : 0.0;
+      const double x1 = (j + 4 >= i) ? xr[(long long)(j + 4) * ts] : 0.0;
+      const double x2 = (j + 8 >= i) ? xr[(long long)(j + 8) * ts] : 0.0;
+      const double x3 = (j + 12 >= i) ? xr[(long long)(j + 12) * ts] : 0.0;
+      a0 = fma(x0, ins[j], a0);
+      a1 = fma(x1, ins[j + 4], a1);
+      a2 = fma(x2, ins[j + 8], a2);
+      a3 = fma(x3, ins[j + 12], a3);
+    }
+    for (; j < ts; j += 4)
+      if (j >= i) a0 = fma(xr[(long long)j * ts], ins[j], a0);
   }
-  red[g][rl] = acc;
+  red[g][rl] = (a0 + a1) + (a2 + a3);
   __syncthreads();
   if (g == 0 && i < ts) out[i] = ((red[0][rl] + red[1][rl]) + red[2][rl]) + red[3][rl];
 }

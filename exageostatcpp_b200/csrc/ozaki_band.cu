@@ -37,11 +37,12 @@
 #include "common.cuh"
 #include "kernels.cuh"
 #include "mbarrier.cuh"
+#include "panel_scales.cuh"
 
 namespace egs {
 
 namespace oz {
-constexpr int S = 7;                       // slices per operand
+constexpr int S = kOzSlices;               // slices per operand
 constexpr int NGROUPS = S;                 // d = 2 .. S+1
 constexpr int BM = 128, BN = 64, BK = 64;  // BK int8 = one 64-byte swizzle row
 constexpr int STAGES = 2;
@@ -65,30 +66,98 @@ constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >
 // Slicing of the solved panel
 // ---------------------------------------------------------------------------
 
-__device__ __forceinline__ double oz_row_scale(double m) {
-  if (!(m > 0.0)) return (m == 0.0) ? 0.0 : __longlong_as_double(0x7ff8000000000000ll);  // NaN rows stay NaN
-  const long long bits = __double_as_longlong(m);
-  const int e = (int)((bits >> 52) & 0x7FF) - 1023;  // 2^e <= m < 2^(e+1) for normal m
-  return (e >= 1023) ? __longlong_as_double(0x7ff8000000000000ll) : ldexp(1.0, e + 1);
-}
-
-// Row scale of column-major tile t (tiles0 + t ts^2, global tile row
-// row_tile0 + t): scale = 2^e with max_c |A(r, c)| < 2^e; 0 rows get scale 0.
-template <typename T>
-__global__ void __launch_bounds__(256)
-ozaki_rowscale_kernel(const T* __restrict__ tiles0, int ts, int row_tile0, double* __restrict__ scale) {
+// Row scales and int8 slices -- and, with kSplit, the FP16 split scales and
+// hi/lo parts -- of ntiles column-major tiles (tiles0 + t ts^2, global tile row
+// row_tile0 + t), in one kernel: one CTA per 64-row strip of a tile reads the
+// strip once for its row maxima, then again in 64 x 64 blocks, transposed
+// through shared memory into the row-major (K contiguous) outputs
+// slices[p][row][c] and Ph / Pl[row][c].
+template <typename T, bool kSplit>
+__global__ void __launch_bounds__(256, 2)
+panel_prepare_kernel(const T* __restrict__ tiles0, int ts, int row_tile0, double* __restrict__ oz_scale,
+                     int8_t* __restrict__ slices, long long slice_stride, float* __restrict__ inv_scale,
+                     __half* __restrict__ Ph, __half* __restrict__ Pl) {
+  __shared__ double Sm[64][65];
   __shared__ double red[4][64];
+  __shared__ double s_oz[64], s_f16[64];
   const int t = blockIdx.y;
-  const int rl = threadIdx.x & 63, g = threadIdx.x >> 6;
-  const int r = blockIdx.x * 64 + rl;
-  const T* col = tiles0 + (long long)t * ts * ts + r;
-  double m = 0.0;
-  for (int c = g; c < ts; c += 4) m = fmax(m, fabs((double)col[(long long)c * ts]));
-  red[g][rl] = m;
-  __syncthreads();
-  if (g == 0) {
-    m = fmax(fmax(red[0][rl], red[1][rl]), fmax(red[2][rl], red[3][rl]));
-    scale[(long long)(row_tile0 + t) * ts + r] = oz_row_scale(m);
+  const int r0 = blockIdx.x * 64;
+  const T* src = tiles0 + (long long)t * ts * ts;
+  const long long grow0 = (long long)(row_tile0 + t) * ts + r0;
+  {
+    const int rl = threadIdx.x & 63, g = threadIdx.x >> 6;
+    const T* col = src + r0 + rl;
+    double m0 = 0.0, m1 = 0.0, m2 = 0.0, m3 = 0.0;  // ts is a multiple of 64
+#pragma unroll 4
+    for (int c = g; c < ts; c += 16) {
+      m0 = fmax(m0, fabs((double)col[(long long)c * ts]));
+      m1 = fmax(m1, fabs((double)col[(long long)(c + 4) * ts]));
+      m2 = fmax(m2, fabs((double)col[(long long)(c + 8) * ts]));
+      m3 = fmax(m3, fabs((double)col[(long long)(c + 12) * ts]));
+    }
+    red[g][rl] = fmax(fmax(m0, m1), fmax(m2, m3));
+    __syncthreads();
+    if (g == 0) {
+      const double m = fmax(fmax(red[0][rl], red[1][rl]), fmax(red[2][rl], red[3][rl]));
+      const double so = oz_row_scale(m);
+      oz_scale[grow0 + rl] = so;
+      s_oz[rl] = (so > 0.0) ? 1.0 / so : 0.0;  // exact: a power of two
+      if constexpr (kSplit) {
+        const float inv = f16_row_inv_scale(m);
+        inv_scale[grow0 + rl] = inv;
+        s_f16[rl] = (inv > 0.0f) ? 1.0 / (double)inv : 0.0;  // exact: a power of two
+      }
+    }
+  }
+  // Pass 2, 64 x 64 blocks; the next block's loads are issued before the
+  // current block is split.  Without kSplit every thread slices 16 columns of
+  // one row; with kSplit warps 0-3 slice and warps 4-7 split to FP16, 2 x 16
+  // columns of one row per thread, so neither needs both sets of registers.
+  T w[16];
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    const int e = q * 256 + threadIdx.x;
+    w[q] = src[(long long)(e >> 6) * ts + r0 + (e & 63)];
+  }
+  for (int c0 = 0; c0 < ts; c0 += 64) {
+    __syncthreads();  // Sm free; the scales are visible
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const int e = q * 256 + threadIdx.x;
+      Sm[e & 63][e >> 6] = (double)w[q];
+    }
+    if (c0 + 64 < ts) {
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const int e = q * 256 + threadIdx.x;
+        w[q] = src[(long long)(c0 + 64 + (e >> 6)) * ts + r0 + (e & 63)];
+      }
+    }
+    __syncthreads();
+    if constexpr (!kSplit) {
+      const int r = threadIdx.x >> 2, cq = (threadIdx.x & 3) * 16;
+      const double io = s_oz[r];
+      double v[16];
+#pragma unroll
+      for (int c = 0; c < 16; ++c) v[c] = Sm[r][cq + c] * io;  // |v| < 1
+      oz_emit_slices(v, slices + (grow0 + r) * ts + c0 + cq, slice_stride);
+    } else {
+      const int tt = threadIdx.x & 127, r = tt >> 1;
+      const bool to_f16 = threadIdx.x >= 128;  // warp-uniform
+      const double sc = to_f16 ? s_f16[r] : s_oz[r];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int cq = (tt & 1) * 32 + h * 16;
+        const long long off = (grow0 + r) * ts + c0 + cq;
+        double v[16];
+#pragma unroll
+        for (int c = 0; c < 16; ++c) v[c] = Sm[r][cq + c] * sc;
+        if (to_f16)
+          f16_emit_split(v, Ph + off, Pl + off);
+        else
+          oz_emit_slices(v, slices + off, slice_stride);  // |v| < 1
+      }
+    }
   }
 }
 
@@ -107,25 +176,6 @@ ozaki_rowscale_rm_kernel(const double* __restrict__ src, int ts, long long row0,
   if (lane == 0) scale[row0 + r] = oz_row_scale(m);
 }
 
-// S slices of 16 values (|v| < 1 after scaling) into 16-byte stores.
-__device__ __forceinline__ void oz_emit_slices(double (&v)[16], int8_t* dst, long long slice_stride) {
-#pragma unroll
-  for (int p = 0; p < oz::S; ++p) {
-    union {
-      int8_t b[16];
-      int4 q;
-    } out;
-#pragma unroll
-    for (int c = 0; c < 16; ++c) {
-      const double x = v[c] * 128.0;  // exact scaling
-      const double a = trunc(x);      // |a| <= 127
-      v[c] = x - a;                   // exact remainder, |v| < 1
-      out.b[c] = (int8_t)__double2int_rz(a);
-    }
-    *reinterpret_cast<int4*>(dst + p * slice_stride) = out.q;
-  }
-}
-
 // Slices of rows stored row by row (row r at src + r ts) into slice rows row0 + r.
 __global__ void __launch_bounds__(256)
 ozaki_slice_rm_kernel(const double* __restrict__ src, int ts, long long row0, const double* __restrict__ scale,
@@ -141,33 +191,6 @@ ozaki_slice_rm_kernel(const double* __restrict__ src, int ts, long long row0, co
 #pragma unroll
   for (int c = 0; c < 16; ++c) v[c] = row[c] * inv;
   oz_emit_slices(v, slices + (row0 + r) * ts + cq, slice_stride);
-}
-
-// Slices of 64 x 64 blocks of column-major tiles (tiles0 + t ts^2, global tile
-// row row_tile0 + t), transposed to row-major int8 rows (K contiguous):
-// slices[p][row][c], p = 0..S-1 for 2^-7 .. 2^-7S.
-template <typename T>
-__global__ void __launch_bounds__(256)
-ozaki_slice_kernel(const T* __restrict__ tiles0, int ts, int row_tile0, const double* __restrict__ scale,
-                   int8_t* __restrict__ slices, long long slice_stride) {
-  __shared__ double Sm[64][65];
-  const int t = blockIdx.z;
-  const int r0 = blockIdx.x * 64, c0 = blockIdx.y * 64;
-  const T* src = tiles0 + (long long)t * ts * ts;
-  for (int e = threadIdx.x; e < 64 * 64; e += 256) {
-    const int r = e & 63, c = e >> 6;
-    Sm[r][c] = (double)src[(long long)(c0 + c) * ts + r0 + r];
-  }
-  __syncthreads();
-  const long long grow0 = (long long)(row_tile0 + t) * ts + r0;
-  // thread: row r, 16 consecutive columns (16-byte stores per slice)
-  const int r = threadIdx.x >> 2, cq = (threadIdx.x & 3) * 16;
-  const double sc = scale[grow0 + r];
-  const double inv = (sc > 0.0) ? 1.0 / sc : 0.0;  // exact: a power of two
-  double v[16];
-#pragma unroll
-  for (int c = 0; c < 16; ++c) v[c] = Sm[r][cq + c] * inv;  // |v| < 1
-  oz_emit_slices(v, slices + (grow0 + r) * ts + c0 + cq, slice_stride);
 }
 
 // ---------------------------------------------------------------------------
@@ -497,19 +520,25 @@ int ozaki_tensor_map(void* storage, const int8_t* slices, int ts, long long rows
 void launch_ozaki_slice(const double* W, int ts, int t0, int ntiles, int row_tile0, double* scale, int8_t* slices,
                         long long rows, cudaStream_t st) {
   if (ntiles <= 0) return;
-  const double* tiles0 = W + (long long)t0 * ts * ts;
-  ozaki_rowscale_kernel<double><<<dim3(ts / 64, ntiles), 256, 0, st>>>(tiles0, ts, row_tile0 + t0, scale);
-  ozaki_slice_kernel<double><<<dim3(ts / 64, ts / 64, ntiles), 256, 0, st>>>(tiles0, ts, row_tile0 + t0, scale,
-                                                                              slices, rows * (long long)ts);
+  panel_prepare_kernel<double, false><<<dim3(ts / 64, ntiles), 256, 0, st>>>(
+      W + (long long)t0 * ts * ts, ts, row_tile0 + t0, scale, slices, rows * (long long)ts, nullptr, nullptr, nullptr);
+}
+
+// As launch_ozaki_slice, plus the FP16 split (inv_scale, Ph, Pl) of the same
+// rows for the split-FP16 update, from one read of the panel.
+void launch_panel_prepare(const double* W, int ts, int t0, int ntiles, int row_tile0, double* oz_scale,
+                          int8_t* slices, long long rows, float* inv_scale, __half* Ph, __half* Pl, cudaStream_t st) {
+  if (ntiles <= 0) return;
+  panel_prepare_kernel<double, true><<<dim3(ts / 64, ntiles), 256, 0, st>>>(
+      W + (long long)t0 * ts * ts, ts, row_tile0 + t0, oz_scale, slices, rows * (long long)ts, inv_scale, Ph, Pl);
 }
 
 // Contiguous FP32 column-major tiles (global tile rows row_tile0 ..).
 void launch_ozaki_slice_f32(const float* tiles0, int ts, int ntiles, int row_tile0, double* scale, int8_t* slices,
                             long long rows, cudaStream_t st) {
   if (ntiles <= 0) return;
-  ozaki_rowscale_kernel<float><<<dim3(ts / 64, ntiles), 256, 0, st>>>(tiles0, ts, row_tile0, scale);
-  ozaki_slice_kernel<float><<<dim3(ts / 64, ts / 64, ntiles), 256, 0, st>>>(tiles0, ts, row_tile0, scale, slices,
-                                                                             rows * (long long)ts);
+  panel_prepare_kernel<float, false><<<dim3(ts / 64, ntiles), 256, 0, st>>>(
+      tiles0, ts, row_tile0, scale, slices, rows * (long long)ts, nullptr, nullptr, nullptr);
 }
 
 // ts rows stored row by row at src into slice rows row0 .. row0 + ts.

@@ -49,6 +49,7 @@
 #include "common.cuh"
 #include "kernels.cuh"
 #include "mbarrier.cuh"
+#include "panel_scales.cuh"
 
 namespace egs {
 
@@ -95,17 +96,7 @@ panel_rowscale_kernel(const double* __restrict__ W, int ts, int t0, int row_tile
   __syncthreads();
   if (g == 0) {
     m = fmax(fmax(red[0][rl], red[1][rl]), fmax(red[2][rl], red[3][rl]));
-    const long long bits = __double_as_longlong(m);
-    const int e = (int)((bits >> 52) & 0x7FF) - 1023;
-    float inv;
-    if (e == 1024) {
-      inv = __int_as_float(0x7fc00000);  // NaN or Inf in the row: propagate
-    } else if (!(m > 0.0) || e < -120) {
-      inv = 0.0f;
-    } else {
-      inv = __int_as_float((e - 13 + 127) << 23);  // 2^(e-13), e <= 1023 - 13 keeps it finite for e <= 140
-    }
-    inv_scale[(long long)(row_tile0 + t) * ts + r] = inv;
+    inv_scale[(long long)(row_tile0 + t) * ts + r] = f16_row_inv_scale(m);
   }
 }
 
