@@ -22,8 +22,11 @@
 //   warp 0    TMA producer: per 64-wide K stage the S slices of the tile's 128
 //             A rows and 64 B rows (64-byte swizzle), 2-stage ring;
 //   warp 1    allocates 512 TMEM columns -- S groups of 64 int32 columns, one
-//             per d -- and issues S(S+1)/2 MMAs per 32-wide K step from one
-//             thread, the first of each group with accumulate = 0;
+//             per d, in order of d -- and issues the S(S+1)/2 slice products
+//             of a 32-wide K step from one thread as ten MMAs (the products of
+//             one A slice with up to four consecutive B slices form one MMA of
+//             N <= 256 over consecutive groups), the first K step with
+//             accumulate = 0;
 //   warps 2-9 epilogue: warp w reads TMEM lane quarter w % 4 and 32 of the 64
 //             columns, combines the groups in FP64 (smallest first), scales by
 //             2^(e_r + e_c) and subtracts from the FP64 band tile.
@@ -58,8 +61,9 @@ static_assert(NGROUPS * BN <= (int)TMEM_COLS, "groups fit in tensor memory");
 static_assert(SMEM_BYTES <= 232448, "shared memory per CTA");
 // Instruction descriptor of kind::i8: D S32 (bits 4-5 = 2), A and B signed 8-bit
 // (bits 7-9 = 1, bits 10-12 = 1), both K-major, N >> 3 at bits 17-22, M >> 4 at 24-28.
-constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
-                           ((uint32_t)(BM >> 4) << 24);
+constexpr uint32_t idesc_i8(int n) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+}
 }  // namespace oz
 
 // ---------------------------------------------------------------------------
@@ -211,34 +215,35 @@ __device__ __forceinline__ uint64_t sdesc_sw64(uint32_t addr) {
 // it from the collector and releases it (lastuse).  Consecutive MMAs with the
 // same A slice read it from shared memory once.
 template <int COLLECT>
-__device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+__device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                        uint32_t accumulate) {
   if constexpr (COLLECT == 0) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(oz::IDESC), "r"(accumulate)
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
         : "memory");
   } else if constexpr (COLLECT == 1) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::i8.collector::a::fill [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(oz::IDESC), "r"(accumulate)
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
         : "memory");
   } else if constexpr (COLLECT == 2) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::i8.collector::a::use [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(oz::IDESC), "r"(accumulate)
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
         : "memory");
   } else {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::i8.collector::a::lastuse [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(oz::IDESC), "r"(accumulate)
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
         : "memory");
   }
 }
@@ -393,24 +398,30 @@ ozaki_band_kernel(const __grid_constant__ CUtensorMap tm_s, const __grid_constan
           oz_fence_after();
           const uint32_t sa = smem_u32(smem + s * STAGE_BYTES);
           const uint32_t sb = sa + S * A_SLICE;
-          // A slice p outermost: its products with B slices q = 1 .. S+1-p go to
-          // the groups d = p + q and take A from the collector after the first
-          // (integer sums are exact, so the order within a group is free).
+          // A slice p against B slices q = 1 .. S+1-p: group d = p + q sits at
+          // TMEM columns (d - 2) BN and the B slices are stacked in shared
+          // memory, so the products of A_p with B_q .. B_q+m-1 are one MMA of
+          // N = m BN into the columns of groups p+q .. p+q+m-1 (N <= 256: at
+          // most four slices a time).  Ten MMAs per 32-wide K step; an A slice
+          // used by two of them is read once through the collector buffer.
 #pragma unroll
           for (int kk = 0; kk < BK / 32; ++kk) {
 #pragma unroll
             for (int p = 1; p <= S; ++p) {
               const uint64_t ad = sdesc_sw64(sa + (p - 1) * A_SLICE + kk * 32);
               const uint32_t acc = (kt > 0 || kk > 0 || p > 1) ? 1u : 0u;  // p = 1 opens every group
+              constexpr int kMaxSlices = 256 / BN;
               const int qmax = S + 1 - p;
+              const int nmma = (qmax + kMaxSlices - 1) / kMaxSlices;
 #pragma unroll
-              for (int q = 1; q <= qmax; ++q) {
-                const uint32_t dcol = tmem_base + (uint32_t)((p + q - 2) * BN);
-                const uint64_t bd = sdesc_sw64(sb + (q - 1) * B_SLICE + kk * 32);
-                if (qmax == 1) umma_i8<0>(dcol, ad, bd, acc);
-                else if (q == 1) umma_i8<1>(dcol, ad, bd, acc);
-                else if (q < qmax) umma_i8<2>(dcol, ad, bd, acc);
-                else umma_i8<3>(dcol, ad, bd, acc);
+              for (int q0 = 1; q0 <= qmax; q0 += kMaxSlices) {
+                const int m = (qmax - q0 + 1) < kMaxSlices ? (qmax - q0 + 1) : kMaxSlices;
+                const uint32_t dcol = tmem_base + (uint32_t)((p + q0 - 2) * BN);
+                const uint64_t bd = sdesc_sw64(sb + (q0 - 1) * B_SLICE + kk * 32);
+                const uint32_t id = idesc_i8(m * BN);
+                if (nmma == 1) umma_i8<0>(dcol, ad, bd, id, acc);
+                else if (q0 == 1) umma_i8<1>(dcol, ad, bd, id, acc);
+                else umma_i8<3>(dcol, ad, bd, id, acc);
               }
             }
           }
