@@ -292,69 +292,47 @@ void free_problem(egs_problem* p) {
 }
 
 // Panel of step k (tile column k of an nt-tile lower layout): factor diagonal
-// tile (k, k) and solve tiles (k+1 .. nt-1, k) against it.  Two-level blocking:
-// the tile's columns go in outer blocks of kOuterBlock; inside an outer block
-// each 64-column block is factored (64x64 potrf), solved for every row below it
-// (row solve) and applied with K = 64 only to the remaining columns of the same
-// outer block; the columns right of the outer block then get one update with
-// K = kOuterBlock.  The K = 64 updates thus touch at most 192 columns, which
-// cuts the read-modify-write traffic of the panel's C operand by ~2.5x against
-// single-level 64-blocking.  col_base is the global column of the tile (for
-// the LAPACK-style info of a failed pivot).  Returns the launch count in *nl.
+// tile (k, k) and solve tiles (k+1 .. nt-1, k) against it, as one right-looking
+// blocked factorisation of the tall tile column.  Two-level blocking: the
+// tile's columns go in outer blocks of kOuterBlock; inside an outer block each
+// 64-column block is factored (64x64 potrf), every row below it -- the rest of
+// the diagonal tile and all tiles below -- is solved in one row-solve launch,
+// and one K = 64 update covers the remaining columns of the same outer block
+// for all those rows; the columns right of the outer block then get one
+// update with K = kOuterBlock.  The K = 64 updates thus touch at most 192
+// columns, which cuts the read-modify-write traffic of the panel's C operand
+// by ~2.5x against single-level 64-blocking.  Every element receives the same
+// operations in the same order as with the diagonal tile factored first.
+// col_base is the global column of the tile (for the LAPACK-style info of a
+// failed pivot).  Returns the launch count in *nl.
 int enqueue_panel(double* tiles, const void* tmap, int ts, int nt, int k, int col_base, int* info, int* err,
                   cudaStream_t st, long long* nl, int max_ctas = 0) {
   const long long skk = tile_slot(k, k, nt);
-  const int ntl = nt - 1 - k;
-  const long long s0 = ntl > 0 ? tile_slot(k + 1, k, nt) : 0;
+  const int ntp = nt - k;         // tiles of the column, the diagonal one first
   const int drow = k * ts;
-  const int below = (k + 1) * ts;
+  const int row_end = nt * ts;    // end of the column's global rows
   for (int KB = 0; KB < ts; KB += kOuterBlock) {
     const int KE = std::min(ts, KB + kOuterBlock);
     for (int kb = KB; kb < KE; kb += kInnerBlock) {
       launch_potrf_diag_block(tiles, ts, skk, kb, col_base, info, st);
       ++*nl;
-      if (kb + kInnerBlock < ts) {
-        launch_trsm_rows(tiles, ts, skk, 1, kb + kInnerBlock, kb, skk, st);
+      const int r0 = drow + kb + kInnerBlock;  // first row below the block
+      if (r0 >= row_end) continue;
+      launch_trsm_rows_panel(tiles, ts, skk, ntp, kb + kInnerBlock, 0, kb, skk, st);
+      ++*nl;
+      if (kb + kInnerBlock < KE) {
+        int rc = launch_gemm_rows(tmap, tiles, ts, nt, row_end - r0, KE - kb - kInnerBlock, kInnerBlock, r0, kb, k,
+                                  r0, kb, k, r0, r0, 1, err, st, max_ctas);
+        if (rc != EGS_OK) return rc;
         ++*nl;
-        if (kb + kInnerBlock < KE) {
-          const int r0 = drow + kb + kInnerBlock;
-          int rc = launch_gemm_rows(tmap, tiles, ts, nt, ts - kb - kInnerBlock, KE - kb - kInnerBlock, kInnerBlock,
-                                    r0, kb, k, r0, kb, k, r0, r0, 1, err, st, max_ctas);
-          if (rc != EGS_OK) return rc;
-          ++*nl;
-        }
       }
     }
     if (KE < ts) {
       const int r0 = drow + KE;
-      int rc = launch_gemm_rows(tmap, tiles, ts, nt, ts - KE, ts - KE, KE - KB, r0, KB, k, r0, KB, k, r0, r0, 1, err,
-                                st, max_ctas);
+      int rc = launch_gemm_rows(tmap, tiles, ts, nt, row_end - r0, ts - KE, KE - KB, r0, KB, k, r0, KB, k, r0, r0, 1,
+                                err, st, max_ctas);
       if (rc != EGS_OK) return rc;
       ++*nl;
-    }
-  }
-  if (ntl > 0) {
-    const int m = ntl * ts;
-    for (int KB = 0; KB < ts; KB += kOuterBlock) {
-      const int KE = std::min(ts, KB + kOuterBlock);
-      for (int kb = KB; kb < KE; kb += kInnerBlock) {
-        launch_trsm_rows(tiles, ts, s0, ntl, 0, kb, skk, st);
-        ++*nl;
-        if (kb + kInnerBlock < KE) {
-          const int brow = drow + kb + kInnerBlock;
-          int rc = launch_gemm_rows(tmap, tiles, ts, nt, m, KE - kb - kInnerBlock, kInnerBlock, below, kb, k, brow, kb,
-                                    k, below, brow, 0, err, st, max_ctas);
-          if (rc != EGS_OK) return rc;
-          ++*nl;
-        }
-      }
-      if (KE < ts) {
-        const int brow = drow + KE;
-        int rc = launch_gemm_rows(tmap, tiles, ts, nt, m, ts - KE, KE - KB, below, KB, k, brow, KB, k, below, brow, 0,
-                                  err, st, max_ctas);
-        if (rc != EGS_OK) return rc;
-        ++*nl;
-      }
     }
   }
   return EGS_OK;

@@ -23,6 +23,8 @@ void launch_potrf_diag_block(double* tiles, int ts, long long slot, int off, int
                              cudaStream_t st);
 void launch_trsm_rows(double* tiles, int ts, long long slot0, int ntiles, int row0, int col0,
                       long long lslot, cudaStream_t st);
+void launch_trsm_rows_panel(double* tiles, int ts, long long slot0, int ntiles, int row0_first, int row0, int col0,
+                            long long lslot, cudaStream_t st);
 void launch_trsv_diag(const double* tiles, int ts, long long slot, double* zk, cudaStream_t st);
 void launch_gemv_panel(const double* tiles, int ts, int nt, int k, double* z, cudaStream_t st);
 void launch_trsv_t_diag(const double* tiles, int ts, long long slot, double* zk, cudaStream_t st);

@@ -32,23 +32,35 @@ void launch_potrf_diag_block(double* tiles, int ts, long long slot, int off, int
   potrf_diag_block_kernel<<<1, 256, 0, st>>>(tiles, ts, slot, off, col_base, info);
 }
 
-// X := A * L^-T for the 64-column block [col0, col0+64) of rows [row0, ts) of
-// ntiles consecutive tiles starting at slot0; L is the factored 64x64 diagonal
-// block at (col0, col0) of tile lslot (trsm_rows_body).
+// X := A * L^-T for the 64-column block [col0, col0+64) of ntiles consecutive
+// tiles starting at slot0: rows [row0_first, ts) of the first tile and rows
+// [row0, ts) of the others; L is the factored 64x64 diagonal block at (col0,
+// col0) of tile lslot (trsm_rows_body).
 __global__ void __launch_bounds__(128)
-trsm_rows_kernel(double* __restrict__ tiles, int ts, long long slot0, int row0, int col0,
-                 long long lslot) {
+trsm_rows_kernel(double* __restrict__ tiles, int ts, long long slot0, int grid_row0, int row0_first, int row0,
+                 int col0, long long lslot) {
+  const int lo = blockIdx.y == 0 ? row0_first : row0;
+  int row = grid_row0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (row < lo) row = ts;  // takes part in loading L only
   trsm_rows_body<128>(tiles + (slot0 + blockIdx.y) * (long long)ts * ts, tiles + lslot * (long long)ts * ts, ts,
-                 row0 + blockIdx.x * blockDim.x + threadIdx.x, col0);
+                      row, col0);
 }
 
 void launch_trsm_rows(double* tiles, int ts, long long slot0, int ntiles, int row0, int col0,
                       long long lslot, cudaStream_t st) {
-  const int rows = ts - row0;
-  if (rows <= 0 || ntiles <= 0) return;
+  launch_trsm_rows_panel(tiles, ts, slot0, ntiles, row0, row0, col0, lslot, st);
+}
+
+void launch_trsm_rows_panel(double* tiles, int ts, long long slot0, int ntiles, int row0_first, int row0, int col0,
+                            long long lslot, cudaStream_t st) {
+  if (ntiles <= 0) return;
+  if (ntiles == 1) row0 = row0_first;
+  const int first = row0 < row0_first ? row0 : row0_first;
+  const int rows = ts - first;
+  if (rows <= 0) return;
   const int threads = 128;
-  trsm_rows_kernel<<<dim3((rows + threads - 1) / threads, ntiles), threads, 0, st>>>(tiles, ts, slot0,
-                                                                                    row0, col0, lslot);
+  trsm_rows_kernel<<<dim3((rows + threads - 1) / threads, ntiles), threads, 0, st>>>(tiles, ts, slot0, first,
+                                                                                    row0_first, row0, col0, lslot);
 }
 
 // Forward substitution on one diagonal tile: z_k := L_kk^-1 z_k (trsv_diag_body).
