@@ -260,17 +260,21 @@ __device__ __forceinline__ void oz_tma_3d(void* dst, const CUtensorMap* map, uin
       "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
       : "memory");
 }
-__device__ __forceinline__ void tmem_ld16_i32(uint32_t taddr, int (&v)[16]) {
-  uint32_t r[16];
+// 32 consecutive int32 columns of this warp's TMEM lane quarter, one load and
+// one wait.
+__device__ __forceinline__ void tmem_ld32_i32(uint32_t taddr, int (&v)[32]) {
+  uint32_t r[32];
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-      "%15}, [%16];"
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
       : "r"(taddr));
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = (int)r[i];
+  for (int i = 0; i < 32; ++i) v[i] = (int)r[i];
 }
 
 // Targets of one step: target t = (i, j, first work item, diagonal flag);
@@ -454,13 +458,10 @@ ozaki_band_kernel(const __grid_constant__ CUtensorMap tm_s, const __grid_constan
 #pragma unroll 1
       for (int g = NGROUPS - 1; g >= 0; --g) {
         const double f = __longlong_as_double((long long)(1023 - 7 * (g + 2)) << 52);  // 2^(-7(g+2))
+        int v[32];
+        tmem_ld32_i32(tl + (uint32_t)(g * BN), v);
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          int v[16];
-          tmem_ld16_i32(tl + (uint32_t)(g * BN + h * 16), v);
-#pragma unroll
-          for (int c = 0; c < 16; ++c) acc[h * 16 + c] = fma((double)v[c], f, acc[h * 16 + c]);
-        }
+        for (int c = 0; c < 32; ++c) acc[c] = fma((double)v[c], f, acc[c]);
       }
       oz_fence_before();
       __syncwarp();

@@ -59,7 +59,7 @@ __device__ __forceinline__ void potrf64_body(double* __restrict__ T, int ts, int
     if (!(d > 0.0)) atomicCAS(info, 0, gcol0 + 1);
     const double ljj = sqrt(d);
     piv[0] = ljj;
-    pinv[0] = 1.0 / ljj;
+    pinv[0] = __drcp_rn(ljj);  // correctly rounded, as 1.0 / ljj
   }
   __syncthreads();
   constexpr int CW = NTHR / 32 < 8 ? NTHR / 32 : 8;
@@ -83,7 +83,7 @@ __device__ __forceinline__ void potrf64_body(double* __restrict__ T, int ts, int
           if (!(d > 0.0)) atomicCAS(info, 0, gcol0 + c1 + 1);
           const double ljj = sqrt(d);
           piv[c1] = ljj;
-          pinv[c1] = 1.0 / ljj;
+          pinv[c1] = __drcp_rn(ljj);
         }
         c1 += CW;
       }
