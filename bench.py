@@ -496,6 +496,16 @@ def main():
            "dot": abs(dot - pdot) / abs(pdot), "against": "plain FP64 B200 path at the same N"}
 
     # --- rooflines of the update kernels (CUDA events around every launch) ---------------
+    # DRAM bytes (read + write) per algorithmic flop of each kernel, from one ncu
+    # capture at N = 16,384 (profiles/split_gemm_kernel_n16384.md: 792,716,032 B
+    # for 78 target tiles of 2 * 1024^3 flops; profiles/ozaki_band_kernel_n16384.md:
+    # 644,593,920 B for the band update of step 0, 7.410e10 FP64-equivalent flops).
+    # Both kernels' traffic grows with their target tiles, so a launch's traffic
+    # is this ratio times its flops.
+    split_bytes_per_flop = 792716032.0 / (78 * 2.0 * 1024 ** 3)
+    ozaki_bytes_per_flop = 644593920.0 / 7.410e10
+    traffic_note = ("DRAM read + write bytes per flop from one ncu capture at N=16384, times this launch's "
+                    "algorithmic flops")
     lo = egs.STAGES.index("update_low")
     bf16_peak = peaks.get("bf16_tflops_sustained") or 1386.0
     roofs = []
@@ -509,7 +519,9 @@ def main():
                       "executed_tflops": 3.0 * a, "frac_executed": 3.0 * a / bf16_peak,
                       "note": "achieved counts the algorithmic 2*ts^3 flops per target tile; the kernel executes "
                               "three FP16 products per tile (hi*hi, hi*lo, lo*hi)",
-                      "traffic": None, "launches": n_l, "ms_per_eval": float(stage_ms[lo]) / args.steps,
+                      "traffic": split_bytes_per_flop * stage_flops[lo] / max(n_l, 1), "traffic_unit": "B",
+                      "traffic_source": traffic_note,
+                      "launches": n_l, "ms_per_eval": float(stage_ms[lo]) / args.steps,
                       "flops_per_launch": stage_flops[lo] / max(n_l, 1)})
     if stage_ms[up] > 0:
         a = stage_flops[up] / (stage_ms[up] * 1e-3) / 1e12
@@ -517,14 +529,16 @@ def main():
         int8_peak = 2.0 * bf16_peak
         roofs.append({"bound": "tensor",
                       "kernel": "ozaki_band_kernel (FP64-class band update: 7 signed 7-bit slices per operand, "
-                                "exact int32 products on tcgen05 kind::i8; stage includes the slicing)",
+                                "exact int32 products on tcgen05 kind::i8, ten MMAs of N <= 256 per K step)",
                       "achieved": a, "peak": fp64_peak, "unit": "TFLOP/s", "frac": a / fp64_peak,
                       "peak_source": "FP64-equivalent flops against cuBLAS DGEMM 8192^3 measured in this run "
                                      "(MEASURED_PEAKS.json has no FP64 entry)",
                       "executed_int8_tops": 28.0 * a, "frac_executed_of_int8": 28.0 * a / int8_peak,
                       "int8_peak_source": "2x MEASURED_PEAKS.json bf16_tflops_sustained (the int8 rate is twice "
                                           "the bf16 rate on B200)",
-                      "traffic": None, "launches": n_u, "ms_per_eval": float(stage_ms[up]) / args.steps,
+                      "traffic": ozaki_bytes_per_flop * stage_flops[up] / max(n_u, 1), "traffic_unit": "B",
+                      "traffic_source": traffic_note,
+                      "launches": n_u, "ms_per_eval": float(stage_ms[up]) / args.steps,
                       "flops_per_launch": stage_flops[up] / max(n_u, 1)})
     roofs.sort(key=lambda r: -r["ms_per_eval"])
     line = {
