@@ -335,65 +335,125 @@ void launch_mixed_solve(const double* band, const float* off, const double* inv,
 
 // ---------------------------------------------------------------------------
 // Refinement residual r = z - C(theta) v, C regenerated in FP64.
-// Block (row block of 256 rows, column split s): partial[s][i] = sum over the
-// columns of split s of C(i, j) v_j, in a fixed order; the reduce kernel adds
-// the splits in order.  Only the n real rows / columns take part.
+// C is symmetric, so every pair i > j is evaluated once and used twice: for row
+// i (C(i, j) v_j) and for column j (C(i, j) v_i).  The lower triangle of
+// 256-row blocks is covered by square super-blocks of 1 .. kResSuper blocks a
+// side (res_side), one CTA each.  A thread owns row i of the current row block: its row sum
+// stays in a register across the super-block's column blocks, and the column
+// sums are formed by warp butterflies and a fixed-order sum over the warps,
+// kept per column block in shared memory by the thread that owns the column.  Super-block
+// partials go to rowpart[sbj][i] and colpart[sbi][j]; the reduce kernel adds
+// them in a fixed order.  Only the n real rows / columns take part.
 // ---------------------------------------------------------------------------
-constexpr int kResSplits = 8;
-constexpr int kResChunk = 256;
+constexpr int kResBlk = 256;    // rows (and columns) per block = threads per CTA
+constexpr int kResSuper = 8;    // most blocks per super-block side
 
-__global__ void __launch_bounds__(256)
+__host__ __device__ __forceinline__ int res_blocks(int n) { return (n + kResBlk - 1) / kResBlk; }
+// Blocks per super-block side: as many as keep at least ~24 super-blocks per
+// side (hundreds of CTAs), at most kResSuper.
+__host__ __device__ __forceinline__ int res_side(int n) {
+  const int s = res_blocks(n) / 24;
+  return s < 1 ? 1 : (s > kResSuper ? kResSuper : s);
+}
+__host__ __device__ __forceinline__ int res_supers(int n) { return (res_blocks(n) + res_side(n) - 1) / res_side(n); }
+
+__global__ void __launch_bounds__(kResBlk, 3)
 matern_residual_partial_kernel(const double* __restrict__ x, const double* __restrict__ y,
                                const double* __restrict__ v, int n, const MaternParams* __restrict__ pp,
-                               const double* __restrict__ ktab, double* __restrict__ partial) {
+                               const double* __restrict__ ktab, double* __restrict__ rowpart,
+                               double* __restrict__ colpart) {
   __shared__ double stab[kKtabDoubles];
-  __shared__ double xs[kResChunk], ys[kResChunk], vs[kResChunk];
+  __shared__ double xs[kResBlk], ys[kResBlk], vs[kResBlk];
+  __shared__ double red[kResBlk / 32][kResBlk];
+  __shared__ double colacc[kResSuper][kResBlk];  // column sums of each column block (thread = column)
   const MaternParams p = *pp;
   stage_ktab(stab, ktab, p);
-  const int i = blockIdx.x * 256 + threadIdx.x;
-  const int per = (n + kResSplits - 1) / kResSplits;
-  const int j0 = blockIdx.y * per, j1 = min(n, j0 + per);
-  const bool row = i < n;
-  const double xi = row ? x[i] : 0.0, yi = row ? y[i] : 0.0;
-  double acc = 0.0;
-  for (int jc = j0; jc < j1; jc += kResChunk) {
-    const int m = min(kResChunk, j1 - jc);
-    __syncthreads();
-    if (threadIdx.x < m) {
-      xs[threadIdx.x] = x[jc + threadIdx.x];
-      ys[threadIdx.x] = y[jc + threadIdx.x];
-      vs[threadIdx.x] = v[jc + threadIdx.x];
+  // super-block (sbi, sbj), sbj <= sbi, from the linear index
+  const int L = blockIdx.x;
+  int sbi = (int)((sqrt(8.0 * (double)L + 1.0) - 1.0) * 0.5);
+  while ((sbi + 1) * (sbi + 2) / 2 <= L) ++sbi;
+  while (sbi * (sbi + 1) / 2 > L) --sbi;
+  const int sbj = L - sbi * (sbi + 1) / 2;
+  const int nb = res_blocks(n), side = res_side(n);
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const int bj0 = sbj * side, bj1 = min(nb, bj0 + side);
+  const int bi0 = sbi * side, bi1 = min(nb, bi0 + side);
+#pragma unroll
+  for (int q = 0; q < kResSuper; ++q) colacc[q][t] = 0.0;
+  for (int bi = bi0; bi < bi1; ++bi) {
+    const int i = bi * kResBlk + t;
+    const bool row = i < n;
+    const double xi = row ? x[i] : 0.0, yi = row ? y[i] : 0.0, vi = row ? v[i] : 0.0;
+    double racc = 0.0;
+#pragma unroll 1
+    for (int q = 0; q < side; ++q) {
+      const int bj = bj0 + q;
+      if (bj >= bj1 || bj > bi) break;  // uniform over the CTA
+      const int jb = bj * kResBlk;
+      __syncthreads();  // previous column block done with xs / ys / vs / red
+      if (jb + t < n) {
+        xs[t] = x[jb + t];
+        ys[t] = y[jb + t];
+        vs[t] = v[jb + t];
+      } else {
+        xs[t] = ys[t] = vs[t] = 0.0;
+      }
+      __syncthreads();
+      const bool diag = (bj == bi);
+      const int m = min(kResBlk, n - jb);
+      for (int jj = 0; jj < m; ++jj) {
+        double c = 0.0;
+        if (row && (!diag || jj <= t)) c = matern_from_dist_tab(euclid_dist(xi, yi, xs[jj], ys[jj]), p, stab);
+        racc = fma(c, vs[jj], racc);
+        // column jj gets C(i, jj) v_i from every row i below it (i > j)
+        double cc = (!diag || jj < t) ? c * vi : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) cc += __shfl_xor_sync(0xffffffffu, cc, o);
+        if (lane == 0) red[warp][jj] = cc;
+      }
+      __syncthreads();
+      double sum = 0.0;
+#pragma unroll
+      for (int w = 0; w < kResBlk / 32; ++w) sum += red[w][t];
+      colacc[q][t] += sum;
     }
-    __syncthreads();
-    if (row) {
-      for (int q = 0; q < m; ++q) acc = fma(matern_from_dist_tab(euclid_dist(xi, yi, xs[q], ys[q]), p, stab), vs[q], acc);
-    }
+    if (row) rowpart[(long long)sbj * n + i] = racc;
   }
-  if (row) partial[(long long)blockIdx.y * n + i] = acc;
+  for (int q = 0; q < side; ++q) {
+    const int j = (bj0 + q) * kResBlk + t;
+    if (bj0 + q < bj1 && j < n) colpart[(long long)sbi * n + j] = colacc[q][t];
+  }
 }
 
+// r_i = z_i - (row partials of super-block columns 0 .. sb(i) + column partials
+// of super-block rows sb(i) .. ns-1), each in a fixed order; padding rows get 0.
 __global__ void __launch_bounds__(256)
-residual_reduce_kernel(const double* __restrict__ z, const double* __restrict__ partial, int n, int np,
-                       double* __restrict__ r) {
+residual_reduce_kernel(const double* __restrict__ z, const double* __restrict__ rowpart,
+                       const double* __restrict__ colpart, int n, int np, double* __restrict__ r) {
   const int i = blockIdx.x * 256 + threadIdx.x;
   if (i >= np) return;
   if (i >= n) {
     r[i] = 0.0;
     return;
   }
-  double s = 0.0;
-  for (int q = 0; q < kResSplits; ++q) s += partial[(long long)q * n + i];
-  r[i] = z[i] - s;
+  const int sb = (i / kResBlk) / res_side(n), ns = res_supers(n);
+  double a = 0.0, b = 0.0;
+  for (int q = 0; q <= sb; ++q) a += rowpart[(long long)q * n + i];
+  for (int q = sb; q < ns; ++q) b += colpart[(long long)q * n + i];
+  r[i] = z[i] - (a + b);
 }
 
-long long residual_scratch_doubles(int n) { return (long long)kResSplits * n; }
+long long residual_scratch_doubles(int n) { return 2LL * res_supers(n) * n; }
 
 void launch_matern_residual(const double* x, const double* y, const double* z, const double* v, int n, int np,
                             const MaternParams* params, const double* ktab, double* scratch, double* r,
                             cudaStream_t st) {
-  matern_residual_partial_kernel<<<dim3((n + 255) / 256, kResSplits), 256, 0, st>>>(x, y, v, n, params, ktab,
-                                                                                     scratch);
-  residual_reduce_kernel<<<(np + 255) / 256, 256, 0, st>>>(z, scratch, n, np, r);
+  const int ns = res_supers(n);
+  double* rowpart = scratch;
+  double* colpart = scratch + (long long)ns * n;
+  const unsigned grid = (unsigned)((long long)ns * (ns + 1) / 2);
+  matern_residual_partial_kernel<<<grid, kResBlk, 0, st>>>(x, y, v, n, params, ktab, rowpart, colpart);
+  residual_reduce_kernel<<<(np + 255) / 256, 256, 0, st>>>(z, rowpart, colpart, n, np, r);
 }
 
 // result = (loglik, logdet, z^T (v + w), info) with the refined solution v + w.
