@@ -63,6 +63,13 @@ struct egs_problem {
   long long graph_launches[EGS_NUM_STAGES] = {};
   long long evals = 0;
   bool graphs_enabled = true;
+  // The same with the per-stage timing events captured as event-record nodes
+  // (used while profiling); pgraphs_ok turns off only this variant.
+  cudaGraph_t pgraph = nullptr;
+  cudaGraphExec_t pgraph_exec = nullptr;
+  int pgraph_band = -1;
+  long long pgraph_launches[EGS_NUM_STAGES] = {};
+  bool pgraphs_ok = true;
   // Per-stage accounting: launch counts always, CUDA-event times when profiling.
   bool profiling = false;
   struct Span {
@@ -73,6 +80,7 @@ struct egs_problem {
   std::vector<cudaEvent_t> events;
   size_t events_used = 0;
   std::vector<Span> spans;
+  std::vector<Span> pgraph_spans;  // the spans of one replay of pgraph
   double stage_ms[EGS_NUM_STAGES] = {};
   double stage_flops[EGS_NUM_STAGES] = {};
   long long stage_launches[EGS_NUM_STAGES] = {};
@@ -162,31 +170,48 @@ cudaEvent_t take_event(egs_problem* p) {
 int span_begin(egs_problem* p, int stage, cudaStream_t on = nullptr) {
   if (!p->profiling) return -1;
   egs_problem::Span s{stage, take_event(p), take_event(p), 0.0};
-  cudaEventRecord(s.a, on ? on : p->stream);
+  // "external" records: inside a stream capture they become event-record
+  // nodes of the graph (a plain record would only mark a dependency)
+  cudaEventRecordWithFlags(s.a, on ? on : p->stream, cudaEventRecordExternal);
   p->spans.push_back(s);
   return (int)p->spans.size() - 1;
 }
 
 void span_end(egs_problem* p, int idx, double flops, cudaStream_t on = nullptr) {
   if (idx < 0) return;
-  cudaEventRecord(p->spans[idx].b, on ? on : p->stream);
+  cudaEventRecordWithFlags(p->spans[idx].b, on ? on : p->stream, cudaEventRecordExternal);
   p->spans[idx].flops = flops;
 }
 
 void count_launches(egs_problem* p, int stage, long long n) { p->stage_launches[stage] += n; }
 
-// After the stream has been synchronised: fold the recorded spans into the totals.
-void collect_spans(egs_problem* p) {
+// After the stream has been synchronised: fold the recorded spans into the
+// totals; returns how many spans had a valid time.
+int collect_spans(egs_problem* p) {
+  int timed = 0;
   for (auto& s : p->spans) {
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, s.a, s.b) == cudaSuccess) {
       p->stage_ms[s.stage] += ms;
       p->stage_flops[s.stage] += s.flops;
+      ++timed;
     }
   }
   cudaGetLastError();
   p->spans.clear();
   p->events_used = 0;
+  return timed;
+}
+
+// Both captured evaluations (after a change of the problem's layout or method).
+void drop_graphs(egs_problem* p) {
+  if (p->graph_exec) cudaGraphExecDestroy(p->graph_exec);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  if (p->pgraph_exec) cudaGraphExecDestroy(p->pgraph_exec);
+  if (p->pgraph) cudaGraphDestroy(p->pgraph);
+  p->graph_exec = p->pgraph_exec = nullptr;
+  p->graph = p->pgraph = nullptr;
+  p->pgraph_spans.clear();
 }
 
 // Device buffers come from the stream-ordered allocator on the owning
@@ -283,8 +308,7 @@ void free_problem(egs_problem* p) {
   pinned_release(p->hparams);
   pinned_release(p->hresult);
   pinned_release(p->hflags);
-  if (p->graph_exec) cudaGraphExecDestroy(p->graph_exec);
-  if (p->graph) cudaGraphDestroy(p->graph);
+  drop_graphs(p);
   if (p->stream) cudaStreamSynchronize(p->stream);
   if (p->own_stream && p->stream) cudaStreamDestroy(p->stream);
   for (cudaEvent_t e : p->events) cudaEventDestroy(e);
@@ -870,19 +894,32 @@ int reject_mixed(const egs_problem* p, const char* where) {
   return EGS_ERR_STATE;
 }
 
-// Capture the parameter upload and enqueue_eval into a graph.  Capture problems
-// (an unsupported call inside the stream) disable replay for this problem.
-int capture_eval(egs_problem* p) {
-  if (p->graph_exec) cudaGraphExecDestroy(p->graph_exec);
-  if (p->graph) cudaGraphDestroy(p->graph);
-  p->graph_exec = nullptr;
-  p->graph = nullptr;
+// Capture the parameter upload and enqueue_eval into a graph: the plain one,
+// or with prof the one that also records the per-stage timing events.  Capture
+// problems (an unsupported call inside the stream) disable that kind of replay
+// for this problem.
+int capture_eval(egs_problem* p, bool prof) {
+  cudaGraph_t& graph = prof ? p->pgraph : p->graph;
+  cudaGraphExec_t& exec = prof ? p->pgraph_exec : p->graph_exec;
+  long long* launches = prof ? p->pgraph_launches : p->graph_launches;
+  if (exec) cudaGraphExecDestroy(exec);
+  if (graph) cudaGraphDestroy(graph);
+  exec = nullptr;
+  graph = nullptr;
+  auto disable = [&]() {
+    if (prof) {
+      p->pgraphs_ok = false;
+    } else {
+      p->graphs_enabled = false;
+    }
+  };
   long long before[EGS_NUM_STAGES];
   for (int i = 0; i < EGS_NUM_STAGES; ++i) before[i] = p->stage_launches[i];
+  const size_t span0 = p->spans.size();
   cudaStream_t st = p->stream;
   if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
     cudaGetLastError();
-    p->graphs_enabled = false;
+    disable();
     return EGS_OK;
   }
   cudaMemcpyAsync(p->dparams, p->hparams, sizeof(MaternParams), cudaMemcpyHostToDevice, st);
@@ -890,18 +927,22 @@ int capture_eval(egs_problem* p) {
   cudaGraph_t g = nullptr;
   const cudaError_t e = cudaStreamEndCapture(st, &g);
   for (int i = 0; i < EGS_NUM_STAGES; ++i) {
-    p->graph_launches[i] = p->stage_launches[i] - before[i];
+    launches[i] = p->stage_launches[i] - before[i];
     p->stage_launches[i] = before[i];
   }
-  if (rc != EGS_OK || e != cudaSuccess || !g || cudaGraphInstantiate(&p->graph_exec, g, 0) != cudaSuccess) {
+  // the captured spans ran nothing yet: keep them for the replays
+  if (prof) p->pgraph_spans.assign(p->spans.begin() + span0, p->spans.end());
+  p->spans.resize(span0);
+  if (rc != EGS_OK || e != cudaSuccess || !g || cudaGraphInstantiate(&exec, g, 0) != cudaSuccess) {
     cudaGetLastError();
     if (g) cudaGraphDestroy(g);
-    p->graph_exec = nullptr;
-    p->graphs_enabled = false;
+    exec = nullptr;
+    if (prof) p->pgraph_spans.clear();
+    disable();
     return EGS_OK;
   }
-  p->graph = g;
-  p->graph_band = p->band;
+  graph = g;
+  (prof ? p->pgraph_band : p->graph_band) = p->band;
   return EGS_OK;
 }
 
@@ -1062,10 +1103,7 @@ int egs_problem_set_precision(egs_problem* p, int precision, int band_tiles) {
     return EGS_ERR_STATE;
   }
   EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
-  if (p->graph_exec) cudaGraphExecDestroy(p->graph_exec);
-  if (p->graph) cudaGraphDestroy(p->graph);
-  p->graph_exec = nullptr;
-  p->graph = nullptr;
+  drop_graphs(p);
   const int rc = setup_mixed(p, band_tiles);
   if (rc != EGS_OK) {
     // leave a problem that reports the failure instead of a half-built layout
@@ -1079,10 +1117,7 @@ int egs_problem_set_lookahead(egs_problem* p, int sms) {
   if (!p || sms < 0 || sms >= gemm_num_sms()) return EGS_ERR_INVALID;
   if (sms == p->lookahead_sms) return EGS_OK;
   EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
-  if (p->graph_exec) cudaGraphExecDestroy(p->graph_exec);
-  if (p->graph) cudaGraphDestroy(p->graph);
-  p->graph_exec = nullptr;
-  p->graph = nullptr;
+  drop_graphs(p);
   p->lookahead_sms = sms;
   return EGS_OK;
 }
@@ -1095,10 +1130,7 @@ int egs_problem_set_band_method(egs_problem* p, int method) {
   }
   if (method == p->band_method) return EGS_OK;
   EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
-  if (p->graph_exec) cudaGraphExecDestroy(p->graph_exec);
-  if (p->graph) cudaGraphDestroy(p->graph);
-  p->graph_exec = nullptr;
-  p->graph = nullptr;
+  drop_graphs(p);
   p->band_method = method;
   return EGS_OK;
 }
@@ -1233,20 +1265,28 @@ int egs_mle_eval(egs_problem* p, const double* theta, double* loglik, double* lo
   // The pinned mirrors may still be in use by the previous evaluation.
   EGS_CUDA_TRY(cudaStreamSynchronize(st));
   *p->hparams = mp;
-  const bool replay = p->graphs_enabled && !p->profiling && p->evals > 0;
-  if (replay && (!p->graph_exec || p->graph_band != p->band)) {
-    if ((rc = capture_eval(p)) != EGS_OK) return rc;
+  const bool prof = p->profiling;
+  const bool replay = p->graphs_enabled && (!prof || p->pgraphs_ok) && p->evals > 0;
+  cudaGraphExec_t& exec = prof ? p->pgraph_exec : p->graph_exec;
+  if (replay && (!exec || (prof ? p->pgraph_band : p->graph_band) != p->band)) {
+    if ((rc = capture_eval(p, prof)) != EGS_OK) return rc;
   }
-  if (replay && p->graph_exec) {
-    EGS_CUDA_TRY(cudaGraphLaunch(p->graph_exec, st));
-    for (int i = 0; i < EGS_NUM_STAGES; ++i) p->stage_launches[i] += p->graph_launches[i];
+  if (replay && exec) {
+    EGS_CUDA_TRY(cudaGraphLaunch(exec, st));
+    const long long* launches = prof ? p->pgraph_launches : p->graph_launches;
+    for (int i = 0; i < EGS_NUM_STAGES; ++i) p->stage_launches[i] += launches[i];
+    if (prof) p->spans.insert(p->spans.end(), p->pgraph_spans.begin(), p->pgraph_spans.end());
   } else {
     EGS_CUDA_TRY(cudaMemcpyAsync(p->dparams, p->hparams, sizeof(MaternParams), cudaMemcpyHostToDevice, st));
     if ((rc = enqueue_eval(p)) != EGS_OK) return rc;
   }
   ++p->evals;
   EGS_CUDA_TRY(cudaStreamSynchronize(st));
-  collect_spans(p);
+  const size_t nspans = p->spans.size();
+  if (collect_spans(p) == 0 && nspans > 0 && prof && replay) {
+    // the replayed timing events gave no times: time the next ones eagerly
+    p->pgraphs_ok = false;
+  }
   if (p->hflags[1] != 0) {
     set_last_error("a device-side wait exceeded its limit", "tensor-core update");
     return EGS_ERR_TIMEOUT;
