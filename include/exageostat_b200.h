@@ -244,8 +244,11 @@ EGS_API int egs_mle_eval_noalloc(int n, int dts, const double* x, const double* 
                                  void* cuda_stream);
 
 /* From its second evaluation on, egs_mle_eval replays the whole evaluation of a
- * problem as one CUDA graph (captured once; disabled while profiling).  enable = 0
- * turns replay off for this problem, 1 (the default) on. */
+ * problem as one CUDA graph (captured once).  While profiling is on, a second
+ * graph that also records the stage-timing events is captured and replayed
+ * (at the first profiled evaluation after the first one); if its events give no
+ * times, profiled evaluations of this problem fall back to direct launches.
+ * enable = 0 turns replay off for this problem, 1 (the default) on. */
 EGS_API int egs_problem_set_graphs(egs_problem* p, int enable);
 
 /* ---- batched evaluation of many independent problems -------------------- */
