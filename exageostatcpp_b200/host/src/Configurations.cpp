@@ -1,5 +1,6 @@
 // Non-template parts of Configurations (src/configurations/Configurations.cpp,
-// Parser.cpp:23-81, Validator.cpp:209-255 for the theta strings).
+// Parser.cpp:23-81, Validator.cpp:209-255 for the theta strings,
+// Validator.cpp:108-136 for the computation and precision values).
 #include "configurations/Configurations.hpp"
 
 #include <cctype>
@@ -57,6 +58,46 @@ std::vector<double> parse_theta(const std::string& v) {
 
 bool parse_bool(const std::string& v) { return v == "true" || v == "1" || v == "TRUE" || v == "True"; }
 
+// Validator::CheckKernelValue (Validator.cpp:138-158): a snake_case name becomes
+// CamelCase ("univariate_matern_stationary" -> "UnivariateMaternStationary"),
+// the form the kernel registry and the parameter-count map are keyed by.
+std::string camel_kernel_name(const std::string& v) {
+  if (v.empty() || (v.find('_') == std::string::npos && !std::islower((unsigned char)v[0]))) return v;
+  std::string out;
+  bool up = true;
+  for (char c : v) {
+    if (c == '_') {
+      up = true;
+      continue;
+    }
+    out += up ? (char)std::toupper((unsigned char)c) : c;
+    up = false;
+  }
+  return out;
+}
+
+// Validator::CheckComputationValue (Validator.cpp:108-121): the same spellings
+// and message; tile low-rank is a value the reference accepts but this build
+// does not run.
+common::Computation parse_computation(const std::string& v) {
+  if (v == "exact" || v == "Exact" || v == "Dense" || v == "dense") return common::EXACT_DENSE;
+  if (v == "diag_approx" || v == "diagonal_approx") return common::DIAGONAL_APPROX;
+  if (v == "lr_approx" || v == "tlr" || v == "TLR")
+    throw std::domain_error("--computation=" + v + ": tile low-rank is not on the B200 path");
+  throw std::range_error("Invalid value for Computation. Please use Exact, diagonal_approx or TLR.");
+}
+
+// Validator::CheckPrecisionValue (Validator.cpp:123-136): the same spellings and
+// message; single precision throughout is a value the reference accepts but
+// this build does not run (its mixed form keeps FP64 where it matters).
+common::Precision parse_precision(const std::string& v) {
+  if (v == "double" || v == "Double") return common::DOUBLE;
+  if (v == "mix" || v == "Mix" || v == "Mixed" || v == "mixed") return common::MIXED;
+  if (v == "single" || v == "Single")
+    throw std::domain_error("--precision=" + v + ": single precision is not on the B200 path");
+  throw std::range_error("Invalid value for Computation. Please use Single, Double or Mixed.");
+}
+
 }  // namespace
 
 void Configurations::InitializeArguments(const int& argc, char** argv) {
@@ -68,7 +109,7 @@ void Configurations::InitializeArguments(const int& argc, char** argv) {
     const std::string key = normalise_key(arg.substr(0, eq));
     const std::string val = eq == std::string::npos ? "true" : arg.substr(eq + 1);
     if (key == "n") SetProblemSize(std::stoi(val));
-    else if (key == "kernel") SetKernelName(val);
+    else if (key == "kernel") SetKernelName(camel_kernel_name(val));
     else if (key == "dts") SetDenseTileSize(std::stoi(val));
     else if (key == "seed") SetSeed(std::stoi(val));
     else if (key == "maxmleiterations") SetMaxMleIterations(std::stoi(val));
@@ -79,10 +120,12 @@ void Configurations::InitializeArguments(const int& argc, char** argv) {
     else if (key == "ub" || key == "upperbounds") SetUpperBounds(parse_theta(val));
     else if (key == "etheta" || key == "estimatedtheta") SetEstimatedTheta(parse_theta(val));
     else if (key == "mspe") SetIsMSPE(parse_bool(val));
-    else if (key == "computation") {
-      if (val != "exact") throw std::domain_error("only --computation=exact is on the B200 path");
-      SetComputation(common::EXACT_DENSE);
-    } else if (key == "dimension") {
+    else if (key == "computation") SetComputation(parse_computation(val));
+    else if (key == "precision") SetPrecision(parse_precision(val));
+    else if (key == "band") SetBand(std::stoi(val));
+    else if (key == "mixedband") SetMixedPrecisionBand(std::stoi(val));  // this build: FP64 tile rows of --precision=mixed
+    else if (key == "datapath") SetDataPath(val);
+    else if (key == "dimension") {
       if (val != "2D" && val != "2d") throw std::domain_error("only 2D locations are on the B200 path");
       SetDimension(common::Dimension2D);
     } else if (key == "cores") SetCoresNumber(std::stoi(val));
