@@ -1,6 +1,7 @@
 // Non-template parts of Configurations (src/configurations/Configurations.cpp,
 // Parser.cpp:23-81, Validator.cpp:209-255 for the theta strings,
-// Validator.cpp:108-136 for the computation and precision values).
+// Validator.cpp:108-158 and 285-294 for the computation, precision, kernel
+// and distance values).
 #include "configurations/Configurations.hpp"
 
 #include <cctype>
@@ -76,6 +77,15 @@ std::string camel_kernel_name(const std::string& v) {
   return out;
 }
 
+// Validator::CheckDistanceMetricValue (Validator.cpp:285-294).  The likelihood
+// path always evaluates Euclidean distances (ChameleonImplementation.cpp:172
+// passes metric 0), here as in the reference; the value is kept for callers.
+int parse_distance_metric(const std::string& v) {
+  if (v == "eg" || v == "EG" || v == "euclidean") return common::EUCLIDEAN_DISTANCE;
+  if (v == "gcd" || v == "GCD" || v == "great_circle") return common::GREAT_CIRCLE_DISTANCE;
+  throw std::range_error("Invalid value. Please use eg or gcd values only.");
+}
+
 // Validator::CheckComputationValue (Validator.cpp:108-121): the same spellings
 // and message; tile low-rank is a value the reference accepts but this build
 // does not run.
@@ -120,6 +130,24 @@ void Configurations::InitializeArguments(const int& argc, char** argv) {
     else if (key == "ub" || key == "upperbounds") SetUpperBounds(parse_theta(val));
     else if (key == "etheta" || key == "estimatedtheta") SetEstimatedTheta(parse_theta(val));
     else if (key == "mspe") SetIsMSPE(parse_bool(val));
+    else if (key == "fisher") SetIsFisher(parse_bool(val));
+    else if (key == "mloemmom") SetIsMLOEMMOM(parse_bool(val));
+    else if (key == "idw") {
+      if (parse_bool(val)) throw std::domain_error("--idw: inverse-distance weighting is not on the B200 path");
+      SetIsIDW(false);
+    } else if (key == "isnongaussian") {
+      if (parse_bool(val)) throw std::domain_error("--isnongaussian: non-Gaussian likelihoods are not on the B200 path");
+      SetIsNonGaussian(false);
+    } else if (key == "p" || key == "q") {
+      // process grid of the reference's distributed runs; one process per GPU here
+      if (std::stoi(val) != 1) throw std::domain_error("--" + key + "=" + val + ": one process drives one GPU here");
+    } else if (key == "distancemetric") SetDistanceMetric(parse_distance_metric(val));
+    else if (key == "observationnumber") SetObservationNumber(std::stoi(val));
+    else if (key == "timeslot") SetTimeSlot(std::stoi(val));
+    else if (key == "startingtheta") SetStartingTheta(parse_theta(val));
+    else if (key == "lts") SetLowTileSize(std::stoi(val));
+    else if (key == "maxrank") SetMaxRank(std::stoi(val));
+    else if (key == "recoveryfile") SetRecoveryFile(val);
     else if (key == "computation") SetComputation(parse_computation(val));
     else if (key == "precision") SetPrecision(parse_precision(val));
     else if (key == "band") SetBand(std::stoi(val));

@@ -1,6 +1,6 @@
 // Host-only checks of the command-line parser of Configurations
 // (exageostatcpp_b200/host/src/Configurations.cpp, following the reference's
-// Parser.cpp:23-81 and Validator.cpp:108-158): accepted spellings, the values
+// Parser.cpp:23-81 and Validator.cpp:108-158, 285-294): accepted spellings, the values
 // they set, and the errors for values the reference rejects or this build does
 // not run.  No GPU call is made.  Prints one "name: ok|FAIL ..." line per case
 // and exits non-zero if any case failed.
@@ -87,6 +87,21 @@ int main() {
     report("unknown_argument", e.rfind("invalid:", 0) == 0, e);
     const std::string f = parse_error({"--dimension=3D"});
     report("dimension_3d_not_run", f.rfind("domain:", 0) == 0, f);
+    const std::string g = parse_error({"--distance_metric=manhattan"});
+    report("distance_invalid", g == "range:Invalid value. Please use eg or gcd values only.", g);
+    const std::string h = parse_error({"--idw=true"});
+    report("idw_not_run", h.rfind("domain:", 0) == 0, h);
+    const std::string i = parse_error({"--p=2"});
+    report("process_grid_not_run", i.rfind("domain:", 0) == 0, i);
+  }
+  {
+    Configurations c;
+    parse(c, {"--fisher=true", "--mloe_mmom=true", "--mspe=true", "--distance_metric=gcd", "--p=1", "--q=1",
+              "--observation_number=4", "--idw=false", "--starting_theta=1:0.1:0.5"});
+    report("prediction_flags", c.GetIsFisher() && c.GetIsMLOEMMOM() && c.GetIsMSPE() && !c.GetIsIDW() &&
+                                   c.GetDistanceMetric() == common::GREAT_CIRCLE_DISTANCE &&
+                                   c.GetObservationNumber() == 4 && c.GetStartingTheta().size() == 3 &&
+                                   c.GetStartingTheta()[2] == 0.5);
   }
   return failures == 0 ? 0 : 1;
 }

@@ -19,7 +19,7 @@ ROOT = os.path.dirname(HERE)
 
 CASES = ["mixed_run", "diag_approx", "dense_double", "mix_spelling", "precision_invalid",
          "precision_single_not_run", "computation_invalid", "computation_tlr_not_run", "unknown_argument",
-         "dimension_3d_not_run"]
+         "dimension_3d_not_run", "distance_invalid", "idw_not_run", "process_grid_not_run", "prediction_flags"]
 
 
 def test_configurations_parser(tmp_path):
