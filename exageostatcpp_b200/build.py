@@ -65,6 +65,8 @@ HOST_INCLUDE = os.path.join(HERE, "host", "include")
 HOST_SOURCES = [os.path.join(HERE, "host", "src", "Configurations.cpp")]
 API_TEST_SRC = os.path.join(ROOT, "tests", "cpp", "test_exageostat_api.cpp")
 API_TEST_BIN = os.path.join(ROOT, "tests", "cpp", "_build", "test_exageostat_api")
+EXAMPLE_SRC = os.path.join(HERE, "host", "examples", "end_to_end.cpp")
+EXAMPLE_BIN = os.path.join(HERE, "host", "examples", "_build", "end_to_end")
 
 
 def build_host_tests() -> str:
@@ -76,7 +78,20 @@ def build_host_tests() -> str:
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError(f"host API test build failed:\n{res.stdout}\n{res.stderr}")
+    build_example()
     return API_TEST_BIN
+
+
+def build_example() -> str:
+    """Compile the end-to-end example program of the C++ API (host/examples)."""
+    os.makedirs(os.path.dirname(EXAMPLE_BIN), exist_ok=True)
+    cmd = [nvcc(), "-std=c++17", "-O2", "-x", "c++", "-I", HOST_INCLUDE, "-I", os.path.join(ROOT, "include"),
+           *HOST_SOURCES, EXAMPLE_SRC, "-L", HERE, "-lexageostat_b200",
+           "-Xlinker", "-rpath", "-Xlinker", "$ORIGIN/../../..", "-o", EXAMPLE_BIN]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"example build failed:\n{res.stdout}\n{res.stderr}")
+    return EXAMPLE_BIN
 
 
 if __name__ == "__main__":
