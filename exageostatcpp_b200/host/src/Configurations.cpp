@@ -1,6 +1,6 @@
 // Non-template parts of Configurations (src/configurations/Configurations.cpp,
 // Parser.cpp:23-81, Validator.cpp:209-255 for the theta strings,
-// Validator.cpp:108-158 and 285-294 for the computation, precision, kernel
+// Validator.cpp:108-173 and 285-294 for the computation, precision, kernel
 // and distance values).
 #include "configurations/Configurations.hpp"
 
@@ -59,7 +59,7 @@ std::vector<double> parse_theta(const std::string& v) {
 
 bool parse_bool(const std::string& v) { return v == "true" || v == "1" || v == "TRUE" || v == "True"; }
 
-// Validator::CheckKernelValue (Validator.cpp:138-158): a snake_case name becomes
+// Validator::CheckKernelValue (Validator.cpp:137-173): a snake_case name becomes
 // CamelCase ("univariate_matern_stationary" -> "UnivariateMaternStationary"),
 // the form the kernel registry and the parameter-count map are keyed by.
 std::string camel_kernel_name(const std::string& v) {

@@ -1,6 +1,6 @@
 // Host-only checks of the command-line parser of Configurations
 // (exageostatcpp_b200/host/src/Configurations.cpp, following the reference's
-// Parser.cpp:23-81 and Validator.cpp:108-158, 285-294): accepted spellings, the values
+// Parser.cpp:23-81 and Validator.cpp:108-173, 285-294): accepted spellings, the values
 // they set, and the errors for values the reference rejects or this build does
 // not run.  No GPU call is made.  Prints one "name: ok|FAIL ..." line per case
 // and exits non-zero if any case failed.
