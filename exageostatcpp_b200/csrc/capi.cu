@@ -528,7 +528,7 @@ int enqueue_eval(egs_problem* p) {
   EGS_CUDA_TRY(cudaMemcpyAsync(p->z, p->zcpy, p->np * sizeof(double), cudaMemcpyDeviceToDevice, st));
   int sp = span_begin(p, EGS_STAGE_GENERATE);
   int rc = launch_matern_tiles(p->tiles, p->x, p->y, p->n, p->ts, p->nt, p->dparams, p->ktab, st);
-  if (rc != EGS_OK) return check_cuda("matern");
+  if (rc != EGS_OK) return rc;
   count_launches(p, EGS_STAGE_GENERATE, 1 + (lower_tiles(p->nt) + 65534) / 65535);
   span_end(p, sp, 0.0);
   rc = p->band > 0 ? enqueue_potrf_band(p) : enqueue_potrf(p);
@@ -1188,7 +1188,7 @@ int egs_covariance_generate(egs_problem* p, const double* theta) {
   int rc = set_params(p, theta);
   if (rc != EGS_OK) return rc;
   rc = launch_matern_tiles(p->tiles, p->x, p->y, p->n, p->ts, p->nt, p->dparams, p->ktab, p->stream);
-  if (rc != EGS_OK) return check_cuda("egs_covariance_generate");
+  if (rc != EGS_OK) return rc;
   EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
   return EGS_OK;
 }
@@ -1473,8 +1473,7 @@ int egs_mle_eval_noalloc(int n, int dts, const double* x, const double* y, const
     EGS_CUDA_TRY(cudaMemsetAsync(q.y + n, 0, pad, st));
     EGS_CUDA_TRY(cudaMemsetAsync(q.z + n, 0, pad, st));
   }
-  if ((rc = launch_matern_tiles(q.tiles, q.x, q.y, n, q.ts, q.nt, dparams, ktab, st)) != EGS_OK)
-    return check_cuda("egs_mle_eval_noalloc/matern");
+  if ((rc = launch_matern_tiles(q.tiles, q.x, q.y, n, q.ts, q.nt, dparams, ktab, st)) != EGS_OK) return rc;
   if ((rc = enqueue_potrf(&q)) != EGS_OK) return rc;
   launch_logdet_partials(q.tiles, q.ts, q.nt, n, partial, st);
   enqueue_trsv(&q);
@@ -1530,9 +1529,7 @@ int egs_matern_block(double* a, int lda, int rows, int cols, const double* x1, c
   MaternParams mp;
   int rc = make_matern_params(theta, &mp);
   if (rc != EGS_OK) return rc;
-  rc = launch_matern_block(a, lda, rows, cols, x1, y1, x2, y2, mp, (cudaStream_t)cuda_stream);
-  if (rc != EGS_OK) return check_cuda("egs_matern_block");
-  return EGS_OK;
+  return launch_matern_block(a, lda, rows, cols, x1, y1, x2, y2, mp, (cudaStream_t)cuda_stream);
 }
 
 namespace {
@@ -1603,7 +1600,10 @@ int egs_predict_host(int n_obs, int n_miss, int dts, const double* x_obs, const 
   }
   MaternParams mp;
   make_matern_params(theta, &mp);
-  launch_matern_block(c12t, n_obs, n_obs, n_miss, p->x, p->y, dxm, dym, mp, st);
+  if ((rc = launch_matern_block(c12t, n_obs, n_obs, n_miss, p->x, p->y, dxm, dym, mp, st)) != EGS_OK) {
+    cleanup();
+    return rc;
+  }
   launch_gemv_t_block(c12t, n_obs, n_obs, n_miss, p->z, dzm, st);
   double sum = -1.0;
   if (z_actual) {
@@ -1691,10 +1691,10 @@ int egs_problem_predict(egs_problem* p, const double* theta, int n_miss, const d
   cudaMemcpyAsync(dym, y_miss, n_miss * sizeof(double), cudaMemcpyHostToDevice, st);
   MaternParams mp;
   make_matern_params(theta, &mp);
-  launch_matern_block(c12t, p->n, p->n, n_miss, p->x, p->y, dxm, dym, mp, st);
+  rc = launch_matern_block(c12t, p->n, p->n, n_miss, p->x, p->y, dxm, dym, mp, st);
   launch_gemv_t_block(c12t, p->n, p->n, n_miss, p->z, dzm, st);
   cudaMemcpyAsync(z_miss, dzm, n_miss * sizeof(double), cudaMemcpyDeviceToHost, st);
-  rc = check_cuda("egs_problem_predict");
+  if (rc == EGS_OK) rc = check_cuda("egs_problem_predict");
   for (void* b : {(void*)c12t, (void*)dxm, (void*)dym, (void*)dzm}) dev_free(b, st);
   if (cudaStreamSynchronize(st) != cudaSuccess && rc == EGS_OK) rc = check_cuda("egs_problem_predict/sync");
   return rc;
@@ -1752,9 +1752,9 @@ int egs_mloe_mmom_host(int n_obs, int n_miss, int dts, const double* x_obs, cons
   cudaMemcpyAsync(dxm, x_miss, n_miss * sizeof(double), cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(dym, y_miss, n_miss * sizeof(double), cudaMemcpyHostToDevice, st);
   // k_t, k_a for every target: columns of leading dimension np (padding rows stay 0)
-  launch_matern_block(kt, (int)np, n_obs, n_miss, pa->x, pa->y, dxm, dym, mt, st);
-  launch_matern_block(ka, (int)np, n_obs, n_miss, pa->x, pa->y, dxm, dym, ma, st);
-  if ((rc = egs_problem_set_stream(pt, st)) != EGS_OK) {
+  if ((rc = launch_matern_block(kt, (int)np, n_obs, n_miss, pa->x, pa->y, dxm, dym, mt, st)) != EGS_OK ||
+      (rc = launch_matern_block(ka, (int)np, n_obs, n_miss, pa->x, pa->y, dxm, dym, ma, st)) != EGS_OK ||
+      (rc = egs_problem_set_stream(pt, st)) != EGS_OK) {
     cleanup();
     return rc;
   }

@@ -13,6 +13,8 @@
 // log-determinant and the quadratic form of the real N x N block unchanged.
 #pragma once
 #include <cstdint>
+#include <mutex>
+#include <utility>
 #include <cuda_runtime.h>
 #include "exageostat_b200.h"
 
@@ -24,6 +26,20 @@ __host__ __device__ __forceinline__ long long tile_slot(int i, int j, int nt) {
 
 __host__ __device__ __forceinline__ long long lower_tiles(int nt) {
   return (long long)nt * (nt + 1) / 2;
+}
+
+// Runs f once for each device it is called on (kernel attributes such as the
+// dynamic shared-memory limit belong to the current device's context, so a
+// process that uses several devices sets them on each); devices with an
+// ordinal of 64 or more run f on every call.
+template <typename F>
+inline void once_per_device(std::once_flag (&flags)[64], F&& f) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    f();
+    return;
+  }
+  std::call_once(flags[dev], std::forward<F>(f));
 }
 
 // Spin limit for every device-side wait: after this many polls a waiting thread
@@ -43,4 +59,14 @@ constexpr long long kSpinLimit = 1ll << 26;
 
 namespace egs {
 void set_last_error(const char* what, const char* where);
+
+// Status of the launches just issued: reads (and thereby clears) the runtime's
+// last error once and records its text, so that a caller returning this code
+// does not lose the error to a second cudaGetLastError().
+inline int launch_status(const char* where) {
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) return EGS_OK;
+  set_last_error(cudaGetErrorString(e), where);
+  return EGS_ERR_CUDA;
+}
 }

@@ -400,12 +400,11 @@ int gemm_num_sms() {
 }
 
 static void set_gemm_smem_attributes() {
-  static const bool attr_set = []() {
+  static std::once_flag done[64];
+  once_per_device(done, []() {
     cudaFuncSetAttribute(dgemm_update_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, gemm::SMEM_BYTES);
     cudaFuncSetAttribute(dgemm_update_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, gemm::SMEM_BYTES);
-    return true;
-  }();
-  (void)attr_set;
+  });
 }
 
 void finish_desc(GemmDesc& d) {
@@ -432,7 +431,7 @@ static int launch_desc(const void* tmap, double* tiles, GemmDesc& d, int* err, c
   GemmJobs none{nullptr, nullptr, 0, 0};
   dgemm_update_kernel<false><<<(unsigned)grid, THREADS, SMEM_BYTES, st>>>(
       *reinterpret_cast<const CUtensorMap*>(tmap), tiles, d, none, err);
-  return cudaGetLastError() == cudaSuccess ? EGS_OK : EGS_ERR_CUDA;
+  return launch_status("dgemm_update_kernel");
 }
 
 // Trailing update of step k: C(i, j) -= L(i, k) L(j, k)^T for all k < j <= i.
@@ -490,7 +489,7 @@ int launch_gemm_batched(const void* tmap, double* tiles, const GemmDesc* jobs, c
   GemmJobs J{jobs, begin, njobs, total};
   dgemm_update_kernel<true><<<(unsigned)grid, THREADS, SMEM_BYTES, st>>>(
       *reinterpret_cast<const CUtensorMap*>(tmap), tiles, none, J, err);
-  return cudaGetLastError() == cudaSuccess ? EGS_OK : EGS_ERR_CUDA;
+  return launch_status("dgemm_update_kernel (jobs)");
 }
 
 }  // namespace egs

@@ -254,7 +254,10 @@ extern "C" int egs_fisher_host(int n, int dts, const double* x, const double* y,
   cudaMemcpyAsync(dy, y, n * sizeof(double), cudaMemcpyHostToDevice, st);
   // C with identity padding, dense
   cudaMemsetAsync(C, 0, nn2 * sizeof(double), st);
-  launch_matern_block(C, (int)np, n, n, dx, dy, dx, dy, mp, st);
+  if ((rc = launch_matern_block(C, (int)np, n, n, dx, dy, dx, dy, mp, st)) != EGS_OK) {
+    cleanup();
+    return rc;
+  }
   {
     std::vector<double> one(1, 1.0);
     for (long long r = n; r < np; ++r)

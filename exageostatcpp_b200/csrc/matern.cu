@@ -112,7 +112,7 @@ int launch_matern_tiles(double* tiles, const double* x, const double* y, int n, 
     const unsigned gy = (unsigned)((total - s0) < 65535 ? (total - s0) : 65535);
     matern_tiles_kernel<<<dim3(gx, gy), kGenThreads, 0, st>>>(tiles, x, y, n, ts, nt, s0, p, ktab);
   }
-  return cudaGetLastError() == cudaSuccess ? EGS_OK : EGS_ERR_CUDA;
+  return launch_status("matern_tiles_kernel");
 }
 
 int launch_matern_block(double* a, int lda, int rows, int cols, const double* x1, const double* y1,
@@ -124,7 +124,7 @@ int launch_matern_block(double* a, int lda, int rows, int cols, const double* x1
     matern_block_kernel<<<dim3((rows + threads - 1) / threads, nc), threads, 0, st>>>(
         a + (long long)c0 * lda, lda, rows, nc, x1, y1, x2 + c0, y2 + c0, p);
   }
-  return cudaGetLastError() == cudaSuccess ? EGS_OK : EGS_ERR_CUDA;
+  return launch_status("matern_block_kernel");
 }
 
 }  // namespace egs

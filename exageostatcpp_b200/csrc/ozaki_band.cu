@@ -582,14 +582,12 @@ long long ozaki_targets(int ts, int nt, int band, int k, std::vector<int4>& out)
 
 static int launch_ozaki(const void* tm_s, const OzStep& P, cudaStream_t st) {
   using namespace oz;
-  static const bool attr = []() {
-    cudaFuncSetAttribute(ozaki_band_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-    return true;
-  }();
-  (void)attr;
+  static std::once_flag attr_done[64];
+  once_per_device(attr_done,
+                  []() { cudaFuncSetAttribute(ozaki_band_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES); });
   const long long grid = P.total < gemm_num_sms() ? P.total : gemm_num_sms();
   ozaki_band_kernel<<<(unsigned)grid, THREADS, SMEM_BYTES, st>>>(*reinterpret_cast<const CUtensorMap*>(tm_s), P);
-  return cudaGetLastError() == cudaSuccess ? EGS_OK : EGS_ERR_CUDA;
+  return launch_status("ozaki_band_kernel");
 }
 
 // Targets of the panel solve at step k: off-band tiles i = first .. nt-1, all

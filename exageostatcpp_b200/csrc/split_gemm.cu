@@ -506,11 +506,9 @@ int launch_split_update(const void* tm_hi, const void* tm_lo, const void* tm_c, 
   if (ts % BN != 0) return EGS_ERR_INVALID;
   const long long targets = split_targets(nt, band, k);
   if (targets == 0) return EGS_OK;
-  static const bool attr = []() {
-    cudaFuncSetAttribute(split_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-    return true;
-  }();
-  (void)attr;
+  static std::once_flag attr_done[64];
+  once_per_device(attr_done,
+                  []() { cudaFuncSetAttribute(split_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES); });
   SplitStep P;
   P.ts = ts;
   P.nt = nt;
@@ -528,7 +526,7 @@ int launch_split_update(const void* tm_hi, const void* tm_lo, const void* tm_c, 
                                                                  *reinterpret_cast<const CUtensorMap*>(tm_lo),
                                                                  *reinterpret_cast<const CUtensorMap*>(tm_c),
                                                                  *reinterpret_cast<const CUtensorMap*>(tm_cr), P);
-  return cudaGetLastError() == cudaSuccess ? EGS_OK : EGS_ERR_CUDA;
+  return launch_status("split_gemm_kernel");
 }
 
 }  // namespace egs

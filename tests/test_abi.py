@@ -54,3 +54,27 @@ def test_no_device_is_an_error_not_a_fallback():
     assert lib.egs_problem_create(ctypes.byref(h), 16, 8) == egs.EGS_ERR_NO_DEVICE
     with pytest.raises(egs.EgsError):
         egs.Problem(16, 8)
+
+
+def test_failed_kernel_launch_is_reported_not_swallowed():
+    # On a host without a usable CUDA driver the generator's launch itself fails.
+    # The launch helper reads the runtime's error once; the entry point must return
+    # that failure (EGS_ERR_CUDA with the kernel named), not EGS_OK from a second,
+    # already cleared error read.  Host buffers are passed, so the call is only
+    # made where no device could run the kernel.
+    try:
+        import torch
+        has_gpu = torch.cuda.is_available()
+    except Exception:
+        has_gpu = False
+    if has_gpu:
+        pytest.skip("a GPU is present")
+    import numpy as np
+    lib = egs.load_library()
+    buf = (ctypes.c_double * 16)()
+    vp = ctypes.cast(buf, ctypes.c_void_p)
+    theta = np.array([1.0, 0.1, 0.5])
+    rc = lib.egs_matern_block(vp, 4, 4, 4, vp, vp, vp, vp, theta.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                              0, None)
+    assert rc == egs.EGS_ERR_CUDA
+    assert b"matern_block_kernel" in lib.egs_last_error()

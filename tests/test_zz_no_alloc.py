@@ -58,6 +58,41 @@ def test_noalloc_matches_resident_evaluation_on_two_calls():
     assert np.array_equal(tx.cpu().numpy(), x)
 
 
+def test_noalloc_call_leaves_device_memory_unchanged():
+    # The feature's claim: after a first call (which loads the kernels and looks
+    # up the static array), an evaluation takes no device memory of its own.
+    # Free device memory is read before and after a second call; a cudaMalloc,
+    # cudaMallocAsync or a lazily loaded module anywhere on its path shows up as
+    # a drop.
+    torch = pytest.importorskip("torch")
+    n, dts = 1300, 256
+    x, y, z = O.load_data(n, 4, [1.0, 0.08, 0.9])
+    lib = egs.load_library()
+    need = ctypes.c_longlong()
+    assert lib.egs_mle_noalloc_workspace(n, dts, ctypes.byref(need)) == egs.EGS_OK
+    dev = torch.device("cuda:0")
+    tx, ty, tz = (torch.tensor(a, dtype=torch.float64, device=dev) for a in (x, y, z))
+    work = torch.empty(need.value, dtype=torch.float64, device=dev)
+    stream = torch.cuda.Stream()
+    th = np.array([1.0, 0.08, 0.9], dtype=np.float64)
+    values = []
+    free = []
+    for _ in range(2):
+        torch.cuda.synchronize()
+        free.append(torch.cuda.mem_get_info(dev)[0])
+        out = ctypes.c_double()
+        rc = lib.egs_mle_eval_noalloc(n, dts, _ptr(tx), _ptr(ty), _ptr(tz),
+                                      th.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), _ptr(work), need.value,
+                                      ctypes.byref(out), ctypes.c_void_p(stream.cuda_stream))
+        assert rc == egs.EGS_OK, lib.egs_last_error()
+        torch.cuda.synchronize()
+        values.append(out.value)
+    free.append(torch.cuda.mem_get_info(dev)[0])
+    assert free[2] == free[1], (free, "the second call changed the free device memory")
+    assert values[0] == values[1]
+    assert values[1] == pytest.approx(O.mle_loglik(x, y, z, th), rel=LOGLIK_RTOL, abs=0)
+
+
 def test_noalloc_rejects_sizes_beyond_its_limit():
     lib = egs.load_library()
     need = ctypes.c_longlong()
