@@ -65,6 +65,7 @@ SIGNATURES = {
     "egs_mle_eval": (ctypes.c_int, [_P, _D, _D, _D, _D]),
     "egs_generate_locations": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _D, _D]),
     "egs_dlarnv_normal": (ctypes.c_int, [_I, ctypes.c_int, _D]),
+    "egs_shuffle_split": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _D, _D, _D, _D, _D]),
     "egs_generate_observations": (ctypes.c_int, [_P, _D, ctypes.c_int, _D]),
     "egs_mle_noalloc_workspace": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _LL]),
     "egs_mle_eval_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _P, _P, _P, _D, _P, ctypes.c_longlong, _D,
@@ -341,6 +342,20 @@ def generate_locations(n: int, seed: int, reseed: bool = True):
     _check(lib.egs_generate_locations(int(n), int(seed), 1 if reseed else 0, _dptr(x), _dptr(y)),
            "generate_locations")
     return x, y
+
+
+def shuffle_split(z, x, y, n_miss: int):
+    """The reference's random hold-out split (PickRandomPoints): a Fisher-Yates
+    shuffle on the C library's rand() state as it stands, the first n_miss held
+    out.  Returns (z_obs, x_obs, y_obs, z_miss, x_miss, y_miss)."""
+    lib = load_library()
+    z, x, y = _f64(z), _f64(x), _f64(y)
+    n = len(z)
+    no = max(n - int(n_miss), 0)
+    out = [np.empty(no) for _ in range(3)] + [np.empty(max(int(n_miss), 0)) for _ in range(3)]
+    _check(lib.egs_shuffle_split(n, int(n_miss), _dptr(z), _dptr(x), _dptr(y), *(_dptr(a) for a in out)),
+           "shuffle_split")
+    return tuple(out)
 
 
 def dlarnv_normal(seed: int, n: int) -> np.ndarray:

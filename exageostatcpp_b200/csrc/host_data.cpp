@@ -6,6 +6,12 @@
 //    reference it draws from the C library's srand()/rand() (std::srand(seed) at
 //    src/api/ExaGeoStat.cpp:75-76), so the global rand() state advances exactly as
 //    the reference's does.
+//  * egs_shuffle_split: the random hold-out split of the prediction module,
+//    PredictionHelpers<T>::PickRandomPoints / Shuffle
+//    (src/prediction/PredictionHelpers.cpp:23-168) for one variable: a
+//    Fisher-Yates pass that draws j = i + rand() / (RAND_MAX / (n - i) + 1)
+//    (:146) from the same global rand() state, after which the first n_miss
+//    entries are held out and the rest observed.
 //  * egs_dlarnv_normal: LAPACK DLARNV with IDIST = 3 on top of DLARUV, called by
 //    GenerateObservationsVector with ISEED = {seed, seed, seed, 1}
 //    (src/linear-algebra-solvers/LinearAlgebraMethods.cpp:347-364).  DLARUV is a
@@ -98,6 +104,32 @@ EGS_API int egs_dlarnv_normal(const int* iseed, int n, double* out) {
     }
     state = s;
     for (int i = 0; i < il; ++i) out[iv + i] = std::sqrt(-2.0 * std::log(u[2 * i])) * std::cos(two_pi * u[2 * i + 1]);
+  }
+  return EGS_OK;
+}
+
+EGS_API int egs_shuffle_split(int n, int n_miss, const double* z, const double* x, const double* y,
+                              double* z_obs, double* x_obs, double* y_obs, double* z_miss, double* x_miss,
+                              double* y_miss) {
+  if (n <= 0 || n_miss < 0 || n_miss > n || !z || !x || !y) return EGS_ERR_INVALID;
+  if ((n - n_miss > 0 && (!z_obs || !x_obs || !y_obs)) || (n_miss > 0 && (!z_miss || !x_miss || !y_miss)))
+    return EGS_ERR_INVALID;
+  std::vector<double> sz(z, z + n), sx(x, x + n), sy(y, y + n);
+  for (int i = 0; i + 1 < n; ++i) {
+    const int j = i + std::rand() / (RAND_MAX / (n - i) + 1);
+    std::swap(sz[i], sz[j]);
+    std::swap(sx[i], sx[j]);
+    std::swap(sy[i], sy[j]);
+  }
+  for (int i = 0; i < n_miss; ++i) {
+    z_miss[i] = sz[i];
+    x_miss[i] = sx[i];
+    y_miss[i] = sy[i];
+  }
+  for (int i = n_miss; i < n; ++i) {
+    z_obs[i - n_miss] = sz[i];
+    x_obs[i - n_miss] = sx[i];
+    y_obs[i - n_miss] = sy[i];
   }
   return EGS_OK;
 }

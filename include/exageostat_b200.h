@@ -169,6 +169,15 @@ EGS_API int egs_mle_eval(egs_problem* p, const double* theta, double* loglik, do
  * from the C library's rand(); srand(seed) first when reseed != 0.  Replaces
  * LocationGenerator<T>::GenerateLocations (src/data-generators/LocationGenerator.cpp:25-123). */
 EGS_API int egs_generate_locations(int n, int seed, int reseed, double* x, double* y);
+/* Random hold-out split of n values with their locations (host arrays): a
+ * Fisher-Yates shuffle drawing j = i + rand() / (RAND_MAX / (n - i) + 1) from the
+ * C library's rand() state as it stands (no reseeding), then the first n_miss
+ * entries go to *_miss and the other n - n_miss, in order, to *_obs.  The inputs
+ * are not modified.  Replaces PredictionHelpers<T>::PickRandomPoints / Shuffle
+ * (src/prediction/PredictionHelpers.cpp:23-168, draw at :146) for one variable. */
+EGS_API int egs_shuffle_split(int n, int n_miss, const double* z, const double* x, const double* y,
+                              double* z_obs, double* x_obs, double* y_obs, double* z_miss, double* x_miss,
+                              double* y_miss);
 /* n N(0,1) samples of LAPACK DLARNV(IDIST=3, ISEED) (ISEED entries in [0, 4095],
  * ISEED[3] odd), as drawn at LinearAlgebraMethods.cpp:347-364. */
 EGS_API int egs_dlarnv_normal(const int* iseed, int n, double* out);

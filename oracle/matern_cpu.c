@@ -127,24 +127,44 @@ static double matern(double x, double sigma2, double nu, double con) {
   return scaled ? con * exp(nu * log(x) - x) * knu : con * pow(x, nu) * knu;
 }
 
+int egs_oracle_max_threads(void);
+
 struct job {
   double* a;
   long lda;
-  int n, t, nthreads;
-  const double *x, *y;
+  int m, n, t, nthreads, lower;
+  const double *x, *y, *x2, *y2;
   double sigma2, beta, nu, con;
 };
 
+/* Column j of the job: rows j..m-1 (lower triangle of a square matrix) or
+ * rows 0..m-1 (a block between two location sets); entry (i, j) pairs row
+ * location i of (x, y) with column location j of (x2, y2). */
 static void* worker(void* arg) {
   struct job* jb = (struct job*)arg;
   for (int j = jb->t; j < jb->n; j += jb->nthreads) {
-    for (int i = j; i < jb->n; ++i) {
-      double dx = jb->x[j] - jb->x[i], dy = jb->y[j] - jb->y[i];
+    for (int i = jb->lower ? j : 0; i < jb->m; ++i) {
+      double dx = jb->x2[j] - jb->x[i], dy = jb->y2[j] - jb->y[i];
       double dist = sqrt(dx * dx + dy * dy) / jb->beta;
       jb->a[i + (long)j * jb->lda] = matern(dist, jb->sigma2, jb->nu, jb->con);
     }
   }
   return 0;
+}
+
+static void run_jobs(double* a, long lda, int m, int n, int lower, const double* x, const double* y,
+                     const double* x2, const double* y2, const double* theta, int nthreads) {
+  if (nthreads <= 0) nthreads = egs_oracle_max_threads();
+  if (nthreads > 1024) nthreads = 1024;
+  const double sigma2 = theta[0], beta = theta[1], nu = theta[2];
+  const double con = sigma2 * (1.0 / (pow(2.0, nu - 1.0) * tgamma(nu)));
+  pthread_t tid[1024];
+  struct job jobs[1024];
+  for (int t = 0; t < nthreads; ++t) {
+    jobs[t] = (struct job){a, lda, m, n, t, nthreads, lower, x, y, x2, y2, sigma2, beta, nu, con};
+    pthread_create(&tid[t], 0, worker, &jobs[t]);
+  }
+  for (int t = 0; t < nthreads; ++t) pthread_join(tid[t], 0);
 }
 
 int egs_oracle_max_threads(void) {
@@ -157,15 +177,13 @@ int egs_oracle_max_threads(void) {
  * every online core. */
 void egs_oracle_matern_lower(double* a, long lda, int n, const double* x, const double* y, const double* theta,
                              int nthreads) {
-  if (nthreads <= 0) nthreads = egs_oracle_max_threads();
-  if (nthreads > 1024) nthreads = 1024;
-  const double sigma2 = theta[0], beta = theta[1], nu = theta[2];
-  const double con = sigma2 * (1.0 / (pow(2.0, nu - 1.0) * tgamma(nu)));
-  pthread_t tid[1024];
-  struct job jobs[1024];
-  for (int t = 0; t < nthreads; ++t) {
-    jobs[t] = (struct job){a, lda, n, t, nthreads, x, y, sigma2, beta, nu, con};
-    pthread_create(&tid[t], 0, worker, &jobs[t]);
-  }
-  for (int t = 0; t < nthreads; ++t) pthread_join(tid[t], 0);
+  run_jobs(a, lda, n, n, 1, x, y, x, y, theta, nthreads);
+}
+
+/* The m x n Matern block between row locations (x1, y1) and column locations
+ * (x2, y2), column-major with leading dimension lda (the C12 of the kriging,
+ * LinearAlgebraMethods.cpp:535). */
+void egs_oracle_matern_block(double* a, long lda, int m, int n, const double* x1, const double* y1,
+                             const double* x2, const double* y2, const double* theta, int nthreads) {
+  run_jobs(a, lda, m, n, 0, x1, y1, x2, y2, theta, nthreads);
 }
