@@ -49,8 +49,16 @@ CONFIG = {
     "n": N, "tile": DTS, "band_tiles": BAND, "theta": list(THETA), "precision": "mixed (value) / fp64 (plain_fp64)",
     "l2": "inputs larger than L2 (22 GB mixed / 42 GB FP64 tile storage vs 126 MB L2); no flush",
 }
-# Secondary line item: the reference's plain-FP64 GPU configuration.
-N40_TOTAL, N40_MISS, N40_DTS, N40_THETA = 41000, 1000, 960, (1.0, 0.05, 0.8)
+# The reference's plain-FP64 GPU configuration at N = 40,000: 41,000 points
+# generated, 1,000 held out for kriging, tile 960, two true thetas.
+C2_TOTAL, C2_MISS, C2_DTS = 41000, 1000, 960
+C2_THETAS = ((1.0, 0.03, 1.5), (1.0, 0.05, 0.8))
+# The reference's MLE settings (C1 configuration): bounds [0.01, 5]^3, start at
+# the lower bounds, ftol_abs 1e-9 (--tolerance=9), at most 100 evaluations.
+FIT_LB, FIT_UB, FIT_FTOL, FIT_MAXEVAL = (0.01, 0.01, 0.01), (5.0, 5.0, 5.0), 1e-9, 100
+# Fitted theta and MSPE of the mixed form against the plain form at N = 102,400:
+# both fits start at the true theta with the same trust radius and budget.
+C3_FIT_MAXEVAL, C3_FIT_RHOBEG, C3_MISS = 15, 0.02, 1000
 
 
 def env_rank():
@@ -68,17 +76,33 @@ def workload_data(egs):
     return x, y, z
 
 
-def workload_n40000(egs):
-    """The 40,000-point training split of the 41,000-point plain-FP64 configuration."""
-    import numpy as np
-    x, y = egs.generate_locations(N40_TOTAL, SEED)
-    gen = egs.Problem(N40_TOTAL, N40_DTS)
+def held_out_data(egs, n_total, dts, theta, n_miss):
+    """n_total locations of the reference generator (srand(SEED)), Z = L e at theta
+    generated on the device (FP64), then n_miss points held out by the reference's
+    random split, which continues the generator's rand() stream
+    (PredictionHelpers.cpp:140-168).  Returns (z_obs, x_obs, y_obs, z_miss, x_miss, y_miss)."""
+    x, y = egs.generate_locations(n_total, SEED)
+    gen = egs.Problem(n_total, dts)
     gen.set_locations(x, y)
-    z = gen.generate_observations(N40_THETA, SEED)
+    z = gen.generate_observations(theta, SEED)
     gen.close()
-    perm = np.random.default_rng(SEED).permutation(N40_TOTAL)
-    train = np.sort(perm[N40_MISS:])
-    return x[train].copy(), y[train].copy(), z[train].copy()
+    return egs.shuffle_split(z, x, y, n_miss)
+
+
+def guarded_objective(egs, p):
+    """The log-likelihood of problem p as a fit objective.  A theta whose covariance
+    is not numerically positive definite scores -1e300 and the search goes on (the
+    reference's objective throws there and the fit ends); returns (f, counters)."""
+    count = {"evals": 0, "not_positive_definite": 0}
+
+    def f(theta):
+        count["evals"] += 1
+        try:
+            return p.mle_eval(theta)[0]
+        except egs.NotPositiveDefinite:
+            count["not_positive_definite"] += 1
+            return -1e300
+    return f, count
 
 
 def load_peaks():
@@ -196,6 +220,15 @@ def cpu_sample(x, y, z, target_s: float = 12.0):
 
 
 def run_reference(args):
+    """The reference's FP64 path on the host cores (the oracle's restatement: Matern
+    generation in C on all threads, blocked Cholesky and solves on OpenBLAS).
+
+    Measured in this run: one full evaluation at N = 102,400 (84 GB of host
+    memory) and one at the N = 40,000 configuration.  The K timed steps are
+    bounded samples (one evaluation of the first N_s points each), projected to
+    N = 102,400 by the stages' n^2 / n^3 cost model and multiplied by the ratio
+    of the measured full-size evaluation to the projection of the warm-up
+    samples, so that the reported rate rests on the measured full-size time."""
     rank, world, _ = env_rank()
     if rank != 0:
         return 0
@@ -203,37 +236,58 @@ def run_reference(args):
     from oracle import cpu_baseline as C
     from oracle import oracle as O
     # Same locations as the B200 arm, produced on the host by the oracle's
-    # generator; the CPU path is the reference's FP64 dense evaluation.  Z for
-    # the sampled subset only (its cost does not depend on the values).
+    # generator; observations from DLARNV (the cost does not depend on them).
     t0 = time.perf_counter()
     x, y = O.generate_locations(N, O.GlibcRand(SEED))
+    full = None
+    if not args.no_full_cpu:
+        zf = O.dlarnv_normal(SEED, N)
+        ll_full, st_full = C.timed_eval(x, y, zf, THETA)
+        del zf
+        full = {"n": N, "seconds": sum(st_full.values()), "stage_s": {k: round(v, 3) for k, v in st_full.items()},
+                "loglik": ll_full}
+    # the N = 40,000 configuration: the training split of 41,000 points
+    rng = O.GlibcRand(SEED)
+    x2, y2 = O.generate_locations(C2_TOTAL, rng)
+    z2 = O.dlarnv_normal(SEED, C2_TOTAL)
+    z2o, x2o, y2o, _, _, _ = O.shuffle_split(z2, x2, y2, C2_MISS, rng)
+    _, st_c2 = C.timed_eval(x2o, y2o, z2o, C2_THETAS[1])
+    c2 = {"n": len(z2o), "theta": list(C2_THETAS[1]), "seconds": sum(st_c2.values()),
+          "evals_per_s": 1.0 / sum(st_c2.values()), "stage_s": {k: round(v, 3) for k, v in st_c2.items()}}
+    # bounded samples for the timed steps
     ns = 6000
     z = O.dlarnv_normal(SEED, ns)
     _, st = C.timed_eval(x[:ns], y[:ns], z, THETA)
-    per_step = 4.0
+    per_step = 3.0
     grow = (per_step / max(sum(st.values()), 1e-3)) ** (1.0 / 3.0)
     ns = int(min(16000, max(4000, ns * grow)) // 64 * 64)
     z = O.dlarnv_normal(SEED, ns)
     a = np.zeros((ns, ns), order="F")
+    projected = []
     for _ in range(args.warmup):
-        C.timed_eval(x[:ns], y[:ns], z, THETA, a)
+        _, st = C.timed_eval(x[:ns], y[:ns], z, THETA, a)
+        projected.append(1.0 / C.scaled_evals_per_s(st, ns, N))
+    calib = full["seconds"] / statistics.mean(projected) if full else 1.0
     scaled = []
     lat = []
     for _ in range(args.steps):
         _, st = C.timed_eval(x[:ns], y[:ns], z, THETA, a)
-        scaled.append(1.0 / C.scaled_evals_per_s(st, ns, N))
+        scaled.append(calib / C.scaled_evals_per_s(st, ns, N))
         lat.append(sum(st.values()))
     total = sum(scaled)
     value = args.steps / total
+    how = (f"each step one full FP64 evaluation at N={ns} on all host threads (Matern in C/pthreads, blocked "
+           f"Cholesky and solves on OpenBLAS), projected to N={N} by n^2 (generation, solve) and n^3 (potrf)")
+    if full:
+        how += (f" and calibrated by x{calib:.3f}, the ratio of the full N={N} evaluation measured in this run "
+                f"({full['seconds']:.1f} s) to the projection of the warm-up samples")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (reference generator semantics)",
         "config": CONFIG,
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": C.threads(), "kind": "port",
-                         "sample": f"each step one full FP64 evaluation at N={ns} on all host threads "
-                                   f"(Matern in C/pthreads, LAPACK dpotrf/dtrtrs via OpenBLAS), scaled to "
-                                   f"N={N} by n^2 (generation, solve) and n^3 (potrf)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": C.threads(), "kind": "port", "sample": how,
+                         "measured_full_n": full, "calibration": calib, "measured_c2": c2},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "p50_ms": 1e3 * statistics.median(scaled), "p99_ms": 1e3 * float(np.percentile(scaled, 99)),
         "sample_step_s_p50": statistics.median(lat), "wall_s": time.perf_counter() - t0,
@@ -270,25 +324,95 @@ def timed_evals(torch, p, stream, theta, steps, dist=None):
     return ms, lat, r
 
 
-def plain_n40000(egs, torch, steps, peak):
-    """The plain-FP64 path at the reference's N = 40,000 GPU configuration (tile 960)."""
-    x, y, z = workload_n40000(egs)
-    stream = torch.cuda.Stream()
-    p = egs.Problem(len(z), N40_DTS)
-    p.set_stream(stream.cuda_stream)
-    p.set_locations(x, y)
-    p.set_observations(z)
-    for _ in range(2):
-        p.mle_eval(N40_THETA)
-    warm_profiled(p, N40_THETA)
-    ms, _, r = timed_evals(torch, p, stream, N40_THETA, steps)
-    st_ms, st_fl, _ = p.stage_stats()
-    p.close()
-    up = egs.STAGES.index("update")
-    ach = st_fl[up] / (st_ms[up] * 1e-3) / 1e12
-    return {"config": "plain FP64, N=40000 (41000 generated, 1000 held out), theta=(1,0.05,0.8), tile 960",
-            "evals_per_s": steps / (ms * 1e-3), "ms_per_eval": ms / steps, "loglik": r[0],
-            "trailing_update_tflops": ach, "trailing_update_frac_of_dgemm": ach / peak}
+def c2_leg(egs, torch, steps, peak):
+    """The reference's plain-FP64 GPU configuration, end to end, for both true thetas:
+    41,000 points (a 203-wide jittered grid, srand(0)), 1,000 held out by the
+    reference's split, tile 960; device-timed evaluations at the true theta with
+    the trailing-update roofline, a full fit with the reference's MLE settings
+    (BOBYQA from the lower bounds, ftol_abs 1e-9, at most 100 evaluations), then
+    kriging of the 1,000 held-out points at the fitted theta and MSPE against the
+    truth (LinearAlgebraMethods.cpp:527-577)."""
+    import numpy as np
+    out = []
+    for theta in C2_THETAS:
+        zo, xo, yo, za, xm, ym = held_out_data(egs, C2_TOTAL, C2_DTS, theta, C2_MISS)
+        stream = torch.cuda.Stream()
+        p = egs.Problem(len(zo), C2_DTS)
+        p.set_stream(stream.cuda_stream)
+        p.set_locations(xo, yo)
+        p.set_observations(zo)
+        for _ in range(2):
+            p.mle_eval(theta)
+        warm_profiled(p, theta)
+        ms, _, r = timed_evals(torch, p, stream, theta, steps)
+        st_ms, st_fl, _ = p.stage_stats()
+        p.set_profiling(False)
+        up = egs.STAGES.index("update")
+        ach = st_fl[up] / (st_ms[up] * 1e-3) / 1e12
+        f, count = guarded_objective(egs, p)
+        t0 = time.perf_counter()
+        th, fb, ne = egs.bobyqa_maximize(f, FIT_LB, FIT_LB, FIT_UB, FIT_FTOL, FIT_MAXEVAL)
+        fit_s = time.perf_counter() - t0
+        zm = p.predict(th, xm, ym)
+        zt = p.predict(theta, xm, ym)
+        p.close()
+        out.append({
+            "theta_true": list(theta), "n": len(zo), "n_miss": len(za), "tile": C2_DTS,
+            "evals_per_s": steps / (ms * 1e-3), "ms_per_eval": ms / steps, "loglik_at_true": r[0],
+            "logdet_at_true": r[1], "dot_at_true": r[2],
+            "trailing_update_tflops": ach, "trailing_update_frac_of_dgemm": ach / peak,
+            "fit": {"theta": th.tolist(), "loglik": fb, "evals": ne, "seconds": fit_s,
+                    "evals_per_s": count["evals"] / fit_s, "not_positive_definite": count["not_positive_definite"],
+                    "settings": "BOBYQA, bounds [0.01,5]^3, start at the lower bounds, ftol_abs 1e-9, "
+                                "maxeval 100"},
+            "mspe_at_fit": float(np.mean((za - zm) ** 2)), "mspe_at_true": float(np.mean((za - zt) ** 2)),
+        })
+    return {"config": "plain FP64, N=40000 (41000 generated on a 203-wide jittered grid, srand(0); 1000 held out "
+                      "by the reference's rand() split), tile 960", "thetas": out}
+
+
+def c3_fit_leg(egs):
+    """Fitted theta and MSPE of the mixed form against the plain FP64 form at
+    N = 102,400: N + 1,000 points generated (Z = L e at the true theta, FP64), 1,000
+    held out by the reference's split, the 102,400 others fitted by BOBYQA in each
+    form from the true theta (trust radius 0.02, the same budget of evaluations,
+    bounds [0.01, 5]^3, ftol_abs 1e-9), then kriging of the held-out points at each
+    form's fitted theta with its own factorisation (mixed: FP32 off-band storage
+    and one refinement step).  The plain form also evaluates its likelihood at the
+    mixed form's fitted theta: how much likelihood the mixed fit gives up."""
+    import numpy as np
+    zo, xo, yo, za, xm, ym = held_out_data(egs, N + C3_MISS, DTS, THETA, C3_MISS)
+    res = {}
+    for label in ("mixed", "plain"):
+        p = egs.Problem(len(zo), DTS)
+        if label == "mixed":
+            p.set_precision(egs.EGS_PRECISION_MIXED, BAND)
+        p.set_locations(xo, yo)
+        p.set_observations(zo)
+        f, count = guarded_objective(egs, p)
+        t0 = time.perf_counter()
+        th, fb, ne = egs.bobyqa_maximize(f, THETA, FIT_LB, FIT_UB, FIT_FTOL, C3_FIT_MAXEVAL, rhobeg=C3_FIT_RHOBEG)
+        fit_s = time.perf_counter() - t0
+        zm = p.predict(th, xm, ym)
+        res[label] = {"theta": th.tolist(), "loglik": fb, "evals": ne, "seconds": fit_s,
+                      "not_positive_definite": count["not_positive_definite"],
+                      "mspe": float(np.mean((za - zm) ** 2)), "z_miss": zm}
+        if label == "plain":
+            res["plain_loglik_at_mixed_theta"] = p.mle_eval(res["mixed"]["theta"])[0]
+        p.close()
+    tm, tp = np.array(res["mixed"]["theta"]), np.array(res["plain"]["theta"])
+    zm_m, zm_p = res["mixed"].pop("z_miss"), res["plain"].pop("z_miss")
+    theta = {"mixed": res["mixed"], "plain": res["plain"], "abs_diff": np.abs(tm - tp).tolist(),
+             "rel_diff": (np.abs(tm - tp) / np.abs(tp)).tolist(),
+             "plain_loglik_loss_at_mixed_theta": res["plain"]["loglik"] - res["plain_loglik_at_mixed_theta"],
+             "settings": f"N={len(zo)} of {N + C3_MISS} generated ({C3_MISS} held out), BOBYQA from the true theta, "
+                         f"rhobeg {C3_FIT_RHOBEG}, maxeval {C3_FIT_MAXEVAL}, bounds [0.01,5]^3, ftol_abs 1e-9, "
+                         "both forms"}
+    mspe = {"mixed": res["mixed"]["mspe"], "plain": res["plain"]["mspe"],
+            "rel_diff": abs(res["mixed"]["mspe"] - res["plain"]["mspe"]) / res["plain"]["mspe"],
+            "prediction_max_rel_diff": float(np.abs(zm_m - zm_p).max() / np.abs(zm_p).max()),
+            "note": "each form krieges at its own fitted theta with its own factorisation"}
+    return theta, mspe
 
 
 def run_serving(args):
@@ -380,6 +504,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-full-cpu", action="store_true",
+                    help="reference arm: skip the measured full-size CPU evaluation (84 GB of host memory)")
+    ap.add_argument("--no-fits", action="store_true",
+                    help="skip the fitted-theta / MSPE legs (N=102,400 mixed vs plain fits, N=40,000 fits)")
     ap.add_argument("--plain-steps", type=int, default=2, help="timed plain-FP64 evaluations at N=102400")
     ap.add_argument("--profile-eval", action="store_true",
                     help="one mixed evaluation between cudaProfilerStart/Stop (for ncu --profile-from-start off)")
@@ -565,7 +693,9 @@ def main():
         "gpu_launches": int(stage_launches.sum()),
         "clocks": clk,
     }
-    line["plain_n40000"] = plain_n40000(egs, torch, 3, fp64_peak)
+    if world == 1 and not args.no_fits:
+        rel["theta"], rel["mspe"] = c3_fit_leg(egs)
+        line["c2"] = c2_leg(egs, torch, 3, fp64_peak)
     line["small_n"] = small_problem_rate(egs, torch)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, info = cpu_sample(x, y, z)

@@ -1,0 +1,55 @@
+"""The plain-FP64 configuration at N = 40,000 (tile 960), end to end against the oracle.
+
+Data as the reference produces it: 41,000 locations from the reference
+generator with srand(0) (rootN = ceil(sqrt(41,000)) = 203, a 203-wide jittered
+grid whose last column is partial; LocationGenerator.cpp:33-49), Z = L e at the
+true theta (generated on the device; its parity is tested at small N), then
+1,000 points held out by the prediction module's Fisher-Yates split, which
+continues the generator's rand() stream (PredictionHelpers.cpp:140-168).
+For each true theta of the configuration the device evaluation at tile 960
+(ChameleonImplementation.cpp:35-327) and the kriging of the 1,000 held-out
+points (LinearAlgebraMethods.cpp:527-581) are checked against the large-N
+oracle (one generation and one blocked Cholesky on the host serve both):
+log-likelihood, log-determinant and Z^T Sigma^-1 Z within 1e-10 relative,
+predictions and MSPE within 1e-8 relative.  One oracle pass costs about 30 s
+of host time on 16 cores.
+"""
+import numpy as np
+import pytest
+
+import exageostatcpp_b200 as egs
+from oracle import cpu_baseline as C
+
+pytestmark = [pytest.mark.gpu, pytest.mark.slow]
+
+LOGLIK_RTOL = 1e-10
+PREDICT_RTOL = 1e-8
+
+
+@pytest.mark.parametrize("theta", [(1.0, 0.03, 1.5), (1.0, 0.05, 0.8)])
+def test_n40000_loglik_and_kriging_match_the_oracle(theta):
+    x, y = egs.generate_locations(41000, 0)
+    gen = egs.Problem(41000, 960)
+    gen.set_locations(x, y)
+    z = gen.generate_observations(theta, 0)
+    gen.close()
+    zo, xo, yo, za, xm, ym = egs.shuffle_split(z, x, y, 1000)
+    assert len(zo) == 40000 and len(za) == 1000
+
+    p = egs.Problem(40000, 960)
+    p.set_locations(xo, yo)
+    p.set_observations(zo)
+    ll, logdet, dot = p.mle_eval(theta)
+    zm = p.predict(theta, xm, ym)
+    p.close()
+    mspe = float(np.mean((za - zm) ** 2))
+
+    rll, rlogdet, rdot, rzm, rmspe, _ = C.eval_and_predict(xo, yo, zo, xm, ym, theta, za)
+    print(f"theta={theta} loglik {ll!r} oracle {rll!r} rel {abs(ll - rll) / abs(rll):.3e}; "
+          f"dot rel {abs(dot - rdot) / abs(rdot):.3e}; logdet rel {abs(logdet - rlogdet) / abs(rlogdet):.3e}; "
+          f"pred rel {np.abs(zm - rzm).max() / np.abs(rzm).max():.3e}; mspe {mspe!r} oracle {rmspe!r}")
+    assert ll == pytest.approx(rll, rel=LOGLIK_RTOL, abs=0)
+    assert logdet == pytest.approx(rlogdet, rel=LOGLIK_RTOL, abs=0)
+    assert dot == pytest.approx(rdot, rel=LOGLIK_RTOL, abs=0)
+    assert np.abs(zm - rzm).max() <= PREDICT_RTOL * np.abs(rzm).max()
+    assert mspe == pytest.approx(rmspe, rel=PREDICT_RTOL)

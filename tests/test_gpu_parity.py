@@ -232,20 +232,6 @@ def test_loglik_n10000_ts960_nonhalf_nu():
     assert ll == pytest.approx(ref, rel=LOGLIK_RTOL, abs=0)
 
 
-def _fit_pair(n, dts, maxeval):
-    from oracle import cpu_baseline as C
-    x, y, z = synthetic(n, 0, [1.0, 0.1, 0.5])
-    p = egs.Problem(n, dts)
-    p.set_locations(x, y)
-    p.set_observations(z)
-    lb, ub = [0.01] * 3, [5.0] * 3
-    gpu = lambda t: p.mle_eval(t)[0]
-    ora = lambda t: C.timed_eval(x, y, z, t)[0]
-    fit_g = egs.bobyqa_maximize(gpu, lb, lb, ub, 1e-9, maxeval)
-    fit_o = egs.bobyqa_maximize(ora, lb, lb, ub, 1e-9, maxeval)
-    return gpu, ora, fit_g, fit_o
-
-
 def test_fit_is_bit_reproducible_and_its_trajectory_matches_the_oracle():
     # The reference's N=1600 configuration: BOBYQA over [0.01, 5]^3 from the lower
     # bounds, tolerance 1e-9, at most 100 evaluations.
@@ -270,22 +256,83 @@ def test_fit_is_bit_reproducible_and_its_trajectory_matches_the_oracle():
         assert v == pytest.approx(ref, rel=LOGLIK_RTOL, abs=0)
 
 
-@pytest.mark.parametrize("n,dts", [(900, 320), pytest.param(1600, 320, marks=pytest.mark.slow)])
-def test_fit_matches_oracle_fit(n, dts):
-    # Converged fits driven by the GPU and by the CPU oracle.  Along the sigma^2-beta
-    # ridge the likelihood changes by < 1e-8 over ~1e-3 in theta, and the ftol_abs stop
-    # (an improvement below 1e-9) fires at different places when evaluations differ at
-    # 1e-13, so theta cannot agree to 1e-6; what is checked: both converge, to the same
-    # best value within 1e-7 relative, and each fitted theta is an optimum (to that
-    # accuracy) of the other implementation's likelihood.
-    gpu, ora, (th_g, f_g, n_g), (th_o, f_o, n_o) = _fit_pair(n, dts, 2000)
-    assert n_g < 2000 and n_o < 2000
-    tol = 1e-7 * abs(f_o)
-    assert f_g == pytest.approx(f_o, abs=tol)
-    assert ora(th_g) >= f_o - tol
-    assert gpu(th_o) >= f_g - tol
-    assert np.abs(th_g - th_o).max() < 5e-3
+def _newton_polish(f, theta, iters=30, rel_step=1e-4):
+    """Damped Newton ascent on f from theta with central-difference gradient and
+    Hessian (steps rel_step * |theta_i|); stops when a step is below 1e-10.
+    Returns (theta*, f(theta*), -Hessian at theta*)."""
+    t = np.array(theta, dtype=np.float64)
+    k = len(t)
+    negh = None
+    for _ in range(iters):
+        h = rel_step * np.abs(t)
+        f0 = f(t)
+        g = np.zeros(k)
+        hess = np.zeros((k, k))
+        for i in range(k):
+            e = np.zeros(k)
+            e[i] = h[i]
+            fp, fm = f(t + e), f(t - e)
+            g[i] = (fp - fm) / (2 * h[i])
+            hess[i, i] = (fp - 2 * f0 + fm) / h[i] ** 2
+        for i in range(k):
+            for j in range(i + 1, k):
+                ei, ej = np.zeros(k), np.zeros(k)
+                ei[i], ej[j] = h[i], h[j]
+                hess[i, j] = hess[j, i] = (f(t + ei + ej) - f(t + ei - ej) - f(t - ei + ej) + f(t - ei - ej)) / (
+                    4 * h[i] * h[j])
+        negh = -hess
+        step = np.linalg.solve(negh, g)
+        lam = 1.0
+        while f(t + lam * step) < f0 and lam > 1e-4:
+            lam *= 0.5
+        t = t + lam * step
+        if np.abs(lam * step).max() < 1e-10:
+            break
+    return t, f(t), negh
 
+
+@pytest.mark.slow
+def test_fitted_theta_matches_the_oracle_mle():
+    # The reference's N=1600 configuration: BOBYQA over [0.01, 5]^3 from the lower
+    # bounds, ftol_abs 1e-9, at most 100 evaluations (StarpuRuntimeSolver.cpp:38-48),
+    # driven once by the device likelihood and once by the oracle's.
+    #
+    # Where the fit stops is a property of the optimiser, not of the likelihood:
+    # 100 evaluations end ~10 log-units below the maximum, and an optimiser that
+    # stops at sub-optimality delta can sit anywhere within sqrt(2 delta / lambda_i)
+    # of the maximum along the eigenvector v_i of the negative Hessian (eigenvalue
+    # lambda_i).  The fitted theta that is a property of the implementation is the
+    # maximiser itself: each fit is carried to it by damped Newton steps on its own
+    # likelihood (central differences), and the two maximisers must agree within
+    # 1e-6 -- the contract's fitted-theta tolerance.  The BOBYQA stopping points
+    # must differ by no more than the bound derived above along every v_i.
+    from oracle import cpu_baseline as C
+    x, y, z = synthetic(1600, 0, [1.0, 0.1, 0.5])
+    p = egs.Problem(1600, 320)
+    p.set_locations(x, y)
+    p.set_observations(z)
+    lb, ub = [0.01] * 3, [5.0] * 3
+    gpu = lambda t: p.mle_eval(t)[0]  # noqa: E731
+    ora = lambda t: C.timed_eval(x, y, z, t)[0]  # noqa: E731
+    th_g, f_g, n_g = egs.bobyqa_maximize(gpu, lb, lb, ub, 1e-9, 100)
+    th_o, f_o, n_o = egs.bobyqa_maximize(ora, lb, lb, ub, 1e-9, 100)
+    star_g, fs_g, negh = _newton_polish(gpu, th_g)
+    star_o, fs_o, _ = _newton_polish(ora, th_o)
+    print(f"bobyqa gpu {th_g} ({n_g} evals, {f_g!r}) oracle {th_o} ({n_o} evals, {f_o!r}); "
+          f"maximiser gpu {star_g} {fs_g!r} oracle {star_o} {fs_o!r}")
+    # the maximisers of the two likelihoods
+    assert np.abs(star_g - star_o).max() <= 1e-6
+    assert fs_g == pytest.approx(fs_o, rel=LOGLIK_RTOL, abs=0)
+    assert np.all(star_g > lb) and np.all(star_g < ub)
+    # the optimiser's stopping points, against the bound their sub-optimality gives
+    lam, vec = np.linalg.eigh(negh)
+    assert np.all(lam > 0)  # a strict maximum
+    delta_g = max(fs_g - gpu(th_g), 0.0)
+    delta_o = max(fs_o - ora(th_o), 0.0)
+    diff = np.abs(vec.T @ (th_g - th_o))
+    bound = np.sqrt(2 * delta_g / lam) + np.sqrt(2 * delta_o / lam)
+    print(f"eigenvalues {lam}, |v_i^T (theta_gpu - theta_oracle)| {diff}, bound {bound}")
+    assert np.all(diff <= 1.05 * bound + 1e-9)
 
 
 @pytest.mark.parametrize("band", [1, 2, 3, 4, 8])
