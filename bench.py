@@ -634,9 +634,9 @@ def main():
 
     # --- rooflines of the update kernels (CUDA events around every launch) ---------------
     # DRAM bytes (read + write) per algorithmic flop of each kernel, from one ncu
-    # capture at N = 16,384 (profiles/split_gemm_kernel_n16384.md: 792,716,032 B
-    # for 78 target tiles of 2 * 1024^3 flops; profiles/ozaki_band_kernel_n16384.md:
-    # 644,593,920 B for the band update of step 0, 7.410e10 FP64-equivalent flops).
+    # capture of each at N = 16,384: the split kernel moved 792,716,032 B for 78
+    # target tiles of 2 * 1024^3 flops; the Ozaki kernel 644,593,920 B for the band
+    # update of step 0, 7.410e10 FP64-equivalent flops.
     # Both kernels' traffic grows with their target tiles, so a launch's traffic
     # is this ratio times its flops.
     split_bytes_per_flop = 792716032.0 / (78 * 2.0 * 1024 ** 3)

@@ -65,6 +65,12 @@ SIGNATURES = {
     "egs_mle_eval": (ctypes.c_int, [_P, _D, _D, _D, _D]),
     "egs_generate_locations": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _D, _D]),
     "egs_dlarnv_normal": (ctypes.c_int, [_I, ctypes.c_int, _D]),
+    "egs_save_observations": (ctypes.c_int, [_P]),
+    "egs_trsv_transpose": (ctypes.c_int, [_P]),
+    "egs_set_tile": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, _D]),
+    "egs_sequence_create": (ctypes.c_int, [ctypes.POINTER(_P)]),
+    "egs_sequence_wait": (ctypes.c_int, [_P]),
+    "egs_sequence_destroy": (ctypes.c_int, [_P]),
     "egs_shuffle_split": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _D, _D, _D, _D, _D]),
     "egs_generate_observations": (ctypes.c_int, [_P, _D, ctypes.c_int, _D]),
     "egs_mle_noalloc_workspace": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _LL]),

@@ -1252,6 +1252,54 @@ int egs_get_observations(egs_problem* p, double* host_z) {
   return EGS_OK;
 }
 
+int egs_save_observations(egs_problem* p) {
+  if (!p) return EGS_ERR_INVALID;
+  if (!p->have_observations) return EGS_ERR_STATE;
+  EGS_CUDA_TRY(cudaMemcpyAsync(p->zcpy, p->z, p->np * sizeof(double), cudaMemcpyDeviceToDevice, p->stream));
+  EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  return EGS_OK;
+}
+
+int egs_trsv_transpose(egs_problem* p) {
+  if (!p) return EGS_ERR_INVALID;
+  if (int rc = reject_mixed(p, "egs_trsv_transpose")) return rc;
+  enqueue_trsv_t(p);
+  int rc = check_cuda("egs_trsv_transpose");
+  if (rc != EGS_OK) return rc;
+  EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  return EGS_OK;
+}
+
+int egs_set_tile(egs_problem* p, int i, int j, const double* host_in) {
+  if (!p || !host_in || i < j || i >= p->nt || j < 0) return EGS_ERR_INVALID;
+  if (int rc = reject_mixed(p, "egs_set_tile")) return rc;
+  const size_t ts2 = (size_t)p->ts * p->ts;
+  EGS_CUDA_TRY(cudaMemcpyAsync(p->tiles + tile_slot(i, j, p->nt) * ts2, host_in, ts2 * sizeof(double),
+                               cudaMemcpyHostToDevice, p->stream));
+  EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  return EGS_OK;
+}
+
+int egs_sequence_create(void** sequence) {
+  if (!sequence) return EGS_ERR_INVALID;
+  cudaStream_t s = nullptr;
+  EGS_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  *sequence = s;
+  return EGS_OK;
+}
+
+int egs_sequence_wait(void* sequence) {
+  if (!sequence) return EGS_ERR_INVALID;
+  EGS_CUDA_TRY(cudaStreamSynchronize(static_cast<cudaStream_t>(sequence)));
+  return EGS_OK;
+}
+
+int egs_sequence_destroy(void* sequence) {
+  if (!sequence) return EGS_OK;
+  EGS_CUDA_TRY(cudaStreamDestroy(static_cast<cudaStream_t>(sequence)));
+  return EGS_OK;
+}
+
 int egs_mle_eval(egs_problem* p, const double* theta, double* loglik, double* logdet, double* dot) {
   if (!p || !loglik) return EGS_ERR_INVALID;
   if (!p->have_locations || !p->have_observations) return EGS_ERR_STATE;

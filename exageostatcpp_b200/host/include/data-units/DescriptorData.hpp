@@ -17,10 +17,15 @@
 
 namespace exageostat::dataunits {
 
+// The descriptor handle that the solver's tile operations take as void*
+// (the reference passes CHAM_desc_t*): the device problem it lives in and
+// which of the problem's matrices it names.
 template <typename T>
 struct DescriptorView {
   T* mat = nullptr;
   int m = 0, n = 0, mb = 0, nb = 0, mt = 0, nt = 0, lm = 0, ln = 0;
+  egs_problem* problem = nullptr;
+  common::DescriptorName name = common::DESCRIPTOR_C;
 };
 
 template <typename T>
@@ -84,6 +89,8 @@ class DescriptorData {
     v.nt = (aName == common::DESCRIPTOR_C) ? v.mt : 1;
     v.lm = mN;
     v.ln = v.n;
+    v.problem = mProblem;
+    v.name = aName;
     (void)ts;
     BaseDescriptor<T> d;
     d.chameleon_desc = d.cuda_desc = &v;

@@ -70,6 +70,63 @@ class CudaDense : public LinearAlgebraMethods<T> {
     return loglik;
   }
 
+  // ChameleonImplementation<T>::ExaGeoStatLapackCopyTile (ChameleonImplementation.cpp:329-335):
+  // the copies the evaluation makes, Z -> Zcpy (first evaluation, :113-119) and
+  // Zcpy -> Z (later ones, :120-124), on the data set's device problem.
+  void ExaGeoStatLapackCopyTile(const common::UpperLower& aUpperLower, void* apA, void* apB) override {
+    (void)aUpperLower;  // vectors: every part is copied
+    auto* a = this->View(apA, common::DESCRIPTOR_Z, "ExaGeoStatLapackCopyTile", true);
+    auto* b = this->View(apB, common::DESCRIPTOR_Z, "ExaGeoStatLapackCopyTile", true);
+    this->SameProblem(a, b, "ExaGeoStatLapackCopyTile");
+    if (a->name == common::DESCRIPTOR_Z && b->name == common::DESCRIPTOR_Z_COPY)
+      dataunits::EgsCheck(egs_save_observations(a->problem), "egs_save_observations");
+    else if (a->name == common::DESCRIPTOR_Z_COPY && b->name == common::DESCRIPTOR_Z)
+      dataunits::EgsCheck(egs_restore_observations(a->problem), "egs_restore_observations");
+    else
+      throw std::domain_error("ExaGeoStatLapackCopyTile: the device copies Z <-> Zcpy");
+  }
+
+  // ChameleonImplementation<T>::ExaGeoStatSequenceWait / ExaGeoStatCreateSequence
+  // (CHAMELEON_Sequence_Wait / _Create): a sequence is a CUDA stream of the library.
+  void ExaGeoStatSequenceWait(void* apSequence) override {
+    dataunits::EgsCheck(egs_sequence_wait(apSequence), "egs_sequence_wait");
+  }
+  void ExaGeoStatCreateSequence(void* apSequence) override {
+    dataunits::EgsCheck(egs_sequence_create(static_cast<void**>(apSequence)), "egs_sequence_create");
+  }
+
+  // ChameleonDense<T>::ExaGeoStatPotrfTile (ChameleonDense.cpp:25-37): lower Cholesky of
+  // the covariance in place; like the dense reference it ignores the band and the
+  // low-rank arguments (the data set's band approximation, when set, applies).
+  // A non-SPD matrix throws "Matrix is not positive definite" (:29-32).
+  void ExaGeoStatPotrfTile(const common::UpperLower& aUpperLower, void* apA, int aBand, void* apCD, void* apCrk,
+                           const int& aMaxRank, const int& aAcc) override {
+    (void)aBand, (void)apCD, (void)apCrk, (void)aMaxRank, (void)aAcc;
+    if (aUpperLower != common::EXAGEOSTAT_LOWER)
+      throw std::domain_error("the device factorisation is lower (EXAGEOSTAT_LOWER)");
+    auto* a = this->View(apA, common::DESCRIPTOR_C, "ExaGeoStatPotrfTile");
+    dataunits::EgsCheck(egs_potrf(a->problem), "egs_potrf");
+  }
+
+  // ChameleonImplementation<T>::ExaGeoStatTrsmTile (ChameleonImplementation.cpp:337-347):
+  // Z := op(L)^-1 Z with the factor of the same data set; the forms the reference
+  // uses (left, lower, non-unit, alpha 1), op = identity or transpose.
+  void ExaGeoStatTrsmTile(const common::Side& aSide, const common::UpperLower& aUpperLower,
+                          const common::Trans& aTrans, const common::Diag& aDiag, const T& aAlpha, void* apA,
+                          void* apCD, void* apCrk, void* apZ, const int& aMaxRank) override {
+    (void)apCD, (void)apCrk, (void)aMaxRank;
+    if (aSide != common::EXAGEOSTAT_LEFT || aUpperLower != common::EXAGEOSTAT_LOWER ||
+        aDiag != common::EXAGEOSTAT_NON_UNIT || aAlpha != T(1) || aTrans == common::EXAGEOSTAT_CONJ_TRANS)
+      throw std::domain_error("the device solve is left, lower, non-unit, alpha 1, with or without transpose");
+    auto* a = this->View(apA, common::DESCRIPTOR_C, "ExaGeoStatTrsmTile");
+    auto* z = this->View(apZ, common::DESCRIPTOR_Z, "ExaGeoStatTrsmTile");
+    this->SameProblem(a, z, "ExaGeoStatTrsmTile");
+    if (aTrans == common::EXAGEOSTAT_NO_TRANS)
+      dataunits::EgsCheck(egs_trsv(a->problem), "egs_trsv");
+    else
+      dataunits::EgsCheck(egs_trsv_transpose(a->problem), "egs_trsv_transpose");
+  }
+
   // LinearAlgebraMethods<T>::GenerateSyntheticData / GenerateObservationsVector
   // (LinearAlgebraMethods.cpp:322-449): Z = L e at the initial theta, e = DLARNV(3, {s,s,s,1}).
   void GenerateSyntheticData(configurations::Configurations& aConfigurations,

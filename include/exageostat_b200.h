@@ -156,6 +156,25 @@ EGS_API int egs_loglik_parts(egs_problem* p, double* loglik, double* logdet, dou
 EGS_API int egs_get_tile(egs_problem* p, int i, int j, double* host_out);
 /* Copy the current Z (n doubles) to host. */
 EGS_API int egs_get_observations(egs_problem* p, double* host_z);
+/* Zcpy := Z, the iteration-0 copy of ChameleonImplementation.cpp:113-119
+ * (ExaGeoStatLapackCopyTile, ChameleonImplementation.cpp:329-335, from Z to Zcpy). */
+EGS_API int egs_save_observations(egs_problem* p);
+/* Z := L^-T Z with the factor in the tiles: the transposed solve of
+ * ExaGeoStatTrsmTile (ChameleonImplementation.cpp:337-347 with Trans) and the
+ * second half of ExaGeoStatPosvTile (LinearAlgebraMethods.hpp:216, dposv). */
+EGS_API int egs_trsv_transpose(egs_problem* p);
+/* Copy a host tile (ts*ts doubles, column-major) into tile (i, j), i >= j: the
+ * tile-wise form of ExaGeoStatLap2Desc (LinearAlgebraMethods.hpp:275).  The
+ * caller keeps the identity padding of the last diagonal tile. */
+EGS_API int egs_set_tile(egs_problem* p, int i, int j, const double* host_in);
+/* A sequence is a CUDA stream owned by the library: egs_sequence_create replaces
+ * ExaGeoStatCreateSequence (CHAMELEON_Sequence_Create, LinearAlgebraMethods.hpp:169),
+ * egs_sequence_wait replaces ExaGeoStatSequenceWait (CHAMELEON_Sequence_Wait,
+ * LinearAlgebraMethods.hpp:161): it returns when all work on the stream is done.
+ * A problem runs its work on a sequence after egs_problem_set_stream(p, sequence). */
+EGS_API int egs_sequence_create(void** sequence);
+EGS_API int egs_sequence_wait(void* sequence);
+EGS_API int egs_sequence_destroy(void* sequence);
 
 /* One full log-likelihood evaluation at theta on the resident data: restore Z,
  * generate, factor, log-det, solve, dot, assemble.  Replaces

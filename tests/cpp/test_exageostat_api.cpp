@@ -19,6 +19,7 @@
 
 #include "api/ExaGeoStat.hpp"
 #include "hardware/ExaGeoStatHardware.hpp"
+#include "linear-algebra-solvers/LinearAlgebraFactory.hpp"
 
 using namespace exageostat;
 using namespace exageostat::common;
@@ -335,6 +336,95 @@ void csv_roundtrip(const std::string& dir) {
             << ", \"loglik_csv\": " << ll_csv << ", \"bad\": \"" << bad << "\"}" << std::endl;
 }
 
+// The seam's tile operations (LinearAlgebraMethods.hpp:62-64, 153-216, 275, 286)
+// driven the way ChameleonImplementation<T>::ExaGeoStatMLETile strings them
+// together (ChameleonImplementation.cpp:113-265), on descriptor handles from
+// DescriptorData::GetDescriptor: the log-likelihood assembled from the factor's
+// diagonal and the solved Z must equal one egs_mle_eval; dposv, the copies
+// between LAPACK and descriptor layouts and the argument checks are exercised too.
+void seam_tile_operations() {
+  Configurations c = modeling_config();
+  c.SetProblemSize(700);
+  c.SetDenseTileSize(128);
+  const std::vector<double> theta = {1.0, 0.1, 0.5};
+  auto hardware = ExaGeoStatHardware(EXACT_DENSE, 4, 0);
+  std::unique_ptr<ExaGeoStatData<double>> data;
+  api::ExaGeoStat<double>::ExaGeoStatLoadData(c, data);
+  const int n = c.GetProblemSize();
+  std::vector<double> z = data->GetDescriptorData()->HostVector(DESCRIPTOR_Z);
+  auto solver = linearAlgebra::LinearAlgebraFactory<double>::CreateLinearAlgebraSolver(EXACT_DENSE);
+  DescriptorData<double> dd;
+  solver->InitiateDescriptors(c, dd, 1, z.data());
+  egs_problem* p = dd.GetProblem();
+  EgsCheck(egs_problem_set_locations(p, data->GetLocations()->GetLocationX(), data->GetLocations()->GetLocationY()),
+           "egs_problem_set_locations");
+  void* C = dd.GetDescriptor(CHAMELEON_DESCRIPTOR, DESCRIPTOR_C).chameleon_desc;
+  void* Z = dd.GetDescriptor(CHAMELEON_DESCRIPTOR, DESCRIPTOR_Z).chameleon_desc;
+  void* Zcpy = dd.GetDescriptor(CHAMELEON_DESCRIPTOR, DESCRIPTOR_Z_COPY).chameleon_desc;
+  void* sequence = nullptr;
+  solver->ExaGeoStatCreateSequence(&sequence);
+  EgsCheck(egs_problem_set_stream(p, sequence), "egs_problem_set_stream");
+  solver->ExaGeoStatLapackCopyTile(EXAGEOSTAT_UPPER_LOWER, Z, Zcpy);
+  EgsCheck(egs_covariance_generate(p, theta.data()), "egs_covariance_generate");
+  std::vector<double> cov((size_t)n * n, 0.0), cov_back((size_t)n * n, 0.0);
+  solver->ExaGeoStatDesc2Lap(cov.data(), n, C, EXAGEOSTAT_LOWER);
+  solver->ExaGeoStatPotrfTile(EXAGEOSTAT_LOWER, C, 0, nullptr, nullptr, 0, 0);
+  std::vector<double> factor((size_t)n * n, 0.0);
+  solver->ExaGeoStatDesc2Lap(factor.data(), n, C, EXAGEOSTAT_LOWER);
+  solver->ExaGeoStatTrsmTile(EXAGEOSTAT_LEFT, EXAGEOSTAT_LOWER, EXAGEOSTAT_NO_TRANS, EXAGEOSTAT_NON_UNIT, 1.0, C,
+                             nullptr, nullptr, Z, 0);
+  solver->ExaGeoStatSequenceWait(sequence);
+  std::vector<double> v(n);
+  solver->ExaGeoStatDesc2Lap(v.data(), n, Z, EXAGEOSTAT_UPPER_LOWER);
+  double logdet = 0, dot = 0;
+  for (int i = 0; i < n; ++i) {
+    logdet += 2.0 * std::log(factor[i + (size_t)i * n]);
+    dot += v[i] * v[i];
+  }
+  const double ll_tiles = -0.5 * dot - 0.5 * logdet - (n / 2.0) * std::log(2.0 * PI);
+  // dposv on the regenerated covariance, restored Z: w = C^-1 z
+  solver->ExaGeoStatLapackCopyTile(EXAGEOSTAT_UPPER_LOWER, Zcpy, Z);
+  solver->ExaGeoStatLap2Desc(cov.data(), n, C, EXAGEOSTAT_LOWER);
+  std::vector<double> cov_uploaded((size_t)n * n, 0.0);
+  solver->ExaGeoStatDesc2Lap(cov_uploaded.data(), n, C, EXAGEOSTAT_LOWER);
+  double roundtrip = 0;
+  for (size_t i = 0; i < cov.size(); ++i) roundtrip = std::max(roundtrip, std::fabs(cov[i] - cov_uploaded[i]));
+  solver->ExaGeoStatPosvTile(EXAGEOSTAT_LOWER, C, Z);
+  std::vector<double> w(n);
+  solver->ExaGeoStatDesc2Lap(w.data(), n, Z, EXAGEOSTAT_LOWER);
+  // the same evaluation in one call
+  solver->ExaGeoStatLapackCopyTile(EXAGEOSTAT_UPPER_LOWER, Zcpy, Z);
+  double ll_eval = 0;
+  EgsCheck(egs_mle_eval(p, theta.data(), &ll_eval, nullptr, nullptr), "egs_mle_eval");
+  // the forms the device does not take are refused with the reference's exception types
+  std::string bad_uplo = "none", bad_trans = "none", bad_desc = "none";
+  try {
+    solver->ExaGeoStatPotrfTile(EXAGEOSTAT_UPPER, C, 0, nullptr, nullptr, 0, 0);
+  } catch (const std::domain_error& e) {
+    bad_uplo = e.what();
+  }
+  try {
+    solver->ExaGeoStatTrsmTile(EXAGEOSTAT_RIGHT, EXAGEOSTAT_LOWER, EXAGEOSTAT_NO_TRANS, EXAGEOSTAT_NON_UNIT, 1.0, C,
+                               nullptr, nullptr, Z, 0);
+  } catch (const std::domain_error& e) {
+    bad_trans = e.what();
+  }
+  try {
+    solver->ExaGeoStatPotrfTile(EXAGEOSTAT_LOWER, Z, 0, nullptr, nullptr, 0, 0);
+  } catch (const std::domain_error& e) {
+    bad_desc = e.what();
+  }
+  EgsCheck(egs_problem_set_stream(p, nullptr), "egs_problem_set_stream");
+  EgsCheck(egs_sequence_destroy(sequence), "egs_sequence_destroy");
+  std::cout.precision(17);
+  std::cout << "{\"n\": " << n << ", \"loglik_tiles\": " << ll_tiles << ", \"loglik_eval\": " << ll_eval
+            << ", \"logdet\": " << logdet << ", \"dot\": " << dot << ", \"roundtrip\": " << roundtrip
+            << ", \"w\": " << json_array(w.data(), n) << ", \"z\": " << json_array(z.data(), n)
+            << ", \"x\": " << json_array(data->GetLocations()->GetLocationX(), n)
+            << ", \"y\": " << json_array(data->GetLocations()->GetLocationY(), n) << ", \"bad_uplo\": \"" << bad_uplo
+            << "\", \"bad_trans\": \"" << bad_trans << "\", \"bad_desc\": \"" << bad_desc << "\"}" << std::endl;
+}
+
 int main(int argc, char** argv) {
   if (argc < 2) {
     std::cerr << "usage: test_exageostat_api <case> [fixture-file]\n";
@@ -352,6 +442,7 @@ int main(int argc, char** argv) {
     else if (which == "csv_roundtrip") csv_roundtrip(argv[2]);
     else if (which == "generated_locations") generated_locations();
     else if (which == "plugin_and_errors") plugin_and_errors(read_fixture(argv[2]));
+    else if (which == "seam_tile_operations") seam_tile_operations();
     else {
       std::cerr << "unknown case " << which << "\n";
       return 2;

@@ -95,4 +95,8 @@ def main(ref: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("EXAGEOSTAT_REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: extract_reference_goldens.py <ExaGeoStatCPP source tree> "
+                 "(or set EXAGEOSTAT_REFERENCE_ROOT)")
+    main(root)

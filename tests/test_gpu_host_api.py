@@ -117,3 +117,23 @@ def test_csv_loader_round_trip(driver, tmp_path):
     assert abs(out["loglik_csv"] - out["loglik_generated"]) <= 1e-12 * abs(out["loglik_generated"])
     assert "dimensions" in out["bad"]
     assert any(p.name == "SYN_16_1" for p in (tmp_path / "synthetic_ds").iterdir())
+
+
+@pytest.mark.gpu
+def test_seam_tile_operations_match_the_evaluation_and_the_oracle(driver):
+    # LinearAlgebraMethods' tile operations (InitiateDescriptors, CreateSequence,
+    # LapackCopyTile, PotrfTile, TrsmTile, SequenceWait, PosvTile, Desc2Lap,
+    # Lap2Desc) strung together as ChameleonImplementation.cpp:113-265 does.
+    from oracle import oracle as O
+    import scipy.linalg
+    out = run(driver, "seam_tile_operations")
+    x, y, z = (np.array(out[k]) for k in ("x", "y", "z"))
+    theta = [1.0, 0.1, 0.5]
+    ref, rlogdet, rdot = O.mle_loglik(x, y, z, theta, return_parts=True)
+    assert out["loglik_tiles"] == pytest.approx(ref, rel=1e-10, abs=0)
+    assert out["loglik_tiles"] == pytest.approx(out["loglik_eval"], rel=1e-12, abs=0)
+    assert out["dot"] == pytest.approx(rdot, rel=1e-10)
+    w = scipy.linalg.cho_solve(scipy.linalg.cho_factor(O.covariance(x, y, theta), lower=True), z)
+    assert np.abs(np.array(out["w"]) - w).max() <= 1e-9 * np.abs(w).max()
+    assert out["roundtrip"] == 0.0
+    assert "lower" in out["bad_uplo"] and "left" in out["bad_trans"] and "unexpected" in out["bad_desc"]
