@@ -59,6 +59,10 @@ FIT_LB, FIT_UB, FIT_FTOL, FIT_MAXEVAL = (0.01, 0.01, 0.01), (5.0, 5.0, 5.0), 1e-
 # Fitted theta and MSPE of the mixed form against the plain form at N = 102,400:
 # both fits start at the true theta with the same trust radius and budget.
 C3_FIT_MAXEVAL, C3_FIT_RHOBEG, C3_MISS = 15, 0.02, 1000
+# The batched configuration: 2,048 independent problems, N_i log-uniform in
+# [256, 4096], theta_i drawn per problem, one evaluation of all per optimiser step.
+C4_B, C4_NMIN, C4_NMAX, C4_SEED = 2048, 256, 4096, 12345
+C4_TILES = (128, 192, 256, 320)
 
 
 def env_rank():
@@ -371,6 +375,110 @@ def c2_leg(egs, torch, steps, peak):
                       "by the reference's rand() split), tile 960", "thetas": out}
 
 
+def c4_problems(egs):
+    """The batched configuration's problems: seed_i = i (the reference generator's
+    srand and DLARNV seeds), N_i = round(exp(U[ln 256, ln 4096])), sigma^2 ~ U[0.5, 2],
+    beta ~ U[0.02, 0.3], nu ~ U[0.3, 2.5] from one seeded host generator; jittered-grid
+    locations; observations are DLARNV N(0, 1) draws (an evaluation's cost does
+    not depend on their values).  Returns (sizes, x, y, z concatenated, theta (B, 3))."""
+    import numpy as np
+    rng = np.random.default_rng(C4_SEED)
+    sizes = np.rint(np.exp(rng.uniform(math.log(C4_NMIN), math.log(C4_NMAX), C4_B))).astype(np.int32)
+    theta = np.column_stack([rng.uniform(0.5, 2.0, C4_B), rng.uniform(0.02, 0.3, C4_B),
+                             rng.uniform(0.3, 2.5, C4_B)])
+    xs, ys, zs = [], [], []
+    for i, n in enumerate(sizes):
+        x, y = egs.generate_locations(int(n), i)
+        xs.append(x)
+        ys.append(y)
+        zs.append(egs.dlarnv_normal(i % 4096, int(n)))
+    return sizes, np.concatenate(xs), np.concatenate(ys), np.concatenate(zs), theta
+
+
+def c4_leg(egs, torch, steps):
+    """Batched evaluations of the 2,048-problem configuration: the tile size chosen
+    by the autotuner (one timed graph replay per candidate), then `steps` timed
+    replays (CUDA events), against the same problems evaluated one at a time on
+    the plain FP64 path (each problem's own graph replayed, the host waiting for
+    every result as a one-problem-per-call caller does).  Problems whose
+    covariance is not numerically positive definite (smooth, long-range
+    draws) are evaluated all the same and counted."""
+    import numpy as np
+    sizes, x, y, z, theta = c4_problems(egs)
+    t0 = time.perf_counter()
+    ts, tune_ms = egs.batch_autotune(sizes, x, y, z, theta, candidates=C4_TILES)
+    tune_s = time.perf_counter() - t0
+    b = egs.Batch(sizes, x, y, z, dts=ts)
+    for _ in range(3):
+        ll, st = b.eval(theta)
+    info = b.info()
+    # every step waits for its results (the optimiser needs them), so the host
+    # clock around the steps is the step time
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        ll, st = b.eval(theta)
+    host_s = time.perf_counter() - t0
+    b.close()
+    batch_evals_per_s = C4_B * steps / (host_s)
+    # one problem at a time, same problems and thetas, FP64, graph replay
+    offs = np.concatenate([[0], np.cumsum(sizes)])
+    single_s = 0.0
+    single_ll = np.empty(C4_B)
+    for i, n in enumerate(sizes):
+        p = egs.Problem(int(n), ts)
+        p.set_locations(x[offs[i]:offs[i + 1]], y[offs[i]:offs[i + 1]])
+        p.set_observations(z[offs[i]:offs[i + 1]])
+        for _ in range(2):
+            try:
+                p.mle_eval(theta[i])
+            except egs.NotPositiveDefinite:
+                pass
+        t1 = time.perf_counter()
+        try:
+            single_ll[i] = p.mle_eval(theta[i])[0]
+        except egs.NotPositiveDefinite:
+            single_ll[i] = np.nan
+        single_s += time.perf_counter() - t1
+        p.close()
+    ok = st == 0
+    agree = np.abs(ll[ok] - single_ll[ok]) / np.abs(single_ll[ok])
+    # whether the mixed-precision form could pay off at these sizes: one problem
+    # of N points evaluated in both forms (tile 256, FP64 band of 2 tiles)
+    mixed_vs_plain = []
+    for n in (1024, 2048, 4096):
+        xx, yy = egs.generate_locations(n, 0)
+        zz = egs.dlarnv_normal(0, n)
+        row = {"n": n}
+        for label, prec in (("plain_ms", egs.EGS_PRECISION_DOUBLE), ("mixed_ms", egs.EGS_PRECISION_MIXED)):
+            p = egs.Problem(n, 256)
+            if prec == egs.EGS_PRECISION_MIXED:
+                p.set_precision(prec, 2)
+            p.set_locations(xx, yy)
+            p.set_observations(zz)
+            for _ in range(3):
+                p.mle_eval((1.0, 0.1, 0.5))
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            for _ in range(20):
+                p.mle_eval((1.0, 0.1, 0.5))
+            row[label] = 1e3 * (time.perf_counter() - t1) / 20
+            p.close()
+        mixed_vs_plain.append(row)
+    flops = float(np.sum(sizes.astype(np.float64) ** 3 / 3.0))
+    return {"config": f"{C4_B} problems, N_i log-uniform in [{C4_NMIN}, {C4_NMAX}] (sum {int(sizes.sum())}), "
+                      "theta_i: sigma2 ~ U[0.5,2], beta ~ U[0.02,0.3], nu ~ U[0.3,2.5]; plain FP64",
+            "tile": ts, "autotune": {"candidates": list(C4_TILES), "best_ms_per_eval": tune_ms, "seconds": tune_s},
+            "evals_per_s": batch_evals_per_s, "ms_per_step": 1e3 * host_s / steps,
+            "steps": steps, "launches_per_step": info["launches_per_eval"],
+            "not_positive_definite": int((~ok).sum()),
+            "potrf_tflops": flops / (host_s / steps) / 1e12,
+            "one_at_a_time_evals_per_s": C4_B / single_s, "one_at_a_time_s": single_s,
+            "speedup_vs_one_at_a_time": batch_evals_per_s / (C4_B / single_s),
+            "max_rel_diff_vs_one_at_a_time": float(agree.max()) if agree.size else None,
+            "single_problem_mixed_vs_plain": mixed_vs_plain}
+
+
 def c3_fit_leg(egs):
     """Fitted theta and MSPE of the mixed form against the plain FP64 form at
     N = 102,400: N + 1,000 points generated (Z = L e at the true theta, FP64), 1,000
@@ -506,6 +614,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-full-cpu", action="store_true",
                     help="reference arm: skip the measured full-size CPU evaluation (84 GB of host memory)")
+    ap.add_argument("--no-batched", action="store_true", help="skip the 2,048-problem batched leg")
     ap.add_argument("--no-fits", action="store_true",
                     help="skip the fitted-theta / MSPE legs (N=102,400 mixed vs plain fits, N=40,000 fits)")
     ap.add_argument("--plain-steps", type=int, default=2, help="timed plain-FP64 evaluations at N=102400")
@@ -696,6 +805,8 @@ def main():
     if world == 1 and not args.no_fits:
         rel["theta"], rel["mspe"] = c3_fit_leg(egs)
         line["c2"] = c2_leg(egs, torch, 3, fp64_peak)
+    if world == 1 and not args.no_batched:
+        line["batched"] = c4_leg(egs, torch, 5)
     line["small_n"] = small_problem_rate(egs, torch)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, info = cpu_sample(x, y, z)

@@ -26,21 +26,32 @@
 // FP32 registers with round-to-nearest.  The bias drops to that of four
 // instructions (~2e-7 relative), the same order as plain FP32 rounding.
 //
-// Kernel structure (one CTA per SM, persistent over 128 x 256 output tiles):
-//   warp 0    TMA producer: per 64-wide K stage, the A rows (hi, lo) and B rows
-//             (hi, lo) of the tile, 128B-swizzled, into a 2-stage ring; a few
-//             stages before a tile ends it prefetches the tile's C block to L2;
-//   warp 1    allocates 512 TMEM columns (two 128 x 256 FP32 stage
-//             accumulators) and issues the tcgen05.mma instructions from one
-//             thread; commits release the ring stage and hand the stage
-//             accumulator to the epilogue;
-//   warps 2-9 epilogue: warp w reads TMEM lanes 32 (w % 4) .. +32 (thread =
-//             tile row) and one half of the columns, adds every stage into 128
-//             FP32 registers, and after the last stage applies
-//             C -= acc * inv_s_row * inv_s_col, coalesced along each column.
+// Kernel structure: persistent clusters of two CTAs on the two SMs of a TPC,
+// one 256 x 256 output tile per pair at a time, issued as tcgen05.mma of
+// cta_group::2 (M = 256, N = 256): each CTA holds its 128 rows of A and 128
+// of the 256 rows of B in its own shared memory, the tensor cores of both SMs
+// read both B halves, and each CTA's tensor memory receives its 128 rows x 256
+// columns of the product.  Against one CTA per 128 x 256 tile this halves the
+// B operand every SM stages (64 KB per 64-wide K stage instead of 96 KB), so
+// the ring holds three stages instead of two and the L2 -> SM operand traffic
+// per flop drops by a third.
+//   warp 0    TMA producer of each CTA: per K stage its A rows (hi, lo) and its
+//             B half (hi, lo), 128B-swizzled, into a 3-stage ring; the copies of
+//             both CTAs complete on the leader CTA's full barrier; a few stages
+//             before a tile ends it prefetches its C block to L2;
+//   warp 1    allocates 512 TMEM columns in both CTAs (two 128 x 256 FP32 stage
+//             accumulators per CTA); in the leader CTA (rank 0) one thread
+//             issues the MMAs, and its commits arrive on the ring and the
+//             accumulator barriers of both CTAs;
+//   warps 2-9 epilogue of each CTA: warp w reads TMEM lanes 32 (w % 4) .. +32
+//             (thread = tile row) and one half of the columns, adds every stage
+//             into 128 FP32 registers, releases the stage accumulator to the
+//             leader, and after the last stage applies C -= acc * inv_s_row *
+//             inv_s_col through TMA reduce-adds.
 // The two stage accumulators let the MMAs of stage s+1 overlap the draining of
 // stage s.  Every mbarrier wait is bounded; a timed-out CTA records the error,
-// stops, and still frees its tensor memory.
+// stops, and still meets its peer at the final cluster barrier and frees its
+// tensor memory.  No copy is multicast: each CTA loads only what it holds.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_fp16.h>
@@ -54,10 +65,11 @@
 namespace egs {
 
 namespace sg {
-constexpr int BM = 128, BN = 256, BK = 64, STAGES = 2;
+// BM: rows of the output tile each CTA holds; the pair covers PM = 2 BM rows.
+constexpr int BM = 128, PM = 256, BN = 256, BK = 64, STAGES = 3;
 constexpr int BOX_ROWS = 128;                      // TMA box: 64 fp16 (128 B) x 128 rows
-constexpr int A_BYTES = BM * BK * 2;               // 16 KB
-constexpr int B_BYTES = BN * BK * 2;               // 32 KB
+constexpr int A_BYTES = BM * BK * 2;               // 16 KB: this CTA's A rows
+constexpr int B_BYTES = (BN / 2) * BK * 2;         // 16 KB: this CTA's half of B
 constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
 constexpr int EPI_WARPS = 8;                       // two per TMEM lane quarter
 constexpr int THREADS = 64 + 32 * EPI_WARPS;       // producer, MMA issuer, epilogue
@@ -72,8 +84,8 @@ constexpr int SMEM_BYTES = 1024 + STAGES * STAGE_BYTES + STAGING_BYTES + 256;
 static_assert(SMEM_BYTES <= 232448, "shared memory per CTA");
 constexpr uint32_t TMEM_COLS = 512;
 // Instruction descriptor of kind::f16: D F32 (bits 4-5 = 1), A and B F16 (0),
-// both K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28.
-constexpr uint32_t IDESC = (1u << 4) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+// both K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28 (M of the pair).
+constexpr uint32_t IDESC = (1u << 4) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(PM >> 4) << 24);
 }  // namespace sg
 
 // ---------------------------------------------------------------------------
@@ -143,25 +155,52 @@ __device__ __forceinline__ uint64_t sdesc_sw128(uint32_t addr) {
   d |= (uint64_t)2 << 61;             // SWIZZLE_128B
   return d;
 }
-__device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+// D (both CTAs' tensor memory) += A B^T over the CTA pair; issued by one thread
+// of the leader CTA, the operands at the same shared-memory offsets in both CTAs.
+__device__ __forceinline__ void umma_f16_pair(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
       "l"(adesc), "l"(bdesc), "r"(sg::IDESC), "r"(accumulate)
       : "memory");
 }
-__device__ __forceinline__ void umma_commit(uint64_t* bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-               : "memory");
+// Arrives on the barrier at this offset in both CTAs of the pair once the MMAs
+// issued so far have completed.
+__device__ __forceinline__ void umma_commit_pair(uint64_t* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+          smem_u32(bar)),
+      "h"((uint16_t)0x3)
+      : "memory");
+}
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+// Address of this CTA's shared variable p in CTA `rank` of the cluster.
+__device__ __forceinline__ uint32_t cluster_addr(const void* p, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t bar_cluster_addr) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(bar_cluster_addr) : "memory");
+}
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+// Box (x, y) into this CTA's shared memory; the bytes complete on the barrier at
+// bar_cluster_addr, which may lie in the peer CTA of the pair (no multicast).
+__device__ __forceinline__ void tma_load_2d_pair(void* dst, const CUtensorMap* map, uint32_t bar_cluster_addr, int x,
+                                                 int y) {
   asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
-          smem_u32(dst)),
-      "l"((uint64_t)map), "r"(x), "r"(y), "r"(smem_u32(bar))
+      "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+      "[%4];" ::"r"(smem_u32(dst)),
+      "l"((uint64_t)map), "r"(x), "r"(y), "r"(bar_cluster_addr)
       : "memory");
 }
 // out[box at (x, y)] += smem (FP32 add performed at L2), tracked in this thread's bulk group.
@@ -208,7 +247,7 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 }
 
 // Target tile of work item L at step k: targets are enumerated column by column
-// (j = k+1, ...; i = j+band+1 .. nt-1), each split into (ts/BM) x (ts/BN) CTA
+// (j = k+1, ...; i = j+band+1 .. nt-1), each split into (ts/PM) x (ts/BN) pair
 // tiles with the row block fastest.
 struct SplitStep {
   int ts, nt, band, k;
@@ -235,7 +274,7 @@ __device__ __forceinline__ void decode_item(const SplitStep& P, long long L, int
   i = j + P.band + 1 + (int)q;
 }
 
-__global__ void __launch_bounds__(sg::THREADS, 1)
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(sg::THREADS, 1)
 split_gemm_kernel(const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo,
                   const __grid_constant__ CUtensorMap tm_c, const __grid_constant__ CUtensorMap tm_cr,
                   const __grid_constant__ SplitStep P) {
@@ -252,26 +291,31 @@ split_gemm_kernel(const __grid_constant__ CUtensorMap tm_hi, const __grid_consta
   volatile int& bail = bail_flag;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_rank();
+  const bool leader = rank == 0;
+  const long long pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
-      mbar_init(&full[s], 1);
-      mbar_init(&empty[s], 1);
+      mbar_init(&full[s], 1);    // the leader's producer (expect_tx of both CTAs' bytes)
+      mbar_init(&empty[s], 1);   // the leader's MMA commit, in both CTAs
     }
     for (int b = 0; b < 2; ++b) {
-      mbar_init(&acc_full[b], 1);
-      mbar_init(&acc_empty[b], EPI_WARPS);
+      mbar_init(&acc_full[b], 1);               // the leader's MMA commit, in both CTAs
+      mbar_init(&acc_empty[b], 2 * EPI_WARPS);  // the epilogue warps of both CTAs (leader's copy)
     }
     bail = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+    // same warp and same slot offset in both CTAs
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                  "r"(TMEM_COLS)
                  : "memory");
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
   }
   tc_fence_before();
-  __syncthreads();
+  // both CTAs' barriers are initialised before any copy or arrive can reach them
+  cluster_sync_all();
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
   const int ksteps = P.ts / BK;
@@ -281,10 +325,10 @@ split_gemm_kernel(const __grid_constant__ CUtensorMap tm_hi, const __grid_consta
     if (lane == 0) {
       uint32_t it = 0;
       const int mm = P.nt - P.band - 1;
-      for (long long L = blockIdx.x; L < P.total && !bail; L += gridDim.x) {
+      for (long long L = pair; L < P.total && !bail; L += npairs) {
         int i, j, mb, nb;
         decode_item(P, L, i, j, mb, nb);
-        const int arow = i * P.ts + mb * BM, brow = j * P.ts + nb * BN;
+        const int arow = i * P.ts + mb * PM + (int)rank * BM, brow = j * P.ts + nb * BN + (int)rank * (BN / 2);
         for (int kt = 0; kt < ksteps; ++kt, ++it) {
           const uint32_t s = it % STAGES;
           if (it >= (uint32_t)STAGES && !mbar_wait(&empty[s], ((it / STAGES) & 1) ^ 1, P.err)) {
@@ -292,30 +336,32 @@ split_gemm_kernel(const __grid_constant__ CUtensorMap tm_hi, const __grid_consta
             break;
           }
           uint8_t* st = smem + s * STAGE_BYTES;
-          mbar_expect_tx(&full[s], STAGE_BYTES);
+          if (leader) mbar_expect_tx(&full[s], 2 * STAGE_BYTES);
+          const uint32_t fb = cluster_addr(&full[s], 0);
           const int x = kt * BK;
-          tma_load_2d(st, &tm_hi, &full[s], x, arow);
-          tma_load_2d(st + A_BYTES, &tm_lo, &full[s], x, arow);
-          tma_load_2d(st + 2 * A_BYTES, &tm_hi, &full[s], x, brow);
-          tma_load_2d(st + 2 * A_BYTES + BOX_ROWS * 128, &tm_hi, &full[s], x, brow + BOX_ROWS);
-          tma_load_2d(st + 2 * A_BYTES + B_BYTES, &tm_lo, &full[s], x, brow);
-          tma_load_2d(st + 2 * A_BYTES + B_BYTES + BOX_ROWS * 128, &tm_lo, &full[s], x, brow + BOX_ROWS);
+          tma_load_2d_pair(st, &tm_hi, fb, x, arow);
+          tma_load_2d_pair(st + A_BYTES, &tm_lo, fb, x, arow);
+          tma_load_2d_pair(st + 2 * A_BYTES, &tm_hi, fb, x, brow);
+          tma_load_2d_pair(st + 2 * A_BYTES + B_BYTES, &tm_lo, fb, x, brow);
           if (kt == pf_kt) {
-            // the tile's C block (BM rows x BN columns of an FP32 tile) into L2
+            // this CTA's C block (BM rows x BN columns of an FP32 tile) into L2
             const long long slot = tile_slot(i - P.band - 1, j, mm);
-            tma_prefetch_l2_2d(&tm_c, mb * BM, (int)(slot * P.ts + nb * BN));
+            tma_prefetch_l2_2d(&tm_c, mb * PM + (int)rank * BM, (int)(slot * P.ts + nb * BN));
           }
         }
       }
-      // drain: the stages issued last must land before the CTA may exit
-      const uint32_t first = it > (uint32_t)STAGES ? it - STAGES : 0;
-      for (uint32_t q = first; q < it; ++q) mbar_wait(&full[q % STAGES], (q / STAGES) & 1, P.err);
+      // drain (leader): the stages issued last must land before either CTA may exit;
+      // the peer's copies complete on the same barriers
+      if (leader) {
+        const uint32_t first = it > (uint32_t)STAGES ? it - STAGES : 0;
+        for (uint32_t q = first; q < it; ++q) mbar_wait(&full[q % STAGES], (q / STAGES) & 1, P.err);
+      }
     }
   } else if (warp == 1) {
-    if (lane == 0) {
+    if (lane == 0 && leader) {
       uint32_t it = 0;
       bool ok = true;
-      for (long long L = blockIdx.x; L < P.total && ok && !bail; L += gridDim.x) {
+      for (long long L = pair; L < P.total && ok && !bail; L += npairs) {
         for (int kt = 0; kt < ksteps; ++kt, ++it) {
           // stage it accumulates into buffer it & 1 from zero
           const uint32_t ab = it & 1, s = it % STAGES;
@@ -335,16 +381,16 @@ split_gemm_kernel(const __grid_constant__ CUtensorMap tm_hi, const __grid_consta
 #pragma unroll
           for (int kk = 0; kk < BK / 16; ++kk) {
             const uint32_t off = kk * 32;
-            umma_f16(dcol, sdesc_sw128(sa + off), sdesc_sw128(sbl + off), kk > 0 ? 1u : 0u);
-            umma_f16(dcol, sdesc_sw128(sal + off), sdesc_sw128(sbh + off), 1u);
+            umma_f16_pair(dcol, sdesc_sw128(sa + off), sdesc_sw128(sbl + off), kk > 0 ? 1u : 0u);
+            umma_f16_pair(dcol, sdesc_sw128(sal + off), sdesc_sw128(sbh + off), 1u);
           }
 #pragma unroll
           for (int kk = 0; kk < BK / 16; ++kk) {
             const uint32_t off = kk * 32;
-            umma_f16(dcol, sdesc_sw128(sa + off), sdesc_sw128(sbh + off), 1u);
+            umma_f16_pair(dcol, sdesc_sw128(sa + off), sdesc_sw128(sbh + off), 1u);
           }
-          umma_commit(&empty[s]);
-          umma_commit(&acc_full[ab]);
+          umma_commit_pair(&empty[s]);
+          umma_commit_pair(&acc_full[ab]);
         }
       }
       if (!ok) bail = 1;
@@ -355,7 +401,7 @@ split_gemm_kernel(const __grid_constant__ CUtensorMap tm_hi, const __grid_consta
     const uint32_t tl = tmem_base + ((uint32_t)(quarter * 32) << 16) + half * HALF_COLS;
     uint32_t it = 0, red_count = 0;
     bool ok = true;
-    for (long long L = blockIdx.x; L < P.total && ok; L += gridDim.x) {
+    for (long long L = pair; L < P.total && ok; L += npairs) {
       float acc[HALF_COLS];  // zero plus the first stage is that stage's value
 #pragma unroll
       for (int c = 0; c < HALF_COLS; ++c) acc[c] = 0.f;
@@ -379,7 +425,7 @@ split_gemm_kernel(const __grid_constant__ CUtensorMap tm_hi, const __grid_consta
         }
         tc_fence_before();
         __syncwarp();
-        if (lane == 0) mbar_arrive(&acc_empty[ab]);
+        if (lane == 0) mbar_arrive_remote(cluster_addr(&acc_empty[ab], 0));
       }
       if (!ok) break;
       // C -= acc * inv_r * inv_c: the scaled update goes through this warp's
@@ -389,7 +435,7 @@ split_gemm_kernel(const __grid_constant__ CUtensorMap tm_hi, const __grid_consta
       decode_item(P, L, i, j, mb, nb);
       const int mm = P.nt - P.band - 1;
       const long long slot = tile_slot(i - P.band - 1, j, mm);
-      const int r0 = mb * BM + quarter * 32;
+      const int r0 = mb * PM + (int)rank * BM + quarter * 32;
       const int c0 = nb * BN + half * HALF_COLS;
       const float inv_r = P.inv_scale[(long long)i * P.ts + r0 + lane];
       const float* inv_c = P.inv_scale + (long long)j * P.ts + c0;
@@ -418,12 +464,15 @@ split_gemm_kernel(const __grid_constant__ CUtensorMap tm_hi, const __grid_consta
     __syncwarp();
     if (!ok) bail = 1;
   }
+  // neither CTA leaves (or frees its tensor memory) while the other may still
+  // issue MMAs into it, read its shared memory or arrive on its barriers
+  __syncwarp();
   tc_fence_before();
-  __syncthreads();
+  cluster_sync_all();
   if (warp == 1) {
     __syncwarp();
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS) : "memory");
   }
 }
 
@@ -499,6 +548,38 @@ long long split_targets(int nt, int band, int k) {
   return n;
 }
 
+// Clusters of split_gemm_kernel that can be resident at once on the current
+// device (once per device; half the SM count if the query fails).
+static long long split_max_pairs() {
+  static std::once_flag done[64];
+  static long long pairs_of[64];
+  int dev = 0;
+  cudaGetDevice(&dev);
+  auto query = [dev]() {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(2 * 74, 1, 1);
+    cfg.blockDim = dim3(sg::THREADS, 1, 1);
+    cfg.dynamicSmemBytes = sg::SMEM_BYTES;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, split_gemm_kernel, &cfg) != cudaSuccess || n <= 0) {
+      cudaGetLastError();
+      n = gemm_num_sms() / 2;
+    }
+    if (dev >= 0 && dev < 64) pairs_of[dev] = n;
+    return n;
+  };
+  if (dev < 0 || dev >= 64) return query();
+  std::call_once(done[dev], query);
+  return pairs_of[dev];
+}
+
 int launch_split_update(const void* tm_hi, const void* tm_lo, const void* tm_c, const void* tm_cr, int ts, int nt,
                         int band, int k, float* c_pool, const float* inv_scale, int* err, cudaStream_t st,
                         int max_ctas) {
@@ -514,14 +595,18 @@ int launch_split_update(const void* tm_hi, const void* tm_lo, const void* tm_c, 
   P.nt = nt;
   P.band = band;
   P.k = k;
-  P.mblocks = ts / BM;
+  P.mblocks = ts / PM;
   P.nblocks = ts / BN;
   P.total = targets * P.mblocks * P.nblocks;
   P.c_pool = c_pool;
   P.inv_scale = inv_scale;
   P.err = err;
-  const long long cap = (max_ctas > 0 && max_ctas < gemm_num_sms()) ? max_ctas : gemm_num_sms();
-  const long long grid = P.total < cap ? P.total : cap;
+  // clusters of two CTAs: as many pairs as fit on the device at once (SMs of a
+  // TPC pair up; a TPC with one usable SM runs none), at most one per pair tile
+  long long pairs = split_max_pairs();
+  if (max_ctas > 0 && max_ctas / 2 < pairs) pairs = max_ctas / 2 > 0 ? max_ctas / 2 : 1;
+  if (P.total < pairs) pairs = P.total;
+  const long long grid = 2 * pairs;
   split_gemm_kernel<<<(unsigned)grid, THREADS, SMEM_BYTES, st>>>(*reinterpret_cast<const CUtensorMap*>(tm_hi),
                                                                  *reinterpret_cast<const CUtensorMap*>(tm_lo),
                                                                  *reinterpret_cast<const CUtensorMap*>(tm_c),

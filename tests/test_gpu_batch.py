@@ -125,3 +125,41 @@ def test_batch_autotune_returns_a_candidate():
     ts, ms = egs.batch_autotune(sizes, *concat(xs, ys, zs), theta=[1.0, 0.1, 0.5], candidates=(64, 128, 192))
     assert ts in (64, 128, 192)
     assert ms > 0
+
+
+def test_batch_of_64_uneven_problems_matches_the_single_problem_path():
+    # The batched configuration's shape at test size: 64 problems, N log-uniform
+    # in [256, 1024], theta drawn per problem as in that configuration (beta up to
+    # 0.3, nu up to 2.5; a draw whose covariance is not numerically positive
+    # definite must be reported the same way by both paths).
+    rng = np.random.default_rng(7)
+    B = 64
+    sizes = np.rint(np.exp(rng.uniform(np.log(256), np.log(1024), B))).astype(int)
+    th = np.column_stack([rng.uniform(0.5, 2.0, B), rng.uniform(0.02, 0.3, B), rng.uniform(0.3, 2.5, B)])
+    xs, ys, zs = [], [], []
+    for i, n in enumerate(sizes):
+        x, y = egs.generate_locations(int(n), i)
+        xs.append(x)
+        ys.append(y)
+        zs.append(egs.dlarnv_normal(i, int(n)))
+    b = egs.Batch(sizes, *concat(xs, ys, zs), dts=192)
+    ll, st = b.eval(th)
+    ll2, st2 = b.eval(th)  # graph replay
+    assert np.array_equal(ll, ll2) and np.array_equal(st, st2)
+    b.close()
+    compared = 0
+    for i, n in enumerate(sizes):
+        p = egs.Problem(int(n), 192)
+        p.set_locations(xs[i], ys[i])
+        p.set_observations(zs[i])
+        try:
+            ref = p.mle_eval(th[i])[0]
+        except egs.NotPositiveDefinite:
+            assert st[i] > 0, i
+            continue
+        finally:
+            p.close()
+        assert st[i] == 0, i
+        assert abs(ll[i] - ref) <= SAME_TS_RTOL * abs(ref), (i, n, ll[i], ref)
+        compared += 1
+    assert compared >= B // 2
