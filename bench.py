@@ -63,6 +63,9 @@ C3_FIT_MAXEVAL, C3_FIT_RHOBEG, C3_MISS = 15, 0.02, 1000
 # [256, 4096], theta_i drawn per problem, one evaluation of all per optimiser step.
 C4_B, C4_NMIN, C4_NMAX, C4_SEED = 2048, 256, 4096, 12345
 C4_TILES = (128, 192, 256, 320)
+# The serving configuration in the default run: two arrival rates, the
+# reference's fit budget for fit requests.
+SERVE_SECONDS, SERVE_FIT_EVALS = 30.0, 100
 
 
 def env_rank():
@@ -524,6 +527,18 @@ def c3_fit_leg(egs):
 
 
 def run_serving(args):
+    """``--workload serving``: the sweep alone, one JSON line per (form, rate) and a summary."""
+    import torch
+    import exageostatcpp_b200 as egs
+    torch.cuda.set_device(0)
+    lines = serving_sweep(egs, args.serve_rates, args.serve_seconds, args.serve_slots, args.serve_fit_evals,
+                          verbose=True)
+    print(json.dumps({"metric": METRIC, "workload": "serving", "unit": UNIT, "slots": args.serve_slots,
+                      "hbm_budget_gb": 160, "fit_max_evals": args.serve_fit_evals, "sweep": lines}), flush=True)
+    return 0
+
+
+def serving_sweep(egs, rates, seconds, slots, fit_evals, verbose=False):
     """Open-loop Poisson request stream through the serving loop, rate swept.
 
     Mix: 35% log-likelihood, 35% fit (BOBYQA, at most --serve-fit-evals
@@ -534,9 +549,6 @@ def run_serving(args):
     (submission to completion) and evaluations/s per rate, for the plain and the
     mixed form (FP64 band of 2 tiles)."""
     import numpy as np
-    import torch
-    import exageostatcpp_b200 as egs
-    torch.cuda.set_device(0)
     rng = np.random.default_rng(12345)
     pool = []
     for i in range(24):
@@ -546,14 +558,14 @@ def run_serving(args):
         pool.append((x, y, z))
     xm_all, ym_all = rng.random(500), rng.random(500)
     lines = []
-    for rate in args.serve_rates:
+    for rate in rates:
         # one arrival sequence per rate, replayed for both forms
         g = np.random.default_rng(int(rate * 1000) + 7)
         arr = []
         t = 0.0
         while True:
             t += g.exponential(1.0 / rate)
-            if t > args.serve_seconds:
+            if t > seconds:
                 break
             arr.append(t)
         picks = []
@@ -569,11 +581,11 @@ def run_serving(args):
                 dts = 512 if len(z) < 8000 else 1024
                 r = dict(kind=kind, x=x, y=y, z=z, dts=dts, theta=theta, precision=precision,
                          band_tiles=2 if precision == egs.EGS_PRECISION_MIXED else 0,
-                         max_evals=args.serve_fit_evals, ftol_abs=1e-9)
+                         max_evals=fit_evals, ftol_abs=1e-9)
                 if kind == egs.EGS_REQ_PREDICT:
                     r["x_miss"], r["y_miss"] = xm_all, ym_all
                 reqs.append((a, r))
-            with egs.Server(hbm_budget=160 * 10**9, max_active=args.serve_slots) as srv:
+            with egs.Server(hbm_budget=160 * 10**9, max_active=slots) as srv:
                 t0 = time.perf_counter()
                 tickets = []
                 for a, r in reqs:
@@ -596,13 +608,15 @@ def run_serving(args):
                           "failed": int(sum(r.status != 0 for r in res)),
                           "failed_not_positive_definite": int(sum(r.status > 0 for r in res)),
                           "answered_in_fp64": int(sum(r.precision_used != precision for r in res)),
+                          "fp64_predicted": int(sum(r.fp64_reason == egs.EGS_FP64_REASON_PREDICTED for r in res)),
+                          "fp64_after_failure": int(sum(r.fp64_reason == egs.EGS_FP64_REASON_AFTER_FAILURE
+                                                        for r in res)),
                           "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                           "evals_per_s": st["evals"] / span, "span_s": span, "per_kind": per,
                           "peak_active": st["peak_active"], "peak_reserved_gb": st["peak_reserved"] / 1e9})
-            print(json.dumps(lines[-1]), flush=True)
-    print(json.dumps({"metric": METRIC, "workload": "serving", "unit": UNIT, "slots": args.serve_slots,
-                      "hbm_budget_gb": 160, "fit_max_evals": args.serve_fit_evals, "sweep": lines}), flush=True)
-    return 0
+            if verbose:
+                print(json.dumps(lines[-1]), flush=True)
+    return lines
 
 
 def main():
@@ -615,6 +629,7 @@ def main():
     ap.add_argument("--no-full-cpu", action="store_true",
                     help="reference arm: skip the measured full-size CPU evaluation (84 GB of host memory)")
     ap.add_argument("--no-batched", action="store_true", help="skip the 2,048-problem batched leg")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving sweep of the default run")
     ap.add_argument("--no-fits", action="store_true",
                     help="skip the fitted-theta / MSPE legs (N=102,400 mixed vs plain fits, N=40,000 fits)")
     ap.add_argument("--plain-steps", type=int, default=2, help="timed plain-FP64 evaluations at N=102400")
@@ -628,7 +643,7 @@ def main():
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[0.25, 0.5, 1.0])
     ap.add_argument("--serve-seconds", type=float, default=30.0)
     ap.add_argument("--serve-slots", type=int, default=6)
-    ap.add_argument("--serve-fit-evals", type=int, default=10)
+    ap.add_argument("--serve-fit-evals", type=int, default=SERVE_FIT_EVALS)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -807,6 +822,14 @@ def main():
         line["c2"] = c2_leg(egs, torch, 3, fp64_peak)
     if world == 1 and not args.no_batched:
         line["batched"] = c4_leg(egs, torch, 5)
+    if world == 1 and not args.no_serving:
+        rates = (0.15, 0.3)
+        line["serving"] = {
+            "config": f"open-loop Poisson arrivals for {SERVE_SECONDS:.0f} s per rate, 35% log-likelihood, 35% fit "
+                      f"(BOBYQA, at most {SERVE_FIT_EVALS} evaluations, ftol_abs 1e-9: the reference's MLE budget), "
+                      "30% predict (500 targets); N log-uniform in [1000, 60000]; theta as in the batched "
+                      "configuration; 160 GB admission budget; 6 slots; observations i.i.d. N(0,1)",
+            "sweep": serving_sweep(egs, rates, SERVE_SECONDS, 6, SERVE_FIT_EVALS)}
     line["small_n"] = small_problem_rate(egs, torch)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, info = cpu_sample(x, y, z)

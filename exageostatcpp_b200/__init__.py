@@ -29,6 +29,9 @@ EGS_BAND_FP64_DMMA = 1
 EGS_REQ_LOGLIK = 1
 EGS_REQ_FIT = 2
 EGS_REQ_PREDICT = 3
+EGS_FP64_REASON_NONE = 0
+EGS_FP64_REASON_PREDICTED = 1
+EGS_FP64_REASON_AFTER_FAILURE = 2
 
 STAGES = ("generate", "panel", "update", "solve", "reduce", "update_low")
 NUM_STAGES = len(STAGES)
@@ -113,7 +116,8 @@ class Result(ctypes.Structure):
     """egs_result of the serving API."""
     _fields_ = [("status", ctypes.c_int), ("kind", ctypes.c_int), ("loglik", ctypes.c_double),
                 ("theta", ctypes.c_double * 3), ("evals", ctypes.c_int), ("queue_ms", ctypes.c_double),
-                ("latency_ms", ctypes.c_double), ("footprint", ctypes.c_longlong), ("precision_used", ctypes.c_int)]
+                ("latency_ms", ctypes.c_double), ("footprint", ctypes.c_longlong), ("precision_used", ctypes.c_int),
+                ("fp64_reason", ctypes.c_int)]
 
 
 SIGNATURES.update({
@@ -122,6 +126,7 @@ SIGNATURES.update({
     "egs_server_wait": (ctypes.c_int, [_P, ctypes.c_longlong, ctypes.POINTER(Result), _D]),
     "egs_server_stats": (ctypes.c_int, [_P, _I, _I, _LL, _I, _LL, _LL, _LL]),
     "egs_server_destroy": (ctypes.c_int, [_P]),
+    "egs_mixed_conditioning_estimate": (ctypes.c_int, [ctypes.c_int, _D, _D, _D, _D]),
 })
 
 OBJECTIVE = ctypes.CFUNCTYPE(ctypes.c_double, ctypes.c_int, _D, ctypes.c_void_p)
@@ -492,6 +497,16 @@ def fisher_host(x, y, theta, dts: int) -> np.ndarray:
     _check(load_library().egs_fisher_host(len(xx), int(dts), _dptr(xx), _dptr(yy), _dptr(th), _dptr(out)),
            "egs_fisher_host")
     return out.reshape(3, 3).T
+
+
+def mixed_conditioning_estimate(x, y, theta) -> float:
+    """The serving loop's condition estimate of the Matern covariance (host arithmetic)."""
+    lib = load_library()
+    x, y, th = _f64(x), _f64(y), _f64(theta)
+    k = ctypes.c_double()
+    _check(lib.egs_mixed_conditioning_estimate(len(x), _dptr(x), _dptr(y), _dptr(th), ctypes.byref(k)),
+           "mixed_conditioning_estimate")
+    return k.value
 
 
 def footprint(n: int, dts: int, precision: int = EGS_PRECISION_DOUBLE, band_tiles: int = 0) -> int:

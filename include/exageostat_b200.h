@@ -450,7 +450,21 @@ typedef struct egs_result {
   int precision_used;  /* the precision that produced the result: a mixed request whose
                           factorisation is not positive definite (FP32 off-band storage
                           of a very smooth kernel) is answered by the FP64 path */
+  int fp64_reason;     /* why a mixed request was answered in FP64: EGS_FP64_REASON_* */
 } egs_result;
+
+#define EGS_FP64_REASON_NONE 0           /* answered in the requested precision */
+#define EGS_FP64_REASON_PREDICTED 1      /* estimated too ill-conditioned for FP32 tiles: FP64 from the start */
+#define EGS_FP64_REASON_AFTER_FAILURE 2  /* the mixed factorisation failed; re-run in FP64 */
+
+/* Condition estimate of the Matern covariance of n locations at theta that the
+ * serving loop uses to send a mixed-precision request to the FP64 path up front
+ * (no counterpart in the reference, which has no mixed form): with h the mean
+ * spacing sqrt(bounding-box area / n), *kappa = (1 + (pi beta / h)^2)^(nu + 1),
+ * the ratio of the Matern spectral density at frequency 0 and at the grid's
+ * Nyquist frequency pi / h.  Host arithmetic only. */
+EGS_API int egs_mixed_conditioning_estimate(int n, const double* x, const double* y, const double* theta,
+                                            double* kappa);
 
 /* Start a server on `device` with hbm_budget bytes of admission budget and at
  * most max_active concurrently running requests (one host worker thread and

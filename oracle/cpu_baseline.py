@@ -224,6 +224,19 @@ def timed_eval(x, y, z, theta, a=None):
     return loglik, {"generate": t1 - t0, "potrf": t2 - t1, "solve": t3 - t2}
 
 
+def timed_eval_parts(x, y, z, theta):
+    """(loglik, logdet, dot) of one host evaluation (the pieces of timed_eval)."""
+    n = len(z)
+    a = matern_lower(x, y, theta)
+    if potrf_blocked(a) != 0:
+        raise np.linalg.LinAlgError("Matrix is not positive definite")
+    d = np.diag(a)
+    logdet = 2.0 * float(np.sum(np.log(d[d > 0])))
+    w = trsv_blocked(a, z)
+    dot = float(w @ w)
+    return -0.5 * dot - 0.5 * logdet - (n / 2.0) * math.log(2.0 * PI), logdet, dot
+
+
 def scaled_evals_per_s(stage_s: dict, n_sample: int, n_target: int) -> float:
     """Scale a sample evaluation to n_target: generation and solve ~ n^2, potrf ~ n^3."""
     r = n_target / n_sample

@@ -53,3 +53,36 @@ def test_n40000_loglik_and_kriging_match_the_oracle(theta):
     assert dot == pytest.approx(rdot, rel=LOGLIK_RTOL, abs=0)
     assert np.abs(zm - rzm).max() <= PREDICT_RTOL * np.abs(rzm).max()
     assert mspe == pytest.approx(rmspe, rel=PREDICT_RTOL)
+
+
+MIXED_RTOL = 1e-6        # the mixed form's contract for exponential to moderately smooth kernels
+MIXED_SMOOTH_RTOL = 5e-5  # smooth, long-range kernels (nu >= 1.3), as bounded at small N
+
+
+@pytest.mark.parametrize("theta", [(1.0, 0.05, 0.8), (1.0, 0.03, 1.5)])
+def test_n40000_mixed_precision_against_the_oracle(theta):
+    # The mixed form (FP64 diagonal + band of 2 tiles, FP32 off-band tiles with
+    # split-FP16 tensor-core updates, one refinement step) on the same data,
+    # against the FP64 oracle at N = 40,000.
+    x, y = egs.generate_locations(41000, 0)
+    gen = egs.Problem(41000, 960)
+    gen.set_locations(x, y)
+    z = gen.generate_observations(theta, 0)
+    gen.close()
+    zo, xo, yo, za, xm, ym = egs.shuffle_split(z, x, y, 1000)
+    p = egs.Problem(40000, 1024)
+    p.set_precision(egs.EGS_PRECISION_MIXED, 2)
+    p.set_locations(xo, yo)
+    p.set_observations(zo)
+    try:
+        ll, logdet, dot = p.mle_eval(theta)
+    except egs.NotPositiveDefinite:
+        p.close()
+        assert theta[2] >= 1.3, "only a smooth kernel may lose definiteness in FP32 storage"
+        pytest.skip(f"theta={theta}: the FP32 off-band storage is not positive definite (served in FP64)")
+    p.close()
+    rll, rlogdet, rdot = C.timed_eval_parts(xo, yo, zo, theta)
+    rel = abs(ll - rll) / abs(rll)
+    print(f"mixed theta={theta}: loglik rel {rel:.3e}, logdet rel {abs(logdet - rlogdet) / abs(rlogdet):.3e}, "
+          f"dot rel {abs(dot - rdot) / abs(rdot):.3e}")
+    assert rel <= (MIXED_RTOL if theta[2] < 1.3 else MIXED_SMOOTH_RTOL)

@@ -181,6 +181,28 @@ def test_mixed_request_that_loses_definiteness_is_answered_in_fp64():
             if rm.precision_used == D:
                 fell_back += 1
                 assert rm.loglik == rp.loglik
+                assert rm.fp64_reason in (egs.EGS_FP64_REASON_PREDICTED, egs.EGS_FP64_REASON_AFTER_FAILURE)
+            else:
+                assert rm.fp64_reason == egs.EGS_FP64_REASON_NONE
             else:
                 assert abs(rm.loglik - rp.loglik) <= 1e-4 * abs(rp.loglik)
     assert fell_back >= 1
+
+
+def test_ill_conditioned_mixed_request_goes_to_fp64_up_front():
+    # theta = (1, 0.3, 2.5) on 24,000 points: estimated kappa ~ 1e15, far above the
+    # FP32 off-band storage's reach (it fails there on a B200); the request is
+    # answered by the FP64 path without a mixed attempt, with the plain result.
+    # theta = (1, 0.05, 0.5) on the same points stays in mixed precision.
+    x, y = egs.generate_locations(24000, 2)
+    z = egs.dlarnv_normal(2, 24000)
+    with egs.Server(hbm_budget=60 << 30, max_active=2) as s:
+        tm = s.submit(egs.EGS_REQ_LOGLIK, x, y, z, 1024, theta=(1.0, 0.3, 2.5), precision=M, band_tiles=2)
+        tp = s.submit(egs.EGS_REQ_LOGLIK, x, y, z, 1024, theta=(1.0, 0.3, 2.5))
+        (rm, _), (rp, _) = s.wait(tm), s.wait(tp)
+        tk = s.submit(egs.EGS_REQ_LOGLIK, x, y, z, 1024, theta=(1.0, 0.05, 0.5), precision=M, band_tiles=2)
+        rk, _ = s.wait(tk)
+    assert rp.status == 0 and rm.status == 0
+    assert rm.precision_used == D and rm.fp64_reason == egs.EGS_FP64_REASON_PREDICTED
+    assert rm.loglik == rp.loglik and rm.evals == 1
+    assert rk.status == 0 and rk.precision_used == M and rk.fp64_reason == egs.EGS_FP64_REASON_NONE

@@ -45,3 +45,24 @@ def test_server_needs_a_device():
     h = ctypes.c_void_p()
     assert lib.egs_server_create(ctypes.byref(h), 0, 1 << 30, 2) == egs.EGS_ERR_NO_DEVICE
     assert lib.egs_server_create(ctypes.byref(h), 0, 0, 2) == egs.EGS_ERR_INVALID
+
+
+def test_conditioning_estimate_formula_and_measured_classification():
+    # kappa = (1 + (pi beta / h)^2)^(nu + 1), h = sqrt(bounding-box area / n)
+    x = [0.0, 1.0, 0.0, 1.0]
+    y = [0.0, 0.0, 2.0, 2.0]
+    k = egs.mixed_conditioning_estimate(x, y, [1.0, 0.1, 0.5])
+    h = (2.0 / 4) ** 0.5
+    assert k == pytest.approx((1 + (3.141592653589793 * 0.1 / h) ** 2) ** 1.5, rel=1e-14)
+    # Outcomes of the mixed form (FP64 band of 2 tiles, FP32 off-band tiles) measured
+    # on a B200 on jittered unit-square grids; the server's limit is 1e9.
+    measured = [  # (n, beta, nu, mixed factorisation positive definite)
+        (6000, 0.1, 1.8, True), (6000, 0.3, 1.2, True), (24000, 0.2, 1.2, True), (24000, 0.3, 0.7, True),
+        (6000, 0.1, 2.5, False), (6000, 0.2, 1.8, False), (24000, 0.1, 1.8, False), (24000, 0.3, 1.2, False),
+    ]
+    for n, beta, nu, ok in measured:
+        xs, ys = egs.generate_locations(n, 1)
+        kappa = egs.mixed_conditioning_estimate(xs, ys, [1.0, beta, nu])
+        assert (kappa <= 1e9) == ok, (n, beta, nu, kappa)
+    with pytest.raises(egs.EgsError):
+        egs.mixed_conditioning_estimate(x, y, [1.0, -0.1, 0.5])
