@@ -184,7 +184,6 @@ def test_mixed_request_that_loses_definiteness_is_answered_in_fp64():
                 assert rm.fp64_reason in (egs.EGS_FP64_REASON_PREDICTED, egs.EGS_FP64_REASON_AFTER_FAILURE)
             else:
                 assert rm.fp64_reason == egs.EGS_FP64_REASON_NONE
-            else:
                 assert abs(rm.loglik - rp.loglik) <= 1e-4 * abs(rp.loglik)
     assert fell_back >= 1
 
