@@ -185,8 +185,12 @@ __device__ __forceinline__ uint32_t cluster_addr(const void* p, uint32_t rank) {
   asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(rank));
   return r;
 }
+// Arrive on a barrier of the peer CTA.  The default (CTA-scope release)
+// semantics suffice: what the arrive publishes is the completion of this
+// warp's tensor-memory loads, ordered by tcgen05.fence::before_thread_sync;
+// a cluster-scope release would add a memory barrier to every stage.
 __device__ __forceinline__ void mbar_arrive_remote(uint32_t bar_cluster_addr) {
-  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(bar_cluster_addr) : "memory");
+  asm volatile("mbarrier.arrive.shared::cluster.b64 _, [%0];" ::"r"(bar_cluster_addr) : "memory");
 }
 __device__ __forceinline__ void cluster_sync_all() {
   asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
@@ -425,7 +429,12 @@ split_gemm_kernel(const __grid_constant__ CUtensorMap tm_hi, const __grid_consta
         }
         tc_fence_before();
         __syncwarp();
-        if (lane == 0) mbar_arrive_remote(cluster_addr(&acc_empty[ab], 0));
+        if (lane == 0) {
+          if (leader)
+            mbar_arrive(&acc_empty[ab]);
+          else
+            mbar_arrive_remote(cluster_addr(&acc_empty[ab], 0));
+        }
       }
       if (!ok) break;
       // C -= acc * inv_r * inv_c: the scaled update goes through this warp's
