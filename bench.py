@@ -409,9 +409,10 @@ def c4_leg(egs, torch, steps):
     import numpy as np
     sizes, x, y, z, theta = c4_problems(egs)
     t0 = time.perf_counter()
-    ts, tune_ms = egs.batch_autotune(sizes, x, y, z, theta, candidates=C4_TILES)
+    upper, tiles, tune_ms = egs.batch_set_autotune(sizes, x, y, z, theta, candidates=C4_TILES, max_classes=3)
     tune_s = time.perf_counter() - t0
-    b = egs.Batch(sizes, x, y, z, dts=ts)
+    ts1, one_class_ms = egs.batch_autotune(sizes, x, y, z, theta, candidates=C4_TILES)
+    b = egs.BatchSet(sizes, x, y, z, upper_n=upper, dts=tiles)
     for _ in range(3):
         ll, st = b.eval(theta)
     info = b.info()
@@ -429,7 +430,7 @@ def c4_leg(egs, torch, steps):
     single_s = 0.0
     single_ll = np.empty(C4_B)
     for i, n in enumerate(sizes):
-        p = egs.Problem(int(n), ts)
+        p = egs.Problem(int(n), next(t for u, t in zip(info["upper_n"], info["ts"]) if n <= u))
         p.set_locations(x[offs[i]:offs[i + 1]], y[offs[i]:offs[i + 1]])
         p.set_observations(z[offs[i]:offs[i + 1]])
         for _ in range(2):
@@ -471,9 +472,10 @@ def c4_leg(egs, torch, steps):
     flops = float(np.sum(sizes.astype(np.float64) ** 3 / 3.0))
     return {"config": f"{C4_B} problems, N_i log-uniform in [{C4_NMIN}, {C4_NMAX}] (sum {int(sizes.sum())}), "
                       "theta_i: sigma2 ~ U[0.5,2], beta ~ U[0.02,0.3], nu ~ U[0.3,2.5]; plain FP64",
-            "tile": ts, "autotune": {"candidates": list(C4_TILES), "best_ms_per_eval": tune_ms, "seconds": tune_s},
-            "evals_per_s": batch_evals_per_s, "ms_per_step": 1e3 * host_s / steps,
-            "steps": steps, "launches_per_step": info["launches_per_eval"],
+            "schedule": {"classes": info["classes"], "upper_n": info["upper_n"], "tiles": info["ts"]},
+            "autotune": {"candidates": list(C4_TILES), "max_classes": 3, "best_ms_per_eval": tune_ms,
+                         "seconds": tune_s, "one_class_tile": ts1, "one_class_ms_per_eval": one_class_ms},
+            "evals_per_s": batch_evals_per_s, "ms_per_step": 1e3 * host_s / steps, "steps": steps,
             "not_positive_definite": int((~ok).sum()),
             "potrf_tflops": flops / (host_s / steps) / 1e12,
             "one_at_a_time_evals_per_s": C4_B / single_s, "one_at_a_time_s": single_s,

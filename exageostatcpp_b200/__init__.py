@@ -74,6 +74,12 @@ SIGNATURES = {
     "egs_sequence_create": (ctypes.c_int, [ctypes.POINTER(_P)]),
     "egs_sequence_wait": (ctypes.c_int, [_P]),
     "egs_sequence_destroy": (ctypes.c_int, [_P]),
+    "egs_batch_set_create": (ctypes.c_int, [ctypes.POINTER(_P), ctypes.c_int, _I, _D, _D, _D, ctypes.c_int, _I, _I]),
+    "egs_batch_set_destroy": (ctypes.c_int, [_P]),
+    "egs_batch_set_eval": (ctypes.c_int, [_P, _D, _D, _I]),
+    "egs_batch_set_info": (ctypes.c_int, [_P, _I, _I, _I, ctypes.POINTER(ctypes.c_longlong)]),
+    "egs_batch_set_autotune": (ctypes.c_int, [ctypes.c_int, _I, _D, _D, _D, _D, _I, ctypes.c_int, ctypes.c_int, _I,
+                                              _I, _I, _D]),
     "egs_shuffle_split": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _D, _D, _D, _D, _D]),
     "egs_generate_observations": (ctypes.c_int, [_P, _D, ctypes.c_int, _D]),
     "egs_mle_noalloc_workspace": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _LL]),
@@ -460,6 +466,74 @@ def batch_autotune(sizes, x, y, z, theta, candidates=(128, 192, 256, 320)):
                                   _dptr(th), cand.ctypes.data_as(_I), len(cand), ctypes.byref(best),
                                   ctypes.byref(ms)), "egs_batch_autotune")
     return best.value, ms.value
+
+
+class BatchSet:
+    """A batch cut into size classes (``egs_batch_set``), each with its own tile
+    size; the classes of one evaluation overlap on the device.  ``upper_n[c]`` is
+    the largest N of class c; arguments as for :class:`Batch`."""
+
+    def __init__(self, sizes, x, y, z, upper_n, dts):
+        self._lib = load_library()
+        self.sizes = np.ascontiguousarray(sizes, dtype=np.int32)
+        x, y, z = _f64(x), _f64(y), _f64(z)
+        if not (len(x) == len(y) == len(z) == int(self.sizes.sum())):
+            raise ValueError("x, y, z must hold sum(sizes) points")
+        self.B = len(self.sizes)
+        up = np.ascontiguousarray(upper_n, dtype=np.int32)
+        ts = np.ascontiguousarray(dts, dtype=np.int32)
+        self._h = _P()
+        _check(self._lib.egs_batch_set_create(ctypes.byref(self._h), self.B, self.sizes.ctypes.data_as(_I), _dptr(x),
+                                              _dptr(y), _dptr(z), len(up), up.ctypes.data_as(_I),
+                                              ts.ctypes.data_as(_I)), "egs_batch_set_create")
+
+    def info(self):
+        nc = ctypes.c_int()
+        up = np.zeros(16, dtype=np.int32)
+        ts = np.zeros(16, dtype=np.int32)
+        nb = ctypes.c_longlong()
+        _check(self._lib.egs_batch_set_info(self._h, ctypes.byref(nc), up.ctypes.data_as(_I), ts.ctypes.data_as(_I),
+                                            ctypes.byref(nb)), "egs_batch_set_info")
+        return {"classes": nc.value, "upper_n": up[:nc.value].tolist(), "ts": ts[:nc.value].tolist(),
+                "bytes": nb.value}
+
+    def eval(self, theta):
+        th = _f64(np.broadcast_to(np.asarray(theta, dtype=np.float64), (self.B, 3)))
+        ll = np.empty(self.B)
+        st = np.zeros(self.B, dtype=np.int32)
+        rc = self._lib.egs_batch_set_eval(self._h, _dptr(th), _dptr(ll), st.ctypes.data_as(_I))
+        if rc not in (EGS_OK, EGS_ERR_STATE):
+            _check(rc, "egs_batch_set_eval")
+        return ll, st
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.egs_batch_set_destroy(self._h)
+            self._h = _P()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def batch_set_autotune(sizes, x, y, z, theta, candidates=(128, 192, 256, 320), max_classes=3):
+    """Schedule of a batch: (upper_n list, tile list, ms per evaluation) of the fastest class split."""
+    lib = load_library()
+    sizes = np.ascontiguousarray(sizes, dtype=np.int32)
+    B = len(sizes)
+    th = _f64(np.broadcast_to(np.asarray(theta, dtype=np.float64), (B, 3)))
+    cand = np.ascontiguousarray(candidates, dtype=np.int32)
+    nc = ctypes.c_int()
+    up = np.zeros(16, dtype=np.int32)
+    ts = np.zeros(16, dtype=np.int32)
+    ms = ctypes.c_double()
+    _check(lib.egs_batch_set_autotune(B, sizes.ctypes.data_as(_I), _dptr(_f64(x)), _dptr(_f64(y)), _dptr(_f64(z)),
+                                      _dptr(th), cand.ctypes.data_as(_I), len(cand), int(max_classes),
+                                      ctypes.byref(nc), up.ctypes.data_as(_I), ts.ctypes.data_as(_I),
+                                      ctypes.byref(ms)), "egs_batch_set_autotune")
+    return up[:nc.value].tolist(), ts[:nc.value].tolist(), ms.value
 
 
 def split_update(ts: int, nt: int, band: int, k: int, panel_ptr: int, offband_ptr: int) -> float:

@@ -18,6 +18,7 @@
 //  * the whole evaluation of all problems is captured once as a CUDA graph and
 //    replayed for every new set of theta (one graph launch per optimiser step).
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <memory>
 #include <numeric>
@@ -479,8 +480,14 @@ int egs_batch_info(const egs_batch* b, int* ts, int* nt_max, long long* bytes, l
   return EGS_OK;
 }
 
-int egs_batch_eval(egs_batch* b, const double* theta, double* loglik, int* status) {
-  if (!b || !theta || !loglik) return EGS_ERR_INVALID;
+}  // extern "C"
+
+namespace {
+
+// First half of an evaluation: parameters to the device and the whole batched
+// evaluation enqueued on the batch's stream (captured as a graph from the
+// second evaluation on).  Returns without waiting.
+int batch_launch(egs_batch* b, const double* theta) {
   cudaStream_t st = b->stream;
   if (cudaStreamSynchronize(st) != cudaSuccess) return check("egs_batch_eval");
   for (int p = 0; p < b->B; ++p) {
@@ -519,7 +526,12 @@ int egs_batch_eval(egs_batch* b, const double* theta, double* loglik, int* statu
     if (rc != EGS_OK) return rc;
   }
   ++b->evals;
-  if (cudaStreamSynchronize(st) != cudaSuccess) return check("egs_batch_eval/sync");
+  return EGS_OK;
+}
+
+// Second half: wait for the batch's stream and read every problem's result.
+int batch_collect(egs_batch* b, double* loglik, int* status) {
+  if (cudaStreamSynchronize(b->stream) != cudaSuccess) return check("egs_batch_eval/sync");
   if (*b->h_err != 0) {
     set_last_error("a device-side wait exceeded its limit", "egs_batch_eval");
     return EGS_ERR_TIMEOUT;
@@ -532,6 +544,17 @@ int egs_batch_eval(egs_batch* b, const double* theta, double* loglik, int* statu
     if (b->h_info[p] > 0) ++failures;
   }
   return failures ? EGS_ERR_STATE : EGS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int egs_batch_eval(egs_batch* b, const double* theta, double* loglik, int* status) {
+  if (!b || !theta || !loglik) return EGS_ERR_INVALID;
+  const int rc = batch_launch(b, theta);
+  if (rc != EGS_OK) return rc;
+  return batch_collect(b, loglik, status);
 }
 
 int egs_batch_autotune(int B, const int* n, const double* x, const double* y, const double* z,
@@ -564,6 +587,203 @@ int egs_batch_autotune(int B, const int* n, const double* x, const double* y, co
   }
   if (arg < 0) return EGS_ERR_STATE;
   *best_ts = arg;
+  if (best_ms) *best_ms = best;
+  return EGS_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Size classes: problems cut by N into classes, each an egs_batch with its own
+// tile size; one evaluation launches every class on its own stream before it
+// waits for any, so the classes' work overlaps on the device.
+// ---------------------------------------------------------------------------
+
+struct egs_batch_set {
+  int B = 0;
+  std::vector<egs_batch*> cls;
+  std::vector<std::vector<int>> members;  // caller indices of each class
+  std::vector<int> upper, ts;
+  std::vector<double> th, ll;
+  std::vector<int> st;
+};
+
+namespace {
+
+void free_set(egs_batch_set* s) {
+  if (!s) return;
+  for (egs_batch* b : s->cls) free_batch(b);
+  delete s;
+}
+
+// Class boundaries: the sorted sizes cut into ncl runs of about equal n^3 cost;
+// upper[c] is the largest N of class c.
+std::vector<int> cost_boundaries(std::vector<int> sizes, int ncl) {
+  std::sort(sizes.begin(), sizes.end());
+  double total = 0.0;
+  for (int v : sizes) total += (double)v * v * v;
+  std::vector<int> upper;
+  double acc = 0.0;
+  int c = 1;
+  for (size_t i = 0; i < sizes.size(); ++i) {
+    acc += (double)sizes[i] * sizes[i] * sizes[i];
+    if (c < ncl && acc >= total * c / ncl && i + 1 < sizes.size() && sizes[i + 1] > sizes[i]) {
+      upper.push_back(sizes[i]);
+      ++c;
+    }
+  }
+  upper.push_back(sizes.back());
+  return upper;
+}
+
+}  // namespace
+
+extern "C" {
+
+int egs_batch_set_create(egs_batch_set** out, int B, const int* n, const double* x, const double* y,
+                         const double* z, int nclass, const int* upper_n, const int* dts) {
+  if (!out || B <= 0 || !n || !x || !y || !z || nclass <= 0 || nclass > 16 || !upper_n || !dts)
+    return EGS_ERR_INVALID;
+  *out = nullptr;
+  for (int c = 0; c < nclass; ++c)
+    if (dts[c] <= 0 || (c > 0 && upper_n[c] <= upper_n[c - 1])) return EGS_ERR_INVALID;
+  std::vector<long long> off(B + 1, 0);
+  for (int i = 0; i < B; ++i) {
+    if (n[i] <= 0) return EGS_ERR_INVALID;
+    if (n[i] > upper_n[nclass - 1]) {
+      set_last_error("a problem is larger than the last class bound", "egs_batch_set_create");
+      return EGS_ERR_INVALID;
+    }
+    off[i + 1] = off[i] + n[i];
+  }
+  auto* s = new egs_batch_set();
+  s->B = B;
+  for (int c = 0; c < nclass; ++c) {
+    std::vector<int> mem, nn;
+    std::vector<double> cx, cy, cz;
+    for (int i = 0; i < B; ++i) {
+      const int lo = c > 0 ? upper_n[c - 1] : 0;
+      if (n[i] <= lo || n[i] > upper_n[c]) continue;
+      mem.push_back(i);
+      nn.push_back(n[i]);
+      cx.insert(cx.end(), x + off[i], x + off[i + 1]);
+      cy.insert(cy.end(), y + off[i], y + off[i + 1]);
+      cz.insert(cz.end(), z + off[i], z + off[i + 1]);
+    }
+    if (mem.empty()) continue;
+    egs_batch* b = nullptr;
+    const int rc = egs_batch_create(&b, (int)mem.size(), nn.data(), dts[c], cx.data(), cy.data(), cz.data());
+    if (rc != EGS_OK) {
+      free_set(s);
+      return rc;
+    }
+    s->cls.push_back(b);
+    s->members.push_back(std::move(mem));
+    s->upper.push_back(upper_n[c]);
+    s->ts.push_back(b->ts);
+  }
+  *out = s;
+  return EGS_OK;
+}
+
+int egs_batch_set_destroy(egs_batch_set* s) {
+  free_set(s);
+  return EGS_OK;
+}
+
+int egs_batch_set_eval(egs_batch_set* s, const double* theta, double* loglik, int* status) {
+  if (!s || !theta || !loglik) return EGS_ERR_INVALID;
+  int rc = EGS_OK;
+  const size_t ncl = s->cls.size();
+  size_t launched = 0;
+  for (; launched < ncl; ++launched) {
+    const auto& mem = s->members[launched];
+    s->th.resize(3 * mem.size());
+    for (size_t k = 0; k < mem.size(); ++k)
+      for (int q = 0; q < 3; ++q) s->th[3 * k + q] = theta[3 * (size_t)mem[k] + q];
+    if ((rc = batch_launch(s->cls[launched], s->th.data())) != EGS_OK) break;
+  }
+  bool failures = false;
+  for (size_t c = 0; c < launched; ++c) {
+    const auto& mem = s->members[c];
+    s->ll.resize(mem.size());
+    s->st.assign(mem.size(), 0);
+    const int r = batch_collect(s->cls[c], s->ll.data(), s->st.data());
+    if (r == EGS_ERR_STATE) failures = true;
+    else if (r != EGS_OK && rc == EGS_OK) rc = r;
+    for (size_t k = 0; k < mem.size(); ++k) {
+      loglik[mem[k]] = s->ll[k];
+      if (status) status[mem[k]] = s->st[k];
+    }
+  }
+  if (rc != EGS_OK) return rc;
+  return failures ? EGS_ERR_STATE : EGS_OK;
+}
+
+int egs_batch_set_info(const egs_batch_set* s, int* nclass, int* upper_n, int* ts, long long* bytes) {
+  if (!s) return EGS_ERR_INVALID;
+  if (nclass) *nclass = (int)s->cls.size();
+  long long total = 0;
+  for (size_t c = 0; c < s->cls.size(); ++c) {
+    if (upper_n) upper_n[c] = s->upper[c];
+    if (ts) ts[c] = s->ts[c];
+    total += s->cls[c]->bytes;
+  }
+  if (bytes) *bytes = total;
+  return EGS_OK;
+}
+
+int egs_batch_set_autotune(int B, const int* n, const double* x, const double* y, const double* z,
+                           const double* theta, const int* candidates, int ncand, int max_classes, int* nclass,
+                           int* upper_n, int* dts, double* best_ms) {
+  if (B <= 0 || !n || !x || !y || !z || !theta || !candidates || ncand <= 0 || max_classes <= 0 ||
+      max_classes > 16 || !nclass || !upper_n || !dts)
+    return EGS_ERR_INVALID;
+  std::vector<long long> off(B + 1, 0);
+  for (int i = 0; i < B; ++i) off[i + 1] = off[i] + n[i];
+  double best = 1e300;
+  std::vector<double> ll(B);
+  for (int ncl = 1; ncl <= max_classes; ++ncl) {
+    const std::vector<int> upper = cost_boundaries(std::vector<int>(n, n + B), ncl);
+    if ((int)upper.size() < ncl) break;  // fewer distinct sizes than classes
+    // each class's tile size, timed on the class alone
+    std::vector<int> ts(upper.size());
+    bool ok = true;
+    for (size_t c = 0; c < upper.size() && ok; ++c) {
+      const int lo = c > 0 ? upper[c - 1] : 0;
+      std::vector<int> nn;
+      std::vector<double> cx, cy, cz, ct;
+      for (int i = 0; i < B; ++i) {
+        if (n[i] <= lo || n[i] > upper[c]) continue;
+        nn.push_back(n[i]);
+        cx.insert(cx.end(), x + off[i], x + off[i + 1]);
+        cy.insert(cy.end(), y + off[i], y + off[i + 1]);
+        cz.insert(cz.end(), z + off[i], z + off[i + 1]);
+        ct.insert(ct.end(), theta + 3 * (size_t)i, theta + 3 * (size_t)i + 3);
+      }
+      ok = egs_batch_autotune((int)nn.size(), nn.data(), cx.data(), cy.data(), cz.data(), ct.data(), candidates,
+                              ncand, &ts[c], nullptr) == EGS_OK;
+    }
+    if (!ok) continue;
+    // the whole set, classes overlapping: one direct evaluation, one capture, one timed replay
+    egs_batch_set* s = nullptr;
+    if (egs_batch_set_create(&s, B, n, x, y, z, (int)upper.size(), upper.data(), ts.data()) != EGS_OK) continue;
+    egs_batch_set_eval(s, theta, ll.data(), nullptr);
+    egs_batch_set_eval(s, theta, ll.data(), nullptr);
+    const auto t0 = std::chrono::steady_clock::now();
+    const int rc = egs_batch_set_eval(s, theta, ll.data(), nullptr);
+    const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    egs_batch_set_destroy(s);
+    if ((rc == EGS_OK || rc == EGS_ERR_STATE) && ms < best) {
+      best = ms;
+      *nclass = (int)upper.size();
+      for (size_t c = 0; c < upper.size(); ++c) {
+        upper_n[c] = upper[c];
+        dts[c] = ts[c];
+      }
+    }
+  }
+  if (best >= 1e300) return EGS_ERR_STATE;
   if (best_ms) *best_ms = best;
   return EGS_OK;
 }

@@ -313,6 +313,30 @@ EGS_API int egs_batch_autotune(int B, const int* n, const double* x, const doubl
                                const double* theta, const int* candidates, int ncand, int* best_ts,
                                double* best_ms);
 
+/* Size classes of a batch (no counterpart in the reference, which evaluates
+ * one problem per process).  The problems are cut by N into nclass classes --
+ * class c holds upper_n[c-1] < n <= upper_n[c] (upper_n ascending, the last at
+ * least the largest n) -- each an egs_batch with its own tile size dts[c];
+ * egs_batch_set_eval launches every class on its own stream before waiting for
+ * any, so the classes' work overlaps on the device.  Arguments and results are
+ * in the caller's problem order, as for egs_batch_eval. */
+typedef struct egs_batch_set egs_batch_set;
+EGS_API int egs_batch_set_create(egs_batch_set** out, int B, const int* n, const double* x, const double* y,
+                                 const double* z, int nclass, const int* upper_n, const int* dts);
+EGS_API int egs_batch_set_destroy(egs_batch_set* s);
+EGS_API int egs_batch_set_eval(egs_batch_set* s, const double* theta, double* loglik, int* status);
+/* Classes actually formed (empty ones are dropped), their bounds and tile sizes
+ * (arrays of at least nclass entries), device bytes held. */
+EGS_API int egs_batch_set_info(const egs_batch_set* s, int* nclass, int* upper_n, int* ts, long long* bytes);
+/* The schedule for a batch: for 1 .. max_classes classes (bounds at equal shares
+ * of the n^3 cost), each class's tile size from the candidates by timing the
+ * class alone, then one timed replay of the whole set with the classes
+ * overlapping; returns the fastest (nclass, upper_n[], dts[]) and its host-timed
+ * milliseconds per evaluation. */
+EGS_API int egs_batch_set_autotune(int B, const int* n, const double* x, const double* y, const double* z,
+                                   const double* theta, const int* candidates, int ncand, int max_classes,
+                                   int* nclass, int* upper_n, int* dts, double* best_ms);
+
 /* ---- mixed-precision building block --------------------------------------- */
 
 /* No counterpart in the reference.  One step k of the off-band trailing update

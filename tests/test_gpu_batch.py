@@ -163,3 +163,38 @@ def test_batch_of_64_uneven_problems_matches_the_single_problem_path():
         assert abs(ll[i] - ref) <= SAME_TS_RTOL * abs(ref), (i, n, ll[i], ref)
         compared += 1
     assert compared >= B // 2
+
+
+def test_size_classes_match_the_single_problem_path_and_autotune():
+    # Two size classes with their own tiles, launched together: each problem's
+    # result equals its single-problem evaluation at the class's tile size.
+    rng = np.random.default_rng(3)
+    B = 40
+    sizes = np.rint(np.exp(rng.uniform(np.log(200), np.log(1500), B))).astype(int)
+    th = np.column_stack([rng.uniform(0.5, 2.0, B), rng.uniform(0.02, 0.12, B), rng.uniform(0.3, 1.2, B)])
+    xs, ys, zs = [], [], []
+    for i, n in enumerate(sizes):
+        x, y = egs.generate_locations(int(n), 100 + i)
+        xs.append(x)
+        ys.append(y)
+        zs.append(egs.dlarnv_normal(100 + i, int(n)))
+    upper = [600, int(sizes.max())]
+    tiles = [128, 256]
+    s = egs.BatchSet(sizes, *concat(xs, ys, zs), upper_n=upper, dts=tiles)
+    info = s.info()
+    assert info["classes"] == 2 and info["ts"] == tiles
+    ll, st = s.eval(th)
+    ll2, st2 = s.eval(th)  # captured graphs
+    ll3, _ = s.eval(th)    # replays
+    assert np.array_equal(ll, ll2) and np.array_equal(ll, ll3) and np.all(st == 0)
+    s.close()
+    for i, n in enumerate(sizes):
+        ts = tiles[0] if n <= upper[0] else tiles[1]
+        p = egs.Problem(int(n), ts)
+        p.set_locations(xs[i], ys[i])
+        p.set_observations(zs[i])
+        ref = p.mle_eval(th[i])[0]
+        p.close()
+        assert abs(ll[i] - ref) <= SAME_TS_RTOL * abs(ref), (i, n, ll[i], ref)
+    up, ts, ms = egs.batch_set_autotune(sizes, *concat(xs, ys, zs), theta=th, candidates=(128, 256), max_classes=2)
+    assert 1 <= len(up) <= 2 and up[-1] == int(sizes.max()) and all(t in (128, 256) for t in ts) and ms > 0
