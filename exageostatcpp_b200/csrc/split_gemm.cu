@@ -73,7 +73,7 @@ constexpr int B_BYTES = (BN / 2) * BK * 2;         // 16 KB: this CTA's half of 
 constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
 constexpr int EPI_WARPS = 8;                       // two per TMEM lane quarter
 constexpr int THREADS = 64 + 32 * EPI_WARPS;       // producer, MMA issuer, epilogue
-constexpr int WCOLS = BN / (EPI_WARPS / 4);        // accumulator columns per epilogue thread
+constexpr int HALF_COLS = BN / 2;                  // accumulator columns per epilogue thread
 constexpr int PF_AHEAD = 6;                        // stages before a tile's end at which C is prefetched
 // Epilogue staging for the TMA reduce-add of C: per epilogue warp two buffers of
 // 32 rows x RED_COLS columns (column-major, one 128-byte row segment per column).
@@ -400,28 +400,15 @@ split_gemm_kernel(const __grid_constant__ CUtensorMap tm_hi, const __grid_consta
       if (!ok) bail = 1;
     }
   } else {
-    // epilogue warps 2..: TMEM lane quarter = warp % 4, column block by warp group
-    const int quarter = warp & 3, cgroup = (warp - 2) >> 2;
-    const uint32_t tl = tmem_base + ((uint32_t)(quarter * 32) << 16) + cgroup * WCOLS;
+    // epilogue warps 2..9: TMEM lane quarter = warp % 4, column half by warp group
+    const int quarter = warp & 3, half = (warp - 2) >> 2;
+    const uint32_t tl = tmem_base + ((uint32_t)(quarter * 32) << 16) + half * HALF_COLS;
     uint32_t it = 0, red_count = 0;
     bool ok = true;
     for (long long L = pair; L < P.total && ok; L += npairs) {
-      // the tile's coordinates and power-of-two scales, loaded before the K
-      // loop so that their latency hides behind it: lane l holds the row scale
-      // of row r0 + l and the column scales of columns c0 + 32 q + l
-      float inv_r, inv_c[WCOLS / 32];
-      {
-        int i, j, mb, nb;
-        decode_item(P, L, i, j, mb, nb);
-        const int r0 = mb * PM + (int)rank * BM + quarter * 32;
-        const int c0 = nb * BN + cgroup * WCOLS;
-        inv_r = P.inv_scale[(long long)i * P.ts + r0 + lane];
+      float acc[HALF_COLS];  // zero plus the first stage is that stage's value
 #pragma unroll
-        for (int q = 0; q < WCOLS / 32; ++q) inv_c[q] = P.inv_scale[(long long)j * P.ts + c0 + q * 32 + lane];
-      }
-      float acc[WCOLS];  // zero plus the first stage is that stage's value
-#pragma unroll
-      for (int c = 0; c < WCOLS; ++c) acc[c] = 0.f;
+      for (int c = 0; c < HALF_COLS; ++c) acc[c] = 0.f;
       for (int kt = 0; kt < ksteps; ++kt, ++it) {
         const uint32_t ab = it & 1;
         // one lane waits, the warp follows it uniformly (tcgen05.ld needs the whole warp)
@@ -434,7 +421,7 @@ split_gemm_kernel(const __grid_constant__ CUtensorMap tm_hi, const __grid_consta
         }
         tc_fence_after();
 #pragma unroll
-        for (int g = 0; g < WCOLS / 16; ++g) {
+        for (int g = 0; g < HALF_COLS / 16; ++g) {
           float v[16];
           tmem_ld16(tl + ab * BN + g * 16, v);
 #pragma unroll
@@ -458,10 +445,12 @@ split_gemm_kernel(const __grid_constant__ CUtensorMap tm_hi, const __grid_consta
       const int mm = P.nt - P.band - 1;
       const long long slot = tile_slot(i - P.band - 1, j, mm);
       const int r0 = mb * PM + (int)rank * BM + quarter * 32;
-      const int c0 = nb * BN + cgroup * WCOLS;
+      const int c0 = nb * BN + half * HALF_COLS;
+      const float inv_r = P.inv_scale[(long long)i * P.ts + r0 + lane];
+      const float* inv_c = P.inv_scale + (long long)j * P.ts + c0;
       float* stage_w = staging + (warp - 2) * 2 * (RED_BYTES / 4);
 #pragma unroll
-      for (int g = 0; g < WCOLS / RED_COLS; ++g, ++red_count) {
+      for (int g = 0; g < HALF_COLS / RED_COLS; ++g, ++red_count) {
         float* buf = stage_w + (red_count & 1) * (RED_BYTES / 4);
         if (red_count >= 2) {
           // the reduce issued two groups ago has finished reading this buffer
@@ -469,11 +458,8 @@ split_gemm_kernel(const __grid_constant__ CUtensorMap tm_hi, const __grid_consta
           __syncwarp();
         }
 #pragma unroll
-        for (int c = 0; c < RED_COLS; ++c) {
-          const int col = g * RED_COLS + c;
-          const float sc = __shfl_sync(0xffffffffu, inv_c[col / 32], col % 32);
-          buf[c * 32 + lane] = -(acc[col] * inv_r) * sc;
-        }
+        for (int c = 0; c < RED_COLS; ++c)
+          buf[c * 32 + lane] = -(acc[g * RED_COLS + c] * inv_r) * __ldg(inv_c + g * RED_COLS + c);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncwarp();
         if (lane == 0) {
