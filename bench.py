@@ -62,7 +62,7 @@ C3_FIT_MAXEVAL, C3_FIT_RHOBEG, C3_MISS = 15, 0.02, 1000
 # The batched configuration: 2,048 independent problems, N_i log-uniform in
 # [256, 4096], theta_i drawn per problem, one evaluation of all per optimiser step.
 C4_B, C4_NMIN, C4_NMAX, C4_SEED = 2048, 256, 4096, 12345
-C4_TILES = (128, 192, 256, 320)
+C4_TILES = (128, 192, 256, 320, 384, 512)
 # The serving configuration in the default run: two arrival rates, the
 # reference's fit budget for fit requests.
 SERVE_SECONDS, SERVE_FIT_EVALS = 30.0, 100
@@ -641,6 +641,10 @@ def main():
                     help="with --profile-eval: evaluate this many points of a jittered grid with DLARNV "
                          "observations instead of the full workload (small ncu captures)")
     ap.add_argument("--profile-plain", action="store_true", help="with --profile-eval: the plain FP64 path")
+    ap.add_argument("--profile-batched", type=int, default=0,
+                    help="the first B problems of the batched configuration in one size class at --profile-tile: "
+                         "six evaluations (direct launches, graph capture, replays) for ncu launch lists")
+    ap.add_argument("--profile-tile", type=int, default=320)
     ap.add_argument("--workload", default="eval", choices=["eval", "serving"])
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[0.25, 0.5, 1.0])
     ap.add_argument("--serve-seconds", type=float, default=30.0)
@@ -674,6 +678,19 @@ def main():
         bus = f"{props.pci_domain_id:08X}:{props.pci_bus_id:02X}:{props.pci_device_id:02X}.0"
     except AttributeError:
         pass
+
+    if args.profile_batched:
+        sizes, x, y, z, theta = c4_problems(egs)
+        nb = int(min(args.profile_batched, C4_B))
+        npts = int(sizes[:nb].sum())
+        b = egs.Batch(sizes[:nb], x[:npts], y[:npts], z[:npts], dts=args.profile_tile)
+        t0 = time.perf_counter()
+        for _ in range(6):
+            b.eval(theta[:nb])
+        print(json.dumps({"problems": nb, "tile": args.profile_tile, "ms_per_step_incl_capture":
+                          1e3 * (time.perf_counter() - t0) / 6, "info": b.info()}), flush=True)
+        b.close()
+        return 0
 
     if args.profile_eval:
         if args.profile_n:
@@ -760,12 +777,12 @@ def main():
 
     # --- rooflines of the update kernels (CUDA events around every launch) ---------------
     # DRAM bytes (read + write) per algorithmic flop of each kernel, from one ncu
-    # capture of each at N = 16,384: the split kernel moved 792,716,032 B for 78
+    # capture of each at N = 16,384: the split kernel moved 807,166,464 B for 78
     # target tiles of 2 * 1024^3 flops; the Ozaki kernel 644,593,920 B for the band
     # update of step 0, 7.410e10 FP64-equivalent flops.
     # Both kernels' traffic grows with their target tiles, so a launch's traffic
     # is this ratio times its flops.
-    split_bytes_per_flop = 792716032.0 / (78 * 2.0 * 1024 ** 3)
+    split_bytes_per_flop = 807166464.0 / (78 * 2.0 * 1024 ** 3)
     ozaki_bytes_per_flop = 644593920.0 / 7.410e10
     traffic_note = ("DRAM read + write bytes per flop from one ncu capture at N=16384, times this launch's "
                     "algorithmic flops")
