@@ -21,22 +21,27 @@ __device__ __forceinline__ double block_sum_256(double v, double* red) {
   return out;
 }
 
-// Cholesky of the 64x64 block at T (ld ts).  Every thread of the block (NTHR,
-// whole warps) takes part in moving the block between global and shared memory,
-// with all loads issued before any is used.  Up to eight warps factor it; lane
-// l of each owns rows l and l + 32, and warp w the columns c with c % CW == w.
-// At step j every warp scales column j with the reciprocal pivot and applies
-// the rank-1 update to its columns c > j; the owner of column j + 1 updates
-// that column first and computes the next pivot's square root and reciprocal
-// before the step's barrier, so no warp waits on them after it.  Warp 0 stores
-// the scaled column j after the barrier (no warp reads it again).  info
-// records the 1-based global column (gcol0 + j + 1) of the first pivot that is
-// not positive (or NaN).
+// Cholesky of the 64x64 block at T (ld ts), blocked by 16 columns.  Every
+// thread of the block (NTHR, whole warps, at least two) takes part in moving
+// the block between global and shared memory, with all loads issued before any
+// is used.  For each 16-column block: (1) warp 0 factors the 16 x 16 diagonal
+// block in registers (lane l holds row l; the pivot and the scaled column are
+// exchanged with shuffles, so the 16 dependent pivot steps need no block-wide
+// barrier); (2) one thread per row below it solves that row against the block
+// (x_j = (a_j - sum_{q<j} x_q l_jq) / l_jj); (3) all threads update the rest
+// of the 64 x 64 block with the 16 new columns.  Every element receives its
+// multiply-adds in the same order (columns ascending) and every column the
+// same scaling (by the correctly rounded reciprocal of the correctly rounded
+// square root) as in the column-by-column right-looking factorisation, so the
+// result is the same bit for bit; only the barriers are fewer (3 per 16
+// columns instead of 2 per column).  info records the 1-based global column
+// (gcol0 + j + 1) of the first pivot that is not positive (or NaN).
 template <int NTHR>
 __device__ __forceinline__ void potrf64_body(double* __restrict__ T, int ts, int gcol0, int* __restrict__ info) {
-  static_assert(NTHR % 32 == 0 && NTHR >= 32 && NTHR <= 1024, "whole warps");
+  static_assert(NTHR % 32 == 0 && NTHR >= 64 && NTHR <= 1024, "whole warps, at least two");
+  constexpr int kSB = 16;  // sub-block width
   __shared__ double S[kNB][kNB + 1];
-  __shared__ double piv[kNB], pinv[kNB];  // L_jj and 1 / L_jj
+  __shared__ double pinv[kNB];  // 1 / L_jj
   constexpr int per = kNB * kNB / NTHR;
   {
     // column-major block: element e = c * 64 + r; all loads issued first
@@ -54,53 +59,72 @@ __device__ __forceinline__ void potrf64_body(double* __restrict__ T, int ts, int
     }
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    const double d = S[0][0];
-    if (!(d > 0.0)) atomicCAS(info, 0, gcol0 + 1);
-    const double ljj = sqrt(d);
-    piv[0] = ljj;
-    pinv[0] = __drcp_rn(ljj);  // correctly rounded, as 1.0 / ljj
-  }
-  __syncthreads();
-  constexpr int CW = NTHR / 32 < 8 ? NTHR / 32 : 8;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int r0 = lane, r1 = lane + 32;
-  for (int j = 0; j < kNB; ++j) {
-    double l0 = 0.0, l1 = 0.0;
-    if (warp < CW) {
-      const double inv = pinv[j];
-      l0 = (r0 > j) ? S[r0][j] * inv : 0.0;
-      l1 = (r1 > j) ? S[r1][j] * inv : 0.0;
-      // first column of this warp after j
-      int c1 = j + 1 + ((warp - (j + 1)) % CW + CW) % CW;
-      if (c1 == j + 1 && c1 < kNB) {
-        const double lcj = S[c1][j] * inv;
-        if (r0 >= c1) S[r0][c1] = fma(-l0, lcj, S[r0][c1]);
-        if (r1 >= c1) S[r1][c1] = fma(-l1, lcj, S[r1][c1]);
-        __syncwarp();
-        if (lane == 0) {
-          const double d = S[c1][c1];
-          if (!(d > 0.0)) atomicCAS(info, 0, gcol0 + c1 + 1);
-          const double ljj = sqrt(d);
-          piv[c1] = ljj;
-          pinv[c1] = __drcp_rn(ljj);
+#pragma unroll 1
+  for (int c0 = 0; c0 < kNB; c0 += kSB) {
+    // (1) the diagonal sub-block, one warp, in registers
+    if (warp == 0) {
+      const int l = lane < kSB ? lane : kSB - 1;  // lanes 16..31 shadow lane 15 and write nothing
+      double a[kSB];
+#pragma unroll
+      for (int q = 0; q < kSB; ++q) a[q] = (q <= l) ? S[c0 + l][c0 + q] : 0.0;
+#pragma unroll
+      for (int j = 0; j < kSB; ++j) {
+        const double d = __shfl_sync(0xffffffffu, a[j], j);
+        if (lane == j && !(d > 0.0)) atomicCAS(info, 0, gcol0 + c0 + j + 1);
+        const double ljj = sqrt(d);
+        const double inv = __drcp_rn(ljj);  // correctly rounded, as 1.0 / ljj
+        if (l > j) a[j] *= inv;
+        if (l == j) a[j] = ljj;
+        if (lane == j) pinv[c0 + j] = inv;
+#pragma unroll
+        for (int c = 0; c < kSB; ++c) {
+          if (c > j) {
+            const double lcj = __shfl_sync(0xffffffffu, a[j], c);
+            if (l >= c) a[c] = fma(-a[j], lcj, a[c]);
+          }
         }
-        c1 += CW;
       }
-#pragma unroll 4
-      for (int c = c1; c < kNB; c += CW) {
-        const double lcj = S[c][j] * inv;
-        if (r0 >= c) S[r0][c] = fma(-l0, lcj, S[r0][c]);
-        if (r1 >= c) S[r1][c] = fma(-l1, lcj, S[r1][c]);
+      if (lane < kSB) {
+#pragma unroll
+        for (int q = 0; q < kSB; ++q)
+          if (q <= lane) S[c0 + lane][c0 + q] = a[q];
       }
     }
     __syncthreads();
-    if (warp == 0) {
-      if (r0 > j) S[r0][j] = l0;
-      if (r1 > j) S[r1][j] = l1;
-      if (r0 == j) S[r0][j] = piv[j];
-      if (r1 == j) S[r1][j] = piv[j];
+    const int rest = kNB - c0 - kSB;  // rows (and columns) after this sub-block
+    if (rest == 0) break;
+    // (2) the rows below the sub-block, one thread per row
+    if ((int)threadIdx.x < rest) {
+      const int r = c0 + kSB + threadIdx.x;
+      double x[kSB];
+#pragma unroll
+      for (int j = 0; j < kSB; ++j) {
+        double v = S[r][c0 + j];
+#pragma unroll
+        for (int q = 0; q < kSB; ++q)
+          if (q < j) v = fma(-x[q], S[c0 + j][c0 + q], v);
+        x[j] = v * pinv[c0 + j];
+      }
+#pragma unroll
+      for (int j = 0; j < kSB; ++j) S[r][c0 + j] = x[j];
     }
+    __syncthreads();
+    // (3) the rest of the block: S(r, c) -= sum_q L(r, q) L(c, q), c0+16 <= c <= r
+    const int cnt = rest * (rest + 1) / 2;
+    for (int e = threadIdx.x; e < cnt; e += NTHR) {
+      // e -> (r, c) with c <= r in the lower triangle of the rest, rows first
+      int rr = (int)((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
+      while (rr * (rr + 1) / 2 > e) --rr;
+      while ((rr + 1) * (rr + 2) / 2 <= e) ++rr;
+      const int cc = e - rr * (rr + 1) / 2;
+      const int r = c0 + kSB + rr, c = c0 + kSB + cc;
+      double v = S[r][c];
+#pragma unroll
+      for (int q = 0; q < kSB; ++q) v = fma(-S[r][c0 + q], S[c][c0 + q], v);
+      S[r][c] = v;
+    }
+    __syncthreads();
   }
   __syncthreads();
 #pragma unroll
