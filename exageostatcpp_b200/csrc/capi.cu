@@ -55,6 +55,9 @@ struct egs_problem {
   bool own_stream = false;
   bool have_locations = false;
   bool have_observations = false;
+  // Mixed precision only: the order in which the device holds the points
+  // (perm[d] = caller index of device point d), empty when it is the caller's.
+  std::vector<int> perm;
   int band = 0;  // >= 1: diagonal super-tile approximation with this tile band
   // Replay of a whole evaluation: captured at the second evaluation, relaunched after.
   cudaGraph_t graph = nullptr;
@@ -1149,9 +1152,112 @@ int egs_problem_set_stream(egs_problem* p, void* cuda_stream) {
   return EGS_OK;
 }
 
+namespace {
+
+uint64_t spread16(uint64_t v) {
+  v &= 0xffffull;
+  v = (v ^ (v << 24)) & 0x000000ff000000ffull;
+  v = (v ^ (v << 12)) & 0x000f000f000f000full;
+  v = (v ^ (v << 6)) & 0x0303030303030303ull;
+  v = (v ^ (v << 3)) & 0x1111111111111111ull;
+  return v;
+}
+
+// Locality order of n points for the mixed form: the FP64 band of the mixed
+// factorisation holds the tiles next to the diagonal, which carry the large
+// covariances only when nearby points are adjacent in the matrix.  Points are
+// ordered by their Morton (Z-order) code at 16 bits per axis -- the key of the
+// reference's SortLocations (LocationGenerator.cpp:91-123) -- on the unit
+// square when every coordinate lies in [0, 1], else on the bounding box; ties
+// keep the caller's order.  Returns an empty vector when the caller's order is
+// already sorted (the reference generator's output is), so such problems run
+// on exactly the caller's layout.
+std::vector<int> locality_order(int n, const double* x, const double* y) {
+  double x0 = x[0], x1 = x[0], y0 = y[0], y1 = y[0];
+  for (int i = 1; i < n; ++i) {
+    x0 = std::min(x0, x[i]);
+    x1 = std::max(x1, x[i]);
+    y0 = std::min(y0, y[i]);
+    y1 = std::max(y1, y[i]);
+  }
+  const bool unit = x0 >= 0.0 && y0 >= 0.0 && x1 <= 1.0 && y1 <= 1.0;
+  const double ox = unit ? 0.0 : x0, oy = unit ? 0.0 : y0;
+  const double sx = unit ? 1.0 : (x1 > x0 ? x1 - x0 : 1.0), sy = unit ? 1.0 : (y1 > y0 ? y1 - y0 : 1.0);
+  std::vector<uint64_t> key(n);
+  bool sorted = true;
+  for (int i = 0; i < n; ++i) {
+    const uint16_t qx = (uint16_t)((x[i] - ox) / sx * 65535.0 + 0.5);
+    const uint16_t qy = (uint16_t)((y[i] - oy) / sy * 65535.0 + 0.5);
+    key[i] = (spread16(qy) << 1) + spread16(qx);
+    if (i > 0 && key[i] < key[i - 1]) sorted = false;
+  }
+  if (sorted) return {};
+  std::vector<int> perm(n);
+  for (int i = 0; i < n; ++i) perm[i] = i;
+  std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return key[a] < key[b]; });
+  return perm;
+}
+
+// Caller-order host vector -> device order.
+std::vector<double> to_device_order(const egs_problem* p, const double* v) {
+  std::vector<double> out(p->n);
+  for (int d = 0; d < p->n; ++d) out[d] = v[p->perm[d]];
+  return out;
+}
+
+// A caller's vector of n doubles in host memory (copied from the device when
+// kind says it lives there).
+int host_copy(const egs_problem* p, const double* v, cudaMemcpyKind kind, std::vector<double>* out) {
+  out->resize(p->n);
+  if (kind == cudaMemcpyHostToDevice) {
+    std::copy(v, v + p->n, out->begin());
+    return EGS_OK;
+  }
+  EGS_CUDA_TRY(cudaMemcpyAsync(out->data(), v, p->n * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+  EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  return EGS_OK;
+}
+
+}  // namespace
+
 static int set_locs(egs_problem* p, const double* x, const double* y, cudaMemcpyKind kind) {
   if (!p || !x || !y) return EGS_ERR_INVALID;
   if (p->precision == kPrecisionBroken) return EGS_ERR_STATE;
+  if (p->precision == EGS_PRECISION_MIXED) {
+    std::vector<double> hx, hy, hz;
+    const double *hxp = x, *hyp = y;
+    if (kind != cudaMemcpyHostToDevice) {
+      int rc;
+      if ((rc = host_copy(p, x, kind, &hx)) != EGS_OK || (rc = host_copy(p, y, kind, &hy)) != EGS_OK) return rc;
+      hxp = hx.data();
+      hyp = hy.data();
+    }
+    if (p->have_observations) {
+      // observations already uploaded in the previous order: back to the caller's
+      std::vector<double> dz(p->n);
+      EGS_CUDA_TRY(cudaMemcpyAsync(dz.data(), p->zcpy, p->n * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+      EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
+      hz.resize(p->n);
+      for (int d = 0; d < p->n; ++d) hz[p->perm.empty() ? d : p->perm[d]] = dz[d];
+    }
+    p->perm = locality_order(p->n, hxp, hyp);
+    if (!p->perm.empty()) {
+      hx = to_device_order(p, hxp);
+      hy = to_device_order(p, hyp);
+      hxp = hx.data();
+      hyp = hy.data();
+    }
+    EGS_CUDA_TRY(cudaMemcpyAsync(p->x, hxp, p->n * sizeof(double), cudaMemcpyHostToDevice, p->stream));
+    EGS_CUDA_TRY(cudaMemcpyAsync(p->y, hyp, p->n * sizeof(double), cudaMemcpyHostToDevice, p->stream));
+    if (p->have_observations) {
+      if (!p->perm.empty()) hz = to_device_order(p, hz.data());
+      EGS_CUDA_TRY(cudaMemcpyAsync(p->zcpy, hz.data(), p->n * sizeof(double), cudaMemcpyHostToDevice, p->stream));
+      EGS_CUDA_TRY(cudaMemcpyAsync(p->z, p->zcpy, p->np * sizeof(double), cudaMemcpyDeviceToDevice, p->stream));
+    }
+    EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
+    p->have_locations = true;
+    return EGS_OK;
+  }
   EGS_CUDA_TRY(cudaMemcpyAsync(p->x, x, p->n * sizeof(double), kind, p->stream));
   EGS_CUDA_TRY(cudaMemcpyAsync(p->y, y, p->n * sizeof(double), kind, p->stream));
   EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
@@ -1169,6 +1275,18 @@ int egs_problem_set_locations_device(egs_problem* p, const double* x, const doub
 static int set_obs(egs_problem* p, const double* z, cudaMemcpyKind kind) {
   if (!p || !z) return EGS_ERR_INVALID;
   if (p->precision == kPrecisionBroken) return EGS_ERR_STATE;
+  if (!p->perm.empty()) {
+    // a mixed problem holding its points in locality order
+    std::vector<double> hz;
+    int rc = host_copy(p, z, kind, &hz);
+    if (rc != EGS_OK) return rc;
+    hz = to_device_order(p, hz.data());
+    EGS_CUDA_TRY(cudaMemcpyAsync(p->zcpy, hz.data(), p->n * sizeof(double), cudaMemcpyHostToDevice, p->stream));
+    EGS_CUDA_TRY(cudaMemcpyAsync(p->z, p->zcpy, p->np * sizeof(double), cudaMemcpyDeviceToDevice, p->stream));
+    EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
+    p->have_observations = true;
+    return EGS_OK;
+  }
   EGS_CUDA_TRY(cudaMemcpyAsync(p->zcpy, z, p->n * sizeof(double), kind, p->stream));
   EGS_CUDA_TRY(cudaMemcpyAsync(p->z, p->zcpy, p->np * sizeof(double), cudaMemcpyDeviceToDevice, p->stream));
   EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
@@ -1247,6 +1365,13 @@ int egs_get_tile(egs_problem* p, int i, int j, double* host_out) {
 
 int egs_get_observations(egs_problem* p, double* host_z) {
   if (!p || !host_z) return EGS_ERR_INVALID;
+  if (!p->perm.empty()) {
+    std::vector<double> dz(p->n);
+    EGS_CUDA_TRY(cudaMemcpyAsync(dz.data(), p->z, p->n * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+    EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
+    for (int d = 0; d < p->n; ++d) host_z[p->perm[d]] = dz[d];
+    return EGS_OK;
+  }
   EGS_CUDA_TRY(cudaMemcpyAsync(host_z, p->z, p->n * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
   EGS_CUDA_TRY(cudaStreamSynchronize(p->stream));
   return EGS_OK;

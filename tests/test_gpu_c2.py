@@ -55,15 +55,17 @@ def test_n40000_loglik_and_kriging_match_the_oracle(theta):
     assert mspe == pytest.approx(rmspe, rel=PREDICT_RTOL)
 
 
-MIXED_RTOL = 1e-6        # the mixed form's contract for exponential to moderately smooth kernels
-MIXED_SMOOTH_RTOL = 5e-5  # smooth, long-range kernels (nu >= 1.3), as bounded at small N
+MIXED_RTOL = 1e-6  # the mixed form's log-likelihood contract
 
 
 @pytest.mark.parametrize("theta", [(1.0, 0.05, 0.8), (1.0, 0.03, 1.5)])
 def test_n40000_mixed_precision_against_the_oracle(theta):
     # The mixed form (FP64 diagonal + band of 2 tiles, FP32 off-band tiles with
     # split-FP16 tensor-core updates, one refinement step) on the same data,
-    # against the FP64 oracle at N = 40,000.
+    # against the FP64 oracle at N = 40,000.  The observed points come out of
+    # the reference's split in shuffled order; the problem re-sorts them into
+    # locality order (measured on a B200: 6.3e-8 for nu = 0.8 and 5.4e-7 for
+    # nu = 1.5; 1.2e-5 and 7.9e-5 when the shuffled order was kept).
     x, y = egs.generate_locations(41000, 0)
     gen = egs.Problem(41000, 960)
     gen.set_locations(x, y)
@@ -76,13 +78,10 @@ def test_n40000_mixed_precision_against_the_oracle(theta):
     p.set_observations(zo)
     try:
         ll, logdet, dot = p.mle_eval(theta)
-    except egs.NotPositiveDefinite:
+    finally:
         p.close()
-        assert theta[2] >= 1.3, "only a smooth kernel may lose definiteness in FP32 storage"
-        pytest.skip(f"theta={theta}: the FP32 off-band storage is not positive definite (served in FP64)")
-    p.close()
     rll, rlogdet, rdot = C.timed_eval_parts(xo, yo, zo, theta)
     rel = abs(ll - rll) / abs(rll)
     print(f"mixed theta={theta}: loglik rel {rel:.3e}, logdet rel {abs(logdet - rlogdet) / abs(rlogdet):.3e}, "
           f"dot rel {abs(dot - rdot) / abs(rdot):.3e}")
-    assert rel <= (MIXED_RTOL if theta[2] < 1.3 else MIXED_SMOOTH_RTOL)
+    assert rel <= MIXED_RTOL

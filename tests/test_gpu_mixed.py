@@ -118,3 +118,37 @@ def test_lookahead_does_not_change_the_result():
         out.append(p.mle_eval(theta))
         out.append(p.mle_eval(theta))   # captured and replayed as a graph
     assert all(r == out[0] for r in out)
+
+
+def test_mixed_form_is_independent_of_the_callers_point_order():
+    # The likelihood does not depend on the order of the points, but the mixed
+    # form's FP64 band only holds the large covariances when nearby points are
+    # adjacent; the problem therefore keeps its points in locality (Morton) order
+    # whatever order the caller passes.  A shuffled copy of a data set (the
+    # reference's hold-out split shuffles) gives the same log-likelihood and the
+    # same kriging predictions as the sorted one, within the mixed tolerance.
+    n, dts, theta = 3000, 256, (1.0, 0.05, 0.8)
+    x, y, z = O.load_data(n, 7, theta)
+    perm = np.random.default_rng(1).permutation(n)
+    xs, ys, zs = x[perm], y[perm], z[perm]
+    p = mixed_problem(x, y, z, dts, 2)
+    q = mixed_problem(xs, ys, zs, dts, 2)
+    ll_p, ld_p, dot_p = p.mle_eval(theta)
+    ll_q, ld_q, dot_q = q.mle_eval(theta)
+    ref, rlogdet, rdot = O.mle_loglik(x, y, z, theta, return_parts=True)
+    for ll in (ll_p, ll_q):
+        assert abs(ll - ref) <= MIXED_RTOL * abs(ref)
+    assert abs(ll_q - ll_p) <= 1e-9 * abs(ll_p)
+    xm, ym = O.generate_locations(50, O.GlibcRand(9))
+    zm_p, zm_q = p.predict(theta, xm, ym), q.predict(theta, xm, ym)
+    zr, _ = O.predict(x, y, z, xm, ym, theta)
+    assert np.abs(zm_q - zr).max() <= 1e-5 * np.abs(zr).max()
+    assert np.abs(zm_q - zm_p).max() <= 1e-9 * np.abs(zm_p).max()
+    # the observations come back in the caller's order
+    got = np.empty(n)
+    lib = egs.load_library()
+    q.set_observations(zs)
+    assert lib.egs_get_observations(q._h, got.ctypes.data_as(egs._D)) == egs.EGS_OK
+    assert np.array_equal(got, zs)
+    p.close()
+    q.close()
