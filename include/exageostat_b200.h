@@ -122,7 +122,12 @@ EGS_API int egs_problem_create_ex(egs_problem** out, int n, int dts, int precisi
 EGS_API int egs_problem_footprint(int n, int dts, int precision, int band_tiles, long long* bytes);
 
 /* Copy n locations from host memory (Locations<T> SoA x[], y[],
- * src/data-units/Locations.cpp:94-118). */
+ * src/data-units/Locations.cpp:94-118).  A mixed-precision problem keeps its
+ * points in locality (Morton) order: it sorts them here -- keeping the
+ * caller's order when it is already sorted -- and permutes the observations
+ * given to it the same way, so that its FP64 band holds the large covariances;
+ * results do not depend on the caller's order, and egs_get_observations
+ * returns vectors in the caller's order. */
 EGS_API int egs_problem_set_locations(egs_problem* p, const double* x, const double* y);
 /* Same from device memory. */
 EGS_API int egs_problem_set_locations_device(egs_problem* p, const double* x, const double* y);
