@@ -18,7 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libexageostat_b200.so")
 
-SOURCES = ["matern.cu", "potrf.cu", "dgemm_tma.cu", "split_gemm.cu", "ozaki_band.cu", "mixed.cu", "fisher.cu", "capi.cu", "batch.cu", "host_data.cpp", "host_bobyqa.cpp", "host_server.cpp"]
+SOURCES = ["matern.cu", "potrf.cu", "dst.cu", "dgemm_tma.cu", "split_gemm.cu", "ozaki_band.cu", "mixed.cu", "fisher.cu", "capi.cu", "batch.cu", "host_data.cpp", "host_bobyqa.cpp", "host_server.cpp"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

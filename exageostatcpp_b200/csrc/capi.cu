@@ -137,7 +137,6 @@ struct egs_problem {
   alignas(64) unsigned char tm_hi[128];
   alignas(64) unsigned char tm_lo[128];
   alignas(64) unsigned char tm_c[128];
-  alignas(64) unsigned char tm_cr[128];
 };
 
 namespace {
@@ -408,11 +407,21 @@ int enqueue_potrf(egs_problem* p, int steps = -1) {
 // with m < k + band are solved, and only tiles (m, n) with k < n < k + band,
 // n <= m < n + band are updated; the update reads tile (m, k) whether or not it
 // was solved, and tiles outside the band keep their covariance values.
+// Caller tiles that are not device tiles (dts not a multiple of 64) take the
+// element-level form of the same loop on logical tiles of dts (dst.cu).
 int enqueue_potrf_band(egs_problem* p) {
   const int ts = p->ts, nt = p->nt, n = p->n, band = p->band;
   cudaStream_t st = p->stream;
   int* info = p->flags;
   int* err = p->flags + 1;
+  if (p->dts != ts) {
+    const int sp = span_begin(p, EGS_STAGE_PANEL);
+    const int rc = launch_dst_band(p->tiles, ts, nt, n, p->dts, band, info, st);
+    const int ntl = (n + p->dts - 1) / p->dts;
+    count_launches(p, EGS_STAGE_PANEL, 3LL * ntl);
+    span_end(p, sp, 0.0);
+    return rc;
+  }
   for (int k = 0; k < nt; ++k) {
     const long long skk = tile_slot(k, k, nt);
     int sp = span_begin(p, EGS_STAGE_PANEL);
@@ -556,7 +565,7 @@ static int enqueue_offband_update(egs_problem* p, int k, cudaStream_t st, int ma
   const long long off_targets = split_targets(nt, b, k);
   if (off_targets <= 0) return EGS_OK;
   int sp = span_begin(p, EGS_STAGE_UPDATE_LOW);
-  int rc = launch_split_update(p->tm_hi, p->tm_lo, p->tm_c, p->tm_cr, ts, nt, b, k, p->off_pool, p->inv_scale,
+  int rc = launch_split_update(p->tm_hi, p->tm_lo, p->tm_c, ts, nt, b, k, p->off_pool, p->inv_scale,
                                p->flags + 1, st, max_ctas);
   if (rc != EGS_OK) return rc;
   count_launches(p, EGS_STAGE_UPDATE_LOW, 1);
@@ -873,7 +882,7 @@ int setup_mixed(egs_problem* p, int b) {
   if ((rc = gemm_init_tensor_map(p->tmapW, p->W, ts, nt + 1)) != EGS_OK ||
       (rc = split_tensor_map(p->tm_hi, p->ph, ts, p->np)) != EGS_OK ||
       (rc = split_tensor_map(p->tm_lo, p->pl, ts, p->np)) != EGS_OK ||
-      (rc = split_c_maps(p->tm_c, p->tm_cr, p->off_pool, ts, lower_tiles(m))) != EGS_OK)
+      (rc = split_c_map(p->tm_c, p->off_pool, ts, lower_tiles(m))) != EGS_OK)
     return rc;
   EGS_CUDA_TRY(cudaMemset(p->x, 0, p->np * sizeof(double)));
   EGS_CUDA_TRY(cudaMemset(p->y, 0, p->np * sizeof(double)));
@@ -1078,12 +1087,9 @@ int egs_problem_info(const egs_problem* p, int* n, int* ts, int* nt, long long* 
 int egs_problem_set_band(egs_problem* p, int band) {
   if (!p || band < 0) return EGS_ERR_INVALID;
   if (int rc = reject_mixed(p, "egs_problem_set_band")) return rc;
-  if (band > 0 && p->dts != p->ts) {
-    // The approximation is defined on the caller's tiles; merging them into a
-    // larger device tile would change the result.
-    set_last_error("the band approximation needs a tile size that is a multiple of 64", "egs_problem_set_band");
-    return EGS_ERR_INVALID;
-  }
+  // Caller tiles that are not device tiles keep their own size in the band
+  // factorisation (launch_dst_band), since merging them into a larger device
+  // tile would change which elements the approximation keeps.
   p->band = band;
   return EGS_OK;
 }

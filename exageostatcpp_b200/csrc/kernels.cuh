@@ -37,6 +37,10 @@ void launch_trmv(const double* tiles, int ts, int nt, const double* e, double* p
 void launch_gemv_t_block(const double* a, long long lda, int rows, int cols, const double* w, double* out,
                          cudaStream_t st);
 
+// Band (diagonal super-tile) factorisation on logical tiles of dts elements,
+// element by element inside the lower-tile pool (dst.cu); for dts != ts.
+int launch_dst_band(double* tiles, int ts, int nt, int n, int dts, int band, int* info, cudaStream_t st);
+
 // FP64 tensor-core update C -= A * B^T over global row indices (dgemm_tma.cu).
 // Every operand row is a global row of one problem (tile row g / ts); A and B take
 // their K columns from one tile column starting at a local column offset; C is
@@ -103,7 +107,7 @@ void launch_matern_residual(const double* x, const double* y, const double* z, c
 void launch_finalize_mixed(const double* partial, int nt, const double* z, const double* v, const double* w, int n,
                            double* result, const int* info, cudaStream_t st);
 int split_tensor_map(void* storage, const __half* base, int ts, long long rows);
-int split_c_maps(void* tm_c, void* tm_cr, const float* c_pool, int ts, long long nslots);
+int split_c_map(void* tm_c, const float* c_pool, int ts, long long nslots);
 void launch_panel_split(const double* W, int ts, int t0, int ntiles, int row_tile0, float* inv_scale, __half* Ph,
                         __half* Pl, cudaStream_t st);
 long long split_targets(int nt, int band, int k);
@@ -126,7 +130,7 @@ int launch_ozaki_trsm(const void* tm_s, const int4* targets, int ntargets, long 
                       long long b_row_base, double* w_out, const double* scale, int* err, cudaStream_t st);
 int launch_ozaki_band(const void* tm_s, const int4* targets, int ntargets, long long total, int ts, int band,
                       double* band_pool, const double* scale, int* err, cudaStream_t st);
-int launch_split_update(const void* tm_hi, const void* tm_lo, const void* tm_c, const void* tm_cr, int ts, int nt,
+int launch_split_update(const void* tm_hi, const void* tm_lo, const void* tm_c, int ts, int nt,
                         int band, int k, float* c_pool,
                         const float* inv_scale, int* err, cudaStream_t st, int max_ctas = 0);
 

@@ -47,7 +47,8 @@
 //             (thread = tile row) and one half of the columns, adds every stage
 //             into 128 FP32 registers, releases the stage accumulator to the
 //             leader, and after the last stage applies C -= acc * inv_s_row *
-//             inv_s_col through TMA reduce-adds.
+//             inv_s_col with reductions into L2 (red.global.add), issued
+//             straight from the registers without waiting.
 // The two stage accumulators let the MMAs of stage s+1 overlap the draining of
 // stage s.  Every mbarrier wait is bounded; a timed-out CTA records the error,
 // stops, and still meets its peer at the final cluster barrier and frees its
@@ -75,12 +76,7 @@ constexpr int EPI_WARPS = 8;                       // two per TMEM lane quarter
 constexpr int THREADS = 64 + 32 * EPI_WARPS;       // producer, MMA issuer, epilogue
 constexpr int HALF_COLS = BN / 2;                  // accumulator columns per epilogue thread
 constexpr int PF_AHEAD = 6;                        // stages before a tile's end at which C is prefetched
-// Epilogue staging for the TMA reduce-add of C: per epilogue warp two buffers of
-// 32 rows x RED_COLS columns (column-major, one 128-byte row segment per column).
-constexpr int RED_COLS = 16;
-constexpr int RED_BYTES = 32 * RED_COLS * 4;       // 2 KB
-constexpr int STAGING_BYTES = EPI_WARPS * 2 * RED_BYTES;
-constexpr int SMEM_BYTES = 1024 + STAGES * STAGE_BYTES + STAGING_BYTES + 256;
+constexpr int SMEM_BYTES = 1024 + STAGES * STAGE_BYTES + 256;
 static_assert(SMEM_BYTES <= 232448, "shared memory per CTA");
 constexpr uint32_t TMEM_COLS = 512;
 // Instruction descriptor of kind::f16: D F32 (bits 4-5 = 1), A and B F16 (0),
@@ -207,13 +203,6 @@ __device__ __forceinline__ void tma_load_2d_pair(void* dst, const CUtensorMap* m
       "l"((uint64_t)map), "r"(x), "r"(y), "r"(bar_cluster_addr)
       : "memory");
 }
-// out[box at (x, y)] += smem (FP32 add performed at L2), tracked in this thread's bulk group.
-__device__ __forceinline__ void tma_reduce_add_2d(const CUtensorMap* map, const void* src, int x, int y) {
-  asm volatile("cp.reduce.async.bulk.tensor.2d.global.shared::cta.add.bulk_group [%0, {%2, %3}], [%1];" ::"l"(
-                   (uint64_t)map),
-               "r"(smem_u32(src)), "r"(x), "r"(y)
-               : "memory");
-}
 // L2 prefetch of one box of a tiled tensor (no shared memory, no completion).
 __device__ __forceinline__ void tma_prefetch_l2_2d(const CUtensorMap* map, int x, int y) {
   asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];" ::"l"((uint64_t)map), "r"(x),
@@ -250,6 +239,10 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+__device__ __forceinline__ void red_add_f32(float* addr, float v) {
+  asm volatile("red.global.add.f32 [%0], %1;" ::"l"(addr), "f"(v) : "memory");
+}
+
 // Target tile of work item L at step k: targets are enumerated column by column
 // (j = k+1, ...; i = j+band+1 .. nt-1), each split into (ts/PM) x (ts/BN) pair
 // tiles with the row block fastest.
@@ -280,13 +273,12 @@ __device__ __forceinline__ void decode_item(const SplitStep& P, long long L, int
 
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(sg::THREADS, 1)
 split_gemm_kernel(const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo,
-                  const __grid_constant__ CUtensorMap tm_c, const __grid_constant__ CUtensorMap tm_cr,
+                  const __grid_constant__ CUtensorMap tm_c,
                   const __grid_constant__ SplitStep P) {
   using namespace sg;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  float* staging = reinterpret_cast<float*>(smem + STAGES * STAGE_BYTES);
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES + STAGING_BYTES);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
   uint64_t* empty = full + STAGES;
   uint64_t* acc_full = empty + STAGES;
   uint64_t* acc_empty = acc_full + 2;
@@ -437,9 +429,11 @@ split_gemm_kernel(const __grid_constant__ CUtensorMap tm_hi, const __grid_consta
         }
       }
       if (!ok) break;
-      // C -= acc * inv_r * inv_c: the scaled update goes through this warp's
-      // staging buffers to TMA reduce-adds of 32 rows x RED_COLS columns, so the
-      // epilogue never waits for C to be read.
+      // C -= acc * inv_r * inv_c straight from the registers: per column, the
+      // warp's 32 lanes (32 consecutive rows) reduce 128 contiguous bytes of the
+      // column-major FP32 tile in L2 (red.global.add, round to nearest); nothing
+      // waits for the reductions, so the epilogue turns to the next tile's
+      // stages at once.  Each element of C has one writer per launch.
       int i, j, mb, nb;
       decode_item(P, L, i, j, mb, nb);
       const int mm = P.nt - P.band - 1;
@@ -447,30 +441,16 @@ split_gemm_kernel(const __grid_constant__ CUtensorMap tm_hi, const __grid_consta
       const int r0 = mb * PM + (int)rank * BM + quarter * 32;
       const int c0 = nb * BN + half * HALF_COLS;
       const float inv_r = P.inv_scale[(long long)i * P.ts + r0 + lane];
-      const float* inv_c = P.inv_scale + (long long)j * P.ts + c0;
-      float* stage_w = staging + (warp - 2) * 2 * (RED_BYTES / 4);
+      float inv_c[HALF_COLS / 32];  // lane l holds the scales of columns l, l + 32, ...
 #pragma unroll
-      for (int g = 0; g < HALF_COLS / RED_COLS; ++g, ++red_count) {
-        float* buf = stage_w + (red_count & 1) * (RED_BYTES / 4);
-        if (red_count >= 2) {
-          // the reduce issued two groups ago has finished reading this buffer
-          if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
-          __syncwarp();
-        }
+      for (int q = 0; q < HALF_COLS / 32; ++q) inv_c[q] = __ldg(P.inv_scale + (long long)j * P.ts + c0 + q * 32 + lane);
+      float* cp = P.c_pool + (slot * P.ts + c0) * (long long)P.ts + r0 + lane;
 #pragma unroll
-        for (int c = 0; c < RED_COLS; ++c)
-          buf[c * 32 + lane] = -(acc[g * RED_COLS + c] * inv_r) * __ldg(inv_c + g * RED_COLS + c);
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncwarp();
-        if (lane == 0) {
-          tma_reduce_add_2d(&tm_cr, buf, r0, (int)(slot * P.ts + c0 + g * RED_COLS));
-          asm volatile("cp.async.bulk.commit_group;" ::: "memory");
-        }
+      for (int c = 0; c < HALF_COLS; ++c) {
+        const float sc = __shfl_sync(0xffffffffu, inv_c[c >> 5], c & 31);
+        red_add_f32(cp + (long long)c * P.ts, -(acc[c] * inv_r) * sc);
       }
     }
-    // every reduce-add of this thread is complete before the CTA exits
-    if (lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
-    __syncwarp();
     if (!ok) bail = 1;
   }
   // neither CTA leaves (or frees its tensor memory) while the other may still
@@ -510,15 +490,10 @@ int split_tensor_map(void* storage, const __half* base, int ts, long long rows) 
 }
 
 // The off-band FP32 pool as a 2-D tensor (tile rows fastest, then every column
-// of every slot).  Two maps per pool: BM x BN boxes, the C block of a CTA tile
-// prefetched to L2, and 32 x RED_COLS boxes, the epilogue's reduce-adds.
-int split_c_tensor_map(void* storage, const float* c_pool, int ts, long long nslots, int box_rows, int box_cols);
-int split_c_maps(void* tm_c, void* tm_cr, const float* c_pool, int ts, long long nslots) {
-  int rc = split_c_tensor_map(tm_c, c_pool, ts, nslots, sg::BM, sg::BN);
-  if (rc == EGS_OK) rc = split_c_tensor_map(tm_cr, c_pool, ts, nslots, 32, sg::RED_COLS);
-  return rc;
-}
-int split_c_tensor_map(void* storage, const float* c_pool, int ts, long long nslots, int box_rows, int box_cols) {
+// of every slot) in BM x BN boxes: the C block of a CTA tile, prefetched to L2
+// before the tile's last stages.
+int split_c_map(void* storage, const float* c_pool, int ts, long long nslots) {
+  constexpr int box_rows = sg::BM, box_cols = sg::BN;
   std::memset(storage, 0, 128);
   if (nslots <= 0) return EGS_OK;  // no off-band tile, no update launches
   void* fn = nullptr;
@@ -589,7 +564,7 @@ static long long split_max_pairs() {
   return pairs_of[dev];
 }
 
-int launch_split_update(const void* tm_hi, const void* tm_lo, const void* tm_c, const void* tm_cr, int ts, int nt,
+int launch_split_update(const void* tm_hi, const void* tm_lo, const void* tm_c, int ts, int nt,
                         int band, int k, float* c_pool, const float* inv_scale, int* err, cudaStream_t st,
                         int max_ctas) {
   using namespace sg;
@@ -622,8 +597,7 @@ int launch_split_update(const void* tm_hi, const void* tm_lo, const void* tm_c, 
   const long long grid = 2 * pairs;
   split_gemm_kernel<<<(unsigned)grid, THREADS, SMEM_BYTES, st>>>(*reinterpret_cast<const CUtensorMap*>(tm_hi),
                                                                  *reinterpret_cast<const CUtensorMap*>(tm_lo),
-                                                                 *reinterpret_cast<const CUtensorMap*>(tm_c),
-                                                                 *reinterpret_cast<const CUtensorMap*>(tm_cr), P);
+                                                                 *reinterpret_cast<const CUtensorMap*>(tm_c), P);
   return launch_status("split_gemm_kernel");
 }
 
@@ -638,7 +612,7 @@ extern "C" int egs_split_update(int ts, int nt, int band, int k, const double* p
   __half *ph = nullptr, *pl = nullptr;
   float* inv = nullptr;
   int* err = nullptr;
-  alignas(64) unsigned char tmh[128], tml[128], tmc[128], tmcr[128];
+  alignas(64) unsigned char tmh[128], tml[128], tmc[128];
   const long long mm = nt - band - 1 > 0 ? nt - band - 1 : 0;
   int rc = EGS_OK;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -653,13 +627,13 @@ extern "C" int egs_split_update(int ts, int nt, int band, int k, const double* p
   cudaMemset(ph, 0, rows * ts * sizeof(__half));
   cudaMemset(pl, 0, rows * ts * sizeof(__half));
   if ((rc = split_tensor_map(tmh, ph, ts, rows)) != EGS_OK || (rc = split_tensor_map(tml, pl, ts, rows)) != EGS_OK ||
-      (rc = split_c_maps(tmc, tmcr, offband, ts, mm * (mm + 1) / 2)) != EGS_OK)
+      (rc = split_c_map(tmc, offband, ts, mm * (mm + 1) / 2)) != EGS_OK)
     goto done;
   launch_panel_split(panel, ts, k + 1, nt - k - 1, 0, inv, ph, pl, 0);
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   cudaEventRecord(e0, 0);
-  if ((rc = launch_split_update(tmh, tml, tmc, tmcr, ts, nt, band, k, offband, inv, err, 0)) != EGS_OK) goto done;
+  if ((rc = launch_split_update(tmh, tml, tmc, ts, nt, band, k, offband, inv, err, 0)) != EGS_OK) goto done;
   cudaEventRecord(e1, 0);
   if (cudaDeviceSynchronize() != cudaSuccess) {
     rc = EGS_ERR_CUDA;

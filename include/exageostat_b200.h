@@ -68,8 +68,10 @@ EGS_API int egs_problem_set_stream(egs_problem* p, void* cuda_stream);
  * tiles in the band, replacing ChameleonDST<T>::ExaGeoStatPotrfTile
  * (src/linear-algebra-solvers/concrete/chameleon/dst/ChameleonDST.cpp:23-150,
  * --computation=diag_approx --band=b).  The approximation is defined on the
- * caller's tiles, so band >= 1 requires dts to be a multiple of 64 (the device
- * tile); other sizes return EGS_ERR_INVALID. */
+ * caller's tiles of dts elements: when dts is a multiple of 64 they are the
+ * device tiles (tensor-core updates); otherwise the same loop runs on logical
+ * tiles of dts inside the device tiles, element by element (a slower form for
+ * small or odd tiles such as the reference's dts = 8 tests). */
 EGS_API int egs_problem_set_band(egs_problem* p, int band);
 
 /* Precision of the factorisation, the reference's Precision enum

@@ -92,9 +92,11 @@ Configurations modeling_config() {
   return c;
 }
 
-// TestExaGeoStatApi.cpp TEST_MODEL_DATA, section "Data Modeling"
-void modeling_fixture(const Fixture& f) {
+// TestExaGeoStatApi.cpp TEST_MODEL_DATA, section "Data Modeling", for the
+// exact dense factorisation and the diagonal super-tile approximation (dts 8)
+void modeling_fixture(const Fixture& f, Computation computation = EXACT_DENSE) {
   Configurations c = modeling_config();
+  c.SetComputation(computation);
   auto hardware = ExaGeoStatHardware(EXACT_DENSE, 4, 0);
   auto data = std::make_unique<ExaGeoStatData<double>>(c.GetProblemSize(), c.GetDimension());
   std::vector<double> z = f.z, x = f.x, y = f.y;
@@ -435,6 +437,7 @@ int main(int argc, char** argv) {
     if (which == "generate_n16") generate(16, 9);
     else if (which == "generate_n9") generate(9, 5);
     else if (which == "modeling_fixture") modeling_fixture(read_fixture(argv[2]));
+    else if (which == "modeling_fixture_dst") modeling_fixture(read_fixture(argv[2]), DIAGONAL_APPROX);
     else if (which == "generate_and_model") generate_and_model();
     else if (which == "mixed_modeling") mixed_modeling();
     else if (which == "prediction_mspe") prediction_mspe(read_fixture(argv[2]));

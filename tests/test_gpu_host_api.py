@@ -63,6 +63,15 @@ def test_data_modeling_fixture(driver, goldens, fixture_file):
 
 
 @pytest.mark.gpu
+def test_data_modeling_fixture_diagonal_approximation(driver, goldens, fixture_file):
+    # TestExaGeoStatApi.cpp:95: --computation=diag_approx on tiles of 8 (band 1)
+    out = run(driver, "modeling_fixture_dst", fixture_file)
+    g = goldens["modeling_loglik_n16"]
+    assert abs(out["loglik"] - g["diag_approx_band1"]) < g["margin"]
+    assert out["iterations"] == g["max_mle_iterations"]
+
+
+@pytest.mark.gpu
 def test_data_generation_and_modeling(driver, goldens):
     out = run(driver, "generate_and_model")
     g = goldens["modeling_loglik_n16"]

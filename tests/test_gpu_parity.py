@@ -357,15 +357,44 @@ def test_diagonal_super_tile_band_matches_oracle(band):
         assert logdet == pytest.approx(rlogdet, rel=1e-11)
 
 
-def test_diagonal_super_tile_needs_device_sized_tiles(goldens):
-    # The reference golden (dts 8, band 1) is pinned through the oracle
-    # (test_oracle_golden.py); the device refuses tiles it would have to merge.
-    p = egs.Problem(16, 8)
-    with pytest.raises(egs.EgsError) as ei:
-        p.set_band(1)
-    assert ei.value.status == egs.EGS_ERR_INVALID
-    p.set_band(0)
+def test_diagonal_approximation_golden_on_caller_tiles(goldens):
+    # TestExaGeoStatApi.cpp:95: DIAGONAL_APPROX with band 1 on tiles of 8 (the
+    # device tile is 64; the band is kept on the caller's tiles), the three
+    # BOBYQA evaluations of the reference test
+    f = goldens["fixture_n16"]
+    g = goldens["modeling_loglik_n16"]
+    p = egs.Problem(16, g["dts"])
+    p.set_band(1)
+    p.set_locations(f["x"], f["y"])
+    p.set_observations(f["z"])
+    vals = []
+    for th in ([0.1, 0.1, 0.1], [1.325, 0.1, 0.1], [0.1, 1.325, 0.1]):
+        ll, logdet, dot = p.mle_eval(th)
+        ref, rlogdet, rdot = O.dst_loglik(f["x"], f["y"], f["z"], th, g["dts"], 1, return_parts=True)
+        assert ll == pytest.approx(ref, rel=LOGLIK_RTOL, abs=0)
+        vals.append(ll)
+    assert abs(max(vals) - g["diag_approx_band1"]) < g["margin"]
 
+
+@pytest.mark.parametrize("n,dts,band", [(300, 8, 2), (500, 30, 3), (777, 100, 2), (1000, 96, 4), (640, 7, 6)])
+def test_diagonal_super_tile_on_odd_tiles_matches_oracle(n, dts, band):
+    # Caller tiles that are not device tiles: same contract as the device-tile
+    # form, failing exactly where the oracle fails
+    x, y, z = synthetic(n, 5, [1.0, 0.1, 0.5])
+    p = egs.Problem(n, dts)
+    p.set_band(band)
+    p.set_locations(x, y)
+    p.set_observations(z)
+    for theta in ([1.0, 0.1, 0.5], [0.8, 0.05, 0.9], [1.0, 0.02, 0.5]):
+        try:
+            ref, rlogdet, rdot = O.dst_loglik(x, y, z, theta, dts, band, return_parts=True)
+        except np.linalg.LinAlgError:
+            with pytest.raises(egs.NotPositiveDefinite):
+                p.mle_eval(theta)
+            continue
+        ll, logdet, dot = p.mle_eval(theta)
+        assert ll == pytest.approx(ref, rel=LOGLIK_RTOL, abs=0)
+        assert logdet == pytest.approx(rlogdet, rel=1e-11)
 
 
 def test_graph_replay_is_bit_identical_to_direct_launches():
