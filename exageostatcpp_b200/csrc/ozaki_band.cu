@@ -28,10 +28,11 @@
 //             N <= 256 over consecutive groups), the first K step with
 //             accumulate = 0;
 //   warps 2-9 epilogue: warp w reads TMEM lane quarter w % 4 and 32 of the 64
-//             columns, combines the groups in FP64 (smallest first), scales by
-//             2^(e_r + e_c) and subtracts from the FP64 band tile.
+//             columns, combines the groups exactly in 64-bit integers and then
+//             in FP64 (two roundings), scales by 2^(e_r + e_c) and subtracts
+//             from the FP64 band tile.
 // The accumulator is single-buffered (S groups fill TMEM); the epilogue
-// releases it as soon as its TMEM loads are done, before the C update.
+// releases it as soon as its last TMEM load is done, before the C update.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cstdint>
@@ -443,6 +444,19 @@ ozaki_band_kernel(const __grid_constant__ CUtensorMap tm_s, const __grid_constan
     uint32_t tcount = 0;
     bool ok = true;
     for (long long L = blockIdx.x; L < P.total && ok; L += gridDim.x, ++tcount) {
+      int i, j, mb, nb;
+      oz_decode(P, L, i, j, mb, nb);
+      const int r = mb * BM + quarter * 32 + lane;
+      const int c0 = nb * BN + half * 32;
+      double* cp = nullptr;  // this thread's row of the C block, column c0
+      if (P.mode == 0) {
+        cp = P.band_pool + ((long long)j * (P.band + 1) + (i - j)) * P.ts * P.ts + (long long)c0 * P.ts + r;
+        // the warp's 32 x 32 block of C into L2 while the tile's MMAs run: lane l
+        // fetches the two 128-byte lines of column c0 + l
+        const double* col = cp - lane + (long long)lane * P.ts;
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(col));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(col + 16));
+      }
       int w = 1;
       if (lane == 0) w = mbar_wait(acc_full, tcount & 1, P.err) ? 1 : 0;
       w = __shfl_sync(0xffffffffu, w, 0);
@@ -451,38 +465,60 @@ ozaki_band_kernel(const __grid_constant__ CUtensorMap tm_s, const __grid_constan
         break;
       }
       oz_fence_after();
+      // sum_d 2^(-7d) G_d with the groups combined exactly in 64-bit integers
+      // first (group g holds d = g + 2):
+      //   H = G_2 2^21 + G_3 2^14 + G_4 2^7 + G_5,   t = G_6 2^7 + G_7,
+      //   value = H 2^-35 + t 2^-49 + G_8 2^-56,
+      // |H| < 2^50 for K <= 16384, so H and t convert to FP64 exactly and the
+      // value takes two roundings; six FP64 operations per element instead of
+      // fourteen, which shortens the time the accumulator stays held.
+      static_assert(NGROUPS == 7, "the exact grouping below is written for seven slices");
       double acc[32];
-#pragma unroll
-      for (int c = 0; c < 32; ++c) acc[c] = 0.0;
-      // smallest groups first: sum_d 2^(-7d) G_d
-#pragma unroll 1
-      for (int g = NGROUPS - 1; g >= 0; --g) {
-        const double f = __longlong_as_double((long long)(1023 - 7 * (g + 2)) << 52);  // 2^(-7(g+2))
+      {
+        long long h[32];
         int v[32];
-        tmem_ld32_i32(tl + (uint32_t)(g * BN), v);
+        tmem_ld32_i32(tl, v);
 #pragma unroll
-        for (int c = 0; c < 32; ++c) acc[c] = fma((double)v[c], f, acc[c]);
+        for (int c = 0; c < 32; ++c) h[c] = v[c];
+#pragma unroll 1
+        for (int g = 1; g < 4; ++g) {
+          tmem_ld32_i32(tl + (uint32_t)(g * BN), v);
+#pragma unroll
+          for (int c = 0; c < 32; ++c) h[c] = h[c] * 128 + v[c];
+        }
+#pragma unroll
+        for (int c = 0; c < 32; ++c) acc[c] = (double)h[c] * 0x1p-35;
       }
-      oz_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(acc_empty);
-      int i, j, mb, nb;
-      oz_decode(P, L, i, j, mb, nb);
-      const int r = mb * BM + quarter * 32 + lane;
-      const int c0 = nb * BN + half * 32;
+      {
+        int v4[32], v5[32];
+        tmem_ld32_i32(tl + (uint32_t)(4 * BN), v4);
+        tmem_ld32_i32(tl + (uint32_t)(5 * BN), v5);
+#pragma unroll
+        for (int c = 0; c < 32; ++c) acc[c] = fma((double)((long long)v4[c] * 128 + v5[c]), 0x1p-49, acc[c]);
+      }
+      {
+        int v[32];
+        tmem_ld32_i32(tl + (uint32_t)(6 * BN), v);
+        // the last load has completed: the accumulator goes back to the MMAs
+        oz_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(acc_empty);
+#pragma unroll
+        for (int c = 0; c < 32; ++c) acc[c] = fma((double)v[c], 0x1p-56, acc[c]);
+      }
       const double sr = P.scale[(long long)i * P.ts + r];
       if (P.mode == 0) {
+        // all 32 loads of C first: a store may alias a later element as far as
+        // the compiler knows, so interleaved read-modify-writes would serialise
+        // 32 memory round trips per tile
         const double* sc = P.scale + (long long)j * P.ts + c0;
-        double* C = P.band_pool + ((long long)j * (P.band + 1) + (i - j)) * P.ts * P.ts;
-        double* cp = C + (long long)c0 * P.ts + r;
         const bool diag = (i == j);
+        double cv[32];
 #pragma unroll
-        for (int c = 0; c < 32; ++c) {
-          if (!diag || r >= c0 + c) {
-            double* e = cp + (long long)c * P.ts;
-            *e -= acc[c] * (sr * __ldg(sc + c));
-          }
-        }
+        for (int c = 0; c < 32; ++c) cv[c] = (!diag || r >= c0 + c) ? cp[(long long)c * P.ts] : 0.0;
+#pragma unroll
+        for (int c = 0; c < 32; ++c)
+          if (!diag || r >= c0 + c) cp[(long long)c * P.ts] = cv[c] - acc[c] * (sr * __ldg(sc + c));
       } else {
         const double* sc = P.scale + P.b_row_base + c0;
         double* cp = P.w_out + (long long)(i - P.k) * P.ts * P.ts + (long long)c0 * P.ts + r;
