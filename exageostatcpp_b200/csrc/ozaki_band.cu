@@ -18,20 +18,26 @@
 // its applications", Numer. Algorithms 59 (2012), with the integer-slice
 // variant of Ootomo, Ozaki and Yokota (2024).
 //
-// Kernel (one CTA per SM, persistent over 128 x 64 output tiles; 320 threads):
-//   warp 0    TMA producer: per 64-wide K stage the S slices of the tile's 128
-//             A rows and 64 B rows (64-byte swizzle), 2-stage ring;
-//   warp 1    allocates 512 TMEM columns -- S groups of 64 int32 columns, one
-//             per d, in order of d -- and issues the S(S+1)/2 slice products
-//             of a 32-wide K step from one thread as ten MMAs (the products of
-//             one A slice with up to four consecutive B slices form one MMA of
-//             N <= 256 over consecutive groups), the first K step with
-//             accumulate = 0;
+// The band update uses all S = 7 slices; the off-band panel solve (FP32-stored
+// rows times rows of L_kk^-1, written back in FP32) uses the first six, 2^-42
+// of the row maxima, which is 21 slice products instead of 28.
+//
+// Kernel (one CTA per SM, persistent over 128 x 64 output tiles; 320 threads;
+// NS = slices used):
+//   warp 0    TMA producer: per 64-wide K stage the NS slices of the tile's 128
+//             A rows and 64 B rows (64-byte swizzle), a ring of 2 (NS = 7) or
+//             3 (NS = 6) stages;
+//   warp 1    allocates 512 TMEM columns -- NS groups of 64 int32 columns, one
+//             per d, in order of d -- and issues the NS(NS+1)/2 slice products
+//             of a 32-wide K step from one thread as ten (NS = 7) or nine
+//             (NS = 6) MMAs (the products of one A slice with up to four
+//             consecutive B slices form one MMA of N <= 256 over consecutive
+//             groups), the first K step with accumulate = 0;
 //   warps 2-9 epilogue: warp w reads TMEM lane quarter w % 4 and 32 of the 64
 //             columns, combines the groups exactly in 64-bit integers and then
 //             in FP64 (two roundings), scales by 2^(e_r + e_c) and subtracts
 //             from the FP64 band tile.
-// The accumulator is single-buffered (S groups fill TMEM); the epilogue
+// The accumulator is single-buffered (NS groups fill TMEM); the epilogue
 // releases it as soon as its last TMEM load is done, before the C update.
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -46,20 +52,27 @@
 namespace egs {
 
 namespace oz {
-constexpr int S = kOzSlices;               // slices per operand
-constexpr int NGROUPS = S;                 // d = 2 .. S+1
+constexpr int S = kOzSlices;               // slices per operand stored (and used by the band update)
 constexpr int BM = 128, BN = 64, BK = 64;  // BK int8 = one 64-byte swizzle row
-constexpr int STAGES = 2;
 constexpr int BOX_ROWS = 64;
 constexpr int A_SLICE = BM * BK;           // 8 KB
 constexpr int B_SLICE = BN * BK;           // 4 KB
-constexpr int STAGE_BYTES = S * (A_SLICE + B_SLICE);
 constexpr int EPI_WARPS = 8;
 constexpr int THREADS = 64 + 32 * EPI_WARPS;
-constexpr int SMEM_BYTES = 1024 + STAGES * STAGE_BYTES + 256;
 constexpr uint32_t TMEM_COLS = 512;
-static_assert(NGROUPS * BN <= (int)TMEM_COLS, "groups fit in tensor memory");
-static_assert(SMEM_BYTES <= 232448, "shared memory per CTA");
+constexpr int kMaxSmem = 232448;
+// A kernel that uses the first NS slices of each operand: ring stages of NS
+// (A, B) slice pairs, as many as fit up to three, and NS int32 groups of BN
+// columns in tensor memory (groups d = 2 .. NS + 1).
+template <int NS>
+struct Cfg {
+  static constexpr int STAGE_BYTES = NS * (A_SLICE + B_SLICE);
+  static constexpr int STAGES = 1024 + 3 * STAGE_BYTES + 256 <= kMaxSmem ? 3 : 2;
+  static constexpr int SMEM_BYTES = 1024 + STAGES * STAGE_BYTES + 256;
+  static_assert(NS >= 1 && NS <= S, "slices stored per operand");
+  static_assert(NS * BN <= (int)TMEM_COLS, "groups fit in tensor memory");
+  static_assert(SMEM_BYTES <= kMaxSmem, "shared memory per CTA");
+};
 // Instruction descriptor of kind::i8: D S32 (bits 4-5 = 2), A and B signed 8-bit
 // (bits 7-9 = 1, bits 10-12 = 1), both K-major, N >> 3 at bits 17-22, M >> 4 at 24-28.
 constexpr uint32_t idesc_i8(int n) {
@@ -77,7 +90,7 @@ constexpr uint32_t idesc_i8(int n) {
 // strip once for its row maxima, then again in 64 x 64 blocks, transposed
 // through shared memory into the row-major (K contiguous) outputs
 // slices[p][row][c] and Ph / Pl[row][c].
-template <typename T, bool kSplit>
+template <typename T, bool kSplit, int NP>
 __global__ void __launch_bounds__(256, 2)
 panel_prepare_kernel(const T* __restrict__ tiles0, int ts, int row_tile0, double* __restrict__ oz_scale,
                      int8_t* __restrict__ slices, long long slice_stride, float* __restrict__ inv_scale,
@@ -145,7 +158,7 @@ panel_prepare_kernel(const T* __restrict__ tiles0, int ts, int row_tile0, double
       double v[16];
 #pragma unroll
       for (int c = 0; c < 16; ++c) v[c] = Sm[r][cq + c] * io;  // |v| < 1
-      oz_emit_slices(v, slices + (grow0 + r) * ts + c0 + cq, slice_stride);
+      oz_emit_slices<NP>(v, slices + (grow0 + r) * ts + c0 + cq, slice_stride);
     } else {
       const int tt = threadIdx.x & 127, r = tt >> 1;
       const bool to_f16 = threadIdx.x >= 128;  // warp-uniform
@@ -160,7 +173,7 @@ panel_prepare_kernel(const T* __restrict__ tiles0, int ts, int row_tile0, double
         if (to_f16)
           f16_emit_split(v, Ph + off, Pl + off);
         else
-          oz_emit_slices(v, slices + off, slice_stride);  // |v| < 1
+          oz_emit_slices<NP>(v, slices + off, slice_stride);  // |v| < 1
       }
     }
   }
@@ -181,7 +194,9 @@ ozaki_rowscale_rm_kernel(const double* __restrict__ src, int ts, long long row0,
   if (lane == 0) scale[row0 + r] = oz_row_scale(m);
 }
 
-// Slices of rows stored row by row (row r at src + r ts) into slice rows row0 + r.
+// The first NP slices of rows stored row by row (row r at src + r ts) into
+// slice rows row0 + r.
+template <int NP>
 __global__ void __launch_bounds__(256)
 ozaki_slice_rm_kernel(const double* __restrict__ src, int ts, long long row0, const double* __restrict__ scale,
                       int8_t* __restrict__ slices, long long slice_stride) {
@@ -195,7 +210,7 @@ ozaki_slice_rm_kernel(const double* __restrict__ src, int ts, long long row0, co
   double v[16];
 #pragma unroll
   for (int c = 0; c < 16; ++c) v[c] = row[c] * inv;
-  oz_emit_slices(v, slices + (row0 + r) * ts + cq, slice_stride);
+  oz_emit_slices<NP>(v, slices + (row0 + r) * ts + cq, slice_stride);
 }
 
 // ---------------------------------------------------------------------------
@@ -320,9 +335,11 @@ __device__ __forceinline__ void oz_decode(const OzStep& P, long long L, int& i, 
   }
 }
 
+template <int NS>
 __global__ void __launch_bounds__(oz::THREADS, 1)
 ozaki_band_kernel(const __grid_constant__ CUtensorMap tm_s, const __grid_constant__ OzStep P) {
   using namespace oz;
+  constexpr int STAGES = Cfg<NS>::STAGES, STAGE_BYTES = Cfg<NS>::STAGE_BYTES;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
@@ -374,10 +391,10 @@ ozaki_band_kernel(const __grid_constant__ CUtensorMap tm_s, const __grid_constan
           mbar_expect_tx(&full[s], STAGE_BYTES);
           const int x = kt * BK;
 #pragma unroll 1
-          for (int p = 0; p < S; ++p) {
+          for (int p = 0; p < NS; ++p) {
             oz_tma_3d(st + p * A_SLICE, &tm_s, &full[s], x, arow, p);
             oz_tma_3d(st + p * A_SLICE + BOX_ROWS * BK, &tm_s, &full[s], x, arow + BOX_ROWS, p);
-            oz_tma_3d(st + S * A_SLICE + p * B_SLICE, &tm_s, &full[s], x, brow, p);
+            oz_tma_3d(st + NS * A_SLICE + p * B_SLICE, &tm_s, &full[s], x, brow, p);
           }
         }
       }
@@ -402,21 +419,22 @@ ozaki_band_kernel(const __grid_constant__ CUtensorMap tm_s, const __grid_constan
           }
           oz_fence_after();
           const uint32_t sa = smem_u32(smem + s * STAGE_BYTES);
-          const uint32_t sb = sa + S * A_SLICE;
-          // A slice p against B slices q = 1 .. S+1-p: group d = p + q sits at
+          const uint32_t sb = sa + NS * A_SLICE;
+          // A slice p against B slices q = 1 .. NS+1-p: group d = p + q sits at
           // TMEM columns (d - 2) BN and the B slices are stacked in shared
           // memory, so the products of A_p with B_q .. B_q+m-1 are one MMA of
           // N = m BN into the columns of groups p+q .. p+q+m-1 (N <= 256: at
-          // most four slices a time).  Ten MMAs per 32-wide K step; an A slice
-          // used by two of them is read once through the collector buffer.
+          // most four slices a time).  Ten MMAs per 32-wide K step for seven
+          // slices, nine for six; an A slice used by two of them is read once
+          // through the collector buffer.
 #pragma unroll
           for (int kk = 0; kk < BK / 32; ++kk) {
 #pragma unroll
-            for (int p = 1; p <= S; ++p) {
+            for (int p = 1; p <= NS; ++p) {
               const uint64_t ad = sdesc_sw64(sa + (p - 1) * A_SLICE + kk * 32);
               const uint32_t acc = (kt > 0 || kk > 0 || p > 1) ? 1u : 0u;  // p = 1 opens every group
               constexpr int kMaxSlices = 256 / BN;
-              const int qmax = S + 1 - p;
+              const int qmax = NS + 1 - p;
               const int nmma = (qmax + kMaxSlices - 1) / kMaxSlices;
 #pragma unroll
               for (int q0 = 1; q0 <= qmax; q0 += kMaxSlices) {
@@ -468,11 +486,11 @@ ozaki_band_kernel(const __grid_constant__ CUtensorMap tm_s, const __grid_constan
       // sum_d 2^(-7d) G_d with the groups combined exactly in 64-bit integers
       // first (group g holds d = g + 2):
       //   H = G_2 2^21 + G_3 2^14 + G_4 2^7 + G_5,   t = G_6 2^7 + G_7,
-      //   value = H 2^-35 + t 2^-49 + G_8 2^-56,
+      //   value = H 2^-35 + t 2^-49 (+ G_8 2^-56 with seven slices),
       // |H| < 2^50 for K <= 16384, so H and t convert to FP64 exactly and the
-      // value takes two roundings; six FP64 operations per element instead of
-      // fourteen, which shortens the time the accumulator stays held.
-      static_assert(NGROUPS == 7, "the exact grouping below is written for seven slices");
+      // value takes at most two roundings; the tensor memory goes back to the
+      // MMAs right after the last group's load.
+      static_assert(NS == 6 || NS == 7, "the exact grouping below is written for six or seven slices");
       double acc[32];
       {
         long long h[32];
@@ -493,13 +511,17 @@ ozaki_band_kernel(const __grid_constant__ CUtensorMap tm_s, const __grid_constan
         int v4[32], v5[32];
         tmem_ld32_i32(tl + (uint32_t)(4 * BN), v4);
         tmem_ld32_i32(tl + (uint32_t)(5 * BN), v5);
+        if constexpr (NS == 6) {
+          oz_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(acc_empty);
+        }
 #pragma unroll
         for (int c = 0; c < 32; ++c) acc[c] = fma((double)((long long)v4[c] * 128 + v5[c]), 0x1p-49, acc[c]);
       }
-      {
+      if constexpr (NS == 7) {
         int v[32];
         tmem_ld32_i32(tl + (uint32_t)(6 * BN), v);
-        // the last load has completed: the accumulator goes back to the MMAs
         oz_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(acc_empty);
@@ -568,7 +590,7 @@ int ozaki_tensor_map(void* storage, const int8_t* slices, int ts, long long rows
 void launch_ozaki_slice(const double* W, int ts, int t0, int ntiles, int row_tile0, double* scale, int8_t* slices,
                         long long rows, cudaStream_t st) {
   if (ntiles <= 0) return;
-  panel_prepare_kernel<double, false><<<dim3(ts / 64, ntiles), 256, 0, st>>>(
+  panel_prepare_kernel<double, false, kOzSlices><<<dim3(ts / 64, ntiles), 256, 0, st>>>(
       W + (long long)t0 * ts * ts, ts, row_tile0 + t0, scale, slices, rows * (long long)ts, nullptr, nullptr, nullptr);
 }
 
@@ -577,7 +599,7 @@ void launch_ozaki_slice(const double* W, int ts, int t0, int ntiles, int row_til
 void launch_panel_prepare(const double* W, int ts, int t0, int ntiles, int row_tile0, double* oz_scale,
                           int8_t* slices, long long rows, float* inv_scale, __half* Ph, __half* Pl, cudaStream_t st) {
   if (ntiles <= 0) return;
-  panel_prepare_kernel<double, true><<<dim3(ts / 64, ntiles), 256, 0, st>>>(
+  panel_prepare_kernel<double, true, kOzSlices><<<dim3(ts / 64, ntiles), 256, 0, st>>>(
       W + (long long)t0 * ts * ts, ts, row_tile0 + t0, oz_scale, slices, rows * (long long)ts, inv_scale, Ph, Pl);
 }
 
@@ -585,7 +607,7 @@ void launch_panel_prepare(const double* W, int ts, int t0, int ntiles, int row_t
 void launch_ozaki_slice_f32(const float* tiles0, int ts, int ntiles, int row_tile0, double* scale, int8_t* slices,
                             long long rows, cudaStream_t st) {
   if (ntiles <= 0) return;
-  panel_prepare_kernel<float, false><<<dim3(ts / 64, ntiles), 256, 0, st>>>(
+  panel_prepare_kernel<float, false, kOzPanelSlices><<<dim3(ts / 64, ntiles), 256, 0, st>>>(
       tiles0, ts, row_tile0, scale, slices, rows * (long long)ts, nullptr, nullptr, nullptr);
 }
 
@@ -594,7 +616,7 @@ void launch_ozaki_slice_rows(const double* src, int ts, long long row0, double* 
                              long long rows, cudaStream_t st) {
   ozaki_rowscale_rm_kernel<<<(ts + 7) / 8, 256, 0, st>>>(src, ts, row0, scale);
   const long long chunks = (long long)ts * (ts / 16);
-  ozaki_slice_rm_kernel<<<(unsigned)((chunks + 255) / 256), 256, 0, st>>>(src, ts, row0, scale, slices,
+  ozaki_slice_rm_kernel<kOzPanelSlices><<<(unsigned)((chunks + 255) / 256), 256, 0, st>>>(src, ts, row0, scale, slices,
                                                                           rows * (long long)ts);
 }
 
@@ -616,13 +638,16 @@ long long ozaki_targets(int ts, int nt, int band, int k, std::vector<int4>& out)
   return items;
 }
 
+template <int NS>
 static int launch_ozaki(const void* tm_s, const OzStep& P, cudaStream_t st) {
   using namespace oz;
+  constexpr int SMEM_BYTES = Cfg<NS>::SMEM_BYTES;
   static std::once_flag attr_done[64];
-  once_per_device(attr_done,
-                  []() { cudaFuncSetAttribute(ozaki_band_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES); });
+  once_per_device(attr_done, []() {
+    cudaFuncSetAttribute(ozaki_band_kernel<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+  });
   const long long grid = P.total < gemm_num_sms() ? P.total : gemm_num_sms();
-  ozaki_band_kernel<<<(unsigned)grid, THREADS, SMEM_BYTES, st>>>(*reinterpret_cast<const CUtensorMap*>(tm_s), P);
+  ozaki_band_kernel<NS><<<(unsigned)grid, THREADS, SMEM_BYTES, st>>>(*reinterpret_cast<const CUtensorMap*>(tm_s), P);
   return launch_status("ozaki_band_kernel");
 }
 
@@ -653,7 +678,7 @@ int launch_ozaki_trsm(const void* tm_s, const int4* targets, int ntargets, long 
   P.w_out = w_out;
   P.scale = scale;
   P.err = err;
-  return launch_ozaki(tm_s, P, st);
+  return launch_ozaki<kOzPanelSlices>(tm_s, P, st);
 }
 
 int launch_ozaki_band(const void* tm_s, const int4* targets, int ntargets, long long total, int ts, int band,
@@ -671,7 +696,7 @@ int launch_ozaki_band(const void* tm_s, const int4* targets, int ntargets, long 
   P.band_pool = band_pool;
   P.scale = scale;
   P.err = err;
-  return launch_ozaki(tm_s, P, st);
+  return launch_ozaki<kOzSlices>(tm_s, P, st);
 }
 
 }  // namespace egs

@@ -9,6 +9,11 @@
 namespace egs {
 
 constexpr int kOzSlices = 7;  // signed 7-bit slices per value (2^-49 of the row maximum)
+// Slices of the off-band panel solve (FP32-stored rows times rows of L_kk^-1):
+// 2^-42 of the row maxima.  The product with the inverse can cancel by the
+// size of L_kk^-1's entries (10^4 to 10^5 for smooth kernels), which 2^-42
+// still keeps below the FP32 rounding the solved rows get in storage.
+constexpr int kOzPanelSlices = 6;
 
 // FP16 split scale of a row with maximum m: inv_scale = 2^(e - 13) for
 // 2^e <= m < 2^(e+1), so the scaled row lies below 2^14; rows whose maximum is
@@ -30,14 +35,16 @@ __device__ __forceinline__ double oz_row_scale(double m) {
   return (e >= 1023) ? __longlong_as_double(0x7ff8000000000000ll) : ldexp(1.0, e + 1);
 }
 
-// Seven signed 7-bit slices of 16 scaled values (|v| < 1), one 16-byte store
-// per slice: slice p (1..7) of v is sign(v) * (floor(|v| 2^(7p)) mod 2^7),
+// The first NP (at most seven) signed 7-bit slices of 16 scaled values
+// (|v| < 1), one 16-byte store per slice: slice p (1..NP) of v is sign(v) * (floor(|v| 2^(7p)) mod 2^7),
 // read off the truncated 49-bit fixed-point magnitude floor(|v| 2^49), which
 // is the double's significand shifted by its exponent.  These are the values
 // the repeated exact steps a_p = trunc(2^7 v), v <- 2^7 v - a_p give; the
 // integer form keeps the slicing off the FP64 pipe.  Zero, subnormal and
 // non-finite inputs give zero slices.
+template <int NP = kOzSlices>
 __device__ __forceinline__ void oz_emit_slices(const double (&v)[16], int8_t* dst, long long slice_stride) {
+  static_assert(NP >= 1 && NP <= kOzSlices, "slices of the 49-bit magnitude");
   unsigned long long mag[16];
   unsigned neg = 0;
 #pragma unroll
@@ -50,7 +57,7 @@ __device__ __forceinline__ void oz_emit_slices(const double (&v)[16], int8_t* ds
     neg |= (unsigned)(b >> 63) << c;
   }
 #pragma unroll
-  for (int p = 1; p <= kOzSlices; ++p) {
+  for (int p = 1; p <= NP; ++p) {
     union {
       int8_t b[16];
       int4 q;
