@@ -777,13 +777,13 @@ def main():
 
     # --- rooflines of the update kernels (CUDA events around every launch) ---------------
     # DRAM bytes (read + write) per algorithmic flop of each kernel, from one ncu
-    # capture of each at N = 16,384: the split kernel moved 807,166,464 B for 78
-    # target tiles of 2 * 1024^3 flops; the Ozaki kernel 644,593,920 B for the band
+    # capture of each at N = 16,384: the split kernel moved 789,244,160 B for 78
+    # target tiles of 2 * 1024^3 flops; the Ozaki kernel 654,302,464 B for the band
     # update of step 0, 7.410e10 FP64-equivalent flops.
     # Both kernels' traffic grows with their target tiles, so a launch's traffic
     # is this ratio times its flops.
-    split_bytes_per_flop = 807166464.0 / (78 * 2.0 * 1024 ** 3)
-    ozaki_bytes_per_flop = 644593920.0 / 7.410e10
+    split_bytes_per_flop = 789244160.0 / (78 * 2.0 * 1024 ** 3)
+    ozaki_bytes_per_flop = 654302464.0 / 7.410e10
     traffic_note = ("DRAM read + write bytes per flop from one ncu capture at N=16384, times this launch's "
                     "algorithmic flops")
     lo = egs.STAGES.index("update_low")
